@@ -1,0 +1,468 @@
+// Device-side SDF evaluation for sm_100a.
+//
+// Arithmetic: every floating-point operation on the parity path is written as an explicit
+// round-to-nearest intrinsic (__fmul_rn, __fadd_rn, __fsub_rn, __fmaf_rn, __fdiv_rn, __fsqrt_rn), so
+// no result depends on the compiler's contraction choices. The sequence of operations - including
+// which products are fused into adds - is the one the reference's compiled code performs, pinned
+// against the reference's own outputs on the GPU. The functions restate, in that exact order:
+//   SDF primitives        MarchingCubesKernels.cu:129-219
+//   displacements         MarchingCubesKernels.cu:229-243, 604-606
+//   world -> local        MarchingCubesKernels.cu:597-599, Commons.cuh:264-278
+//   CSG combine           MarchingCubesKernels.cu:631-694
+//   map()                 MarchingCubesKernels.cu:570-808
+//   computeNormal         MarchingCubesKernels.cu:814-844
+//
+// Traversal: map() is evaluated for 32 points at once by one warp. The reference runs an
+// independent depth-first search per point (64-entry stack, right child pushed first, at most 256
+// popped nodes, a node is skipped when its box is not closer than the running distance). Here the
+// warp walks ONE stack whose entries are (node, mask of lanes that pushed it). Lane L's own stack is
+// exactly the subsequence of warp entries whose mask holds L, in the same LIFO order, so each lane
+// visits the same nodes in the same order, pops the same number of nodes before the cap, and folds
+// the same primitives in the same order: results are identical to the per-point search, while node
+// and primitive loads are warp-uniform (one broadcast load instead of 32 divergent ones).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sdfb {
+
+// ------------------------------------------------------------------------------------------------
+// exact-operation helpers
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ float MUL(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float ADD(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float SUB(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float FMA(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float DIV(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float SQRT(float a) { return __fsqrt_rn(a); }
+__device__ __forceinline__ float CLAMP(float v, float lo, float hi) { return fmaxf(lo, fminf(v, hi)); }
+
+__device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 add3(float3 a, float3 b) { return f3(ADD(a.x, b.x), ADD(a.y, b.y), ADD(a.z, b.z)); }
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return f3(SUB(a.x, b.x), SUB(a.y, b.y), SUB(a.z, b.z)); }
+__device__ __forceinline__ float3 scl3(float3 a, float s) { return f3(MUL(s, a.x), MUL(s, a.y), MUL(s, a.z)); }
+// a.x*b.x + a.y*b.y + a.z*b.z
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return FMA(a.z, b.z, FMA(a.x, b.x, MUL(a.y, b.y))); }
+__device__ __forceinline__ float len3(float3 a) { return SQRT(dot3(a, a)); }
+__device__ __forceinline__ float len2(float x, float y) { return SQRT(FMA(x, x, MUL(y, y))); }
+// a*b - c*d
+__device__ __forceinline__ float det2(float a, float b, float c, float d) { return FMA(a, b, -MUL(c, d)); }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+    return f3(det2(a.y, b.z, a.z, b.y), det2(a.z, b.x, a.x, b.z), det2(a.x, b.y, a.y, b.x));
+}
+__device__ __forceinline__ bool finite3(float3 v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z); }
+
+// ------------------------------------------------------------------------------------------------
+// scene view: primitives in the reference layout (10 float4 rows of 160 bytes), nodes in the
+// reference layout (2 float4 rows of 32 bytes)
+// ------------------------------------------------------------------------------------------------
+enum { P_SPHERE = 0, P_BOX, P_TORUS, P_CYLINDER, P_CAPSULE, P_CONE, P_RBOX, P_RCYL, P_RCONE, P_ELLIPSOID,
+       P_TRIPRISM, P_OCTA, P_HEXPRISM };
+enum { OP_UNION = 0, OP_SUB, OP_INT, OP_UNION_BLEND, OP_SUB_BLEND, OP_INT_BLEND };
+enum { DSP_NONE = 0, DSP_SINE, DSP_TWIST, DSP_BEND };
+
+struct SceneView {
+    const float4* prims;  // 10 rows per primitive
+    const float4* nodes;  // 2 rows per node
+    int nprims;
+    int nbvh;             // primitives [0, nbvh) are in the BVH, the rest form the linear pass
+    int nnodes;
+};
+
+constexpr int PRIM_ROWS = 10;
+constexpr int MAP_STACK = 64;   // the reference's per-point stack (MarchingCubesKernels.cu:577)
+constexpr int MAP_CAP = 256;    // the reference's popped-node cap (:582)
+
+// row 0 rotation | 1 dispParams | 2 position, blend | 3 scale, rounding | 4 color, annular |
+// 5 params[0..3] | 6 params[4..5], type, operation | 7 displacement, pad, uvScale |
+// 8 uvOffset, uvRotation, uvMode | 9 textureID, atlasIslandID, pad
+struct Leaf {
+    float4 rot, pos, scale, prm;
+    float annular, rounding;
+    int type, op, disp;
+    float dp0, dp1;
+};
+
+__device__ __forceinline__ Leaf load_leaf(const float4* __restrict__ pr) {
+    Leaf L;
+    L.rot = __ldg(pr + 0);
+    L.pos = __ldg(pr + 2);
+    L.scale = __ldg(pr + 3);
+    const float4 r4 = __ldg(pr + 4);
+    L.prm = __ldg(pr + 5);
+    const float4 r6 = __ldg(pr + 6);
+    const float4 r7 = __ldg(pr + 7);
+    L.annular = r4.w;
+    L.rounding = L.scale.w;
+    L.type = __float_as_int(r6.z);
+    L.op = __float_as_int(r6.w);
+    L.disp = __float_as_int(r7.x);
+    L.dp0 = 0.f;
+    L.dp1 = 0.f;
+    if (L.disp == DSP_SINE || L.disp == DSP_TWIST || L.disp == DSP_BEND) {
+        const float4 r1 = __ldg(pr + 1);
+        L.dp0 = r1.x;
+        L.dp1 = r1.y;
+    }
+    return L;
+}
+
+// rotateVector with u = q.xyz, s = q.w (Commons.cuh:264-273)
+__device__ __forceinline__ float3 rotate(float3 v, float ux, float uy, float uz, float s) {
+    const float3 u = f3(ux, uy, uz);
+    const float a = MUL(2.0f, dot3(u, v));
+    const float b = FMA(s, s, -dot3(u, u));
+    const float c = MUL(2.0f, s);
+    const float3 cr = cross3(u, v);
+    return f3(FMA(c, cr.x, FMA(a, u.x, MUL(b, v.x))), FMA(c, cr.y, FMA(a, u.y, MUL(b, v.y))),
+              FMA(c, cr.z, FMA(a, u.z, MUL(b, v.z))));
+}
+// world -> primitive local: subtract position, conjugate rotation, divide by scale
+__device__ __forceinline__ float3 to_local(float3 pw, float4 rot, float4 pos, float4 scale) {
+    float3 p = f3(SUB(pw.x, pos.x), SUB(pw.y, pos.y), SUB(pw.z, pos.z));
+    p = rotate(p, -rot.x, -rot.y, -rot.z, rot.w);
+    return f3(DIV(p.x, scale.x), DIV(p.y, scale.y), DIV(p.z, scale.z));
+}
+
+// ---------------------------------------------------------------- primitive distance functions
+__device__ __forceinline__ float sd_sphere(float3 p, float r) { return SUB(len3(p), r); }
+__device__ __forceinline__ float sd_box(float3 p, float bx, float by, float bz) {
+    const float qx = SUB(fabsf(p.x), bx), qy = SUB(fabsf(p.y), by), qz = SUB(fabsf(p.z), bz);
+    return ADD(len3(f3(fmaxf(qx, 0.f), fmaxf(qy, 0.f), fmaxf(qz, 0.f))), fminf(fmaxf(qx, fmaxf(qy, qz)), 0.f));
+}
+__device__ __forceinline__ float sd_torus(float3 p, float r1, float r2) {
+    return SUB(len2(SUB(len2(p.x, p.z), r1), p.y), r2);
+}
+__device__ __forceinline__ float sd_cylinder(float3 p, float h, float r) {
+    const float dx = SUB(fabsf(len2(p.x, p.z)), r), dy = SUB(fabsf(p.y), h);
+    return ADD(fminf(fmaxf(dx, dy), 0.f), len3(f3(fmaxf(dx, 0.f), fmaxf(dy, 0.f), 0.f)));
+}
+__device__ __forceinline__ float sd_capsule(float3 p, float h, float r) {
+    p.y = SUB(p.y, CLAMP(p.y, 0.f, h));
+    return SUB(len3(p), r);
+}
+__device__ __forceinline__ float sd_cone(float3 p, float h, float angle) {
+    const float cx = sinf(MUL(angle, 0.0174533f)), cy = cosf(MUL(angle, 0.0174533f));
+    const float qx = MUL(h, DIV(cx, cy)), qy = -h;
+    const float wx = len2(p.x, p.z), wy = p.y;
+    const float dwq = FMA(wx, qx, MUL(wy, qy));
+    const float dqq = FMA(qx, qx, MUL(qy, qy));
+    const float t = CLAMP(DIV(dwq, dqq), 0.f, 1.f);
+    const float ax = FMA(-qx, t, wx), ay = FMA(-qy, t, wy);
+    const float tb = CLAMP(DIV(wx, qx), 0.f, 1.f);
+    const float bx = FMA(-qx, tb, wx), by = SUB(wy, qy);
+    const float k = (qy > 0.f) ? 1.f : -1.f;
+    const float d = fminf(FMA(ax, ax, MUL(ay, ay)), FMA(bx, bx, MUL(by, by)));
+    const float s = fmaxf(MUL(k, det2(wx, qy, wy, qx)), MUL(k, SUB(wy, qy)));
+    return MUL(SQRT(d), (s > 0.f ? 1.f : -1.f));
+}
+__device__ __forceinline__ float sd_ellipsoid(float3 p, float rx, float ry, float rz) {
+    const float k0 = len3(f3(DIV(p.x, rx), DIV(p.y, ry), DIV(p.z, rz)));
+    const float k1 = len3(f3(DIV(p.x, MUL(rx, rx)), DIV(p.y, MUL(ry, ry)), DIV(p.z, MUL(rz, rz))));
+    return DIV(MUL(k0, SUB(k0, 1.f)), k1);
+}
+__device__ __forceinline__ float sd_octahedron(float3 p, float s) {
+    return MUL(SUB(ADD(ADD(fabsf(p.x), fabsf(p.y)), fabsf(p.z)), s), 0.57735027f);
+}
+__device__ __forceinline__ float sd_triprism(float3 p, float hx, float hy) {
+    const float qx = fabsf(p.x), qz = fabsf(p.z);
+    return fmaxf(SUB(qz, hy), FMA(-hx, 0.5f, fmaxf(FMA(qx, 0.866025f, MUL(p.y, 0.5f)), -p.y)));
+}
+__device__ __forceinline__ float sd_rounded_cone(float3 p, float h, float r1, float r2) {
+    const float qx = len2(p.x, p.z), qy = p.y;
+    const float b = DIV(SUB(r1, r2), h);
+    const float a = SQRT(FMA(-b, b, 1.f));
+    const float k = FMA(qx, -b, MUL(qy, a));
+    if (k < 0.f) return SUB(len2(qx, qy), r1);
+    if (k > MUL(a, h)) return SUB(len2(qx, SUB(qy, h)), r2);
+    return SUB(FMA(qx, a, MUL(qy, b)), r1);
+}
+__device__ __forceinline__ float sd_rounded_cylinder(float3 p, float h, float r1, float r2) {
+    const float dx = ADD(FMA(-2.f, r1, len2(p.x, p.z)), r2), dy = SUB(fabsf(p.y), h);
+    return SUB(ADD(fminf(fmaxf(dx, dy), 0.f), len2(fmaxf(dx, 0.f), fmaxf(dy, 0.f))), r2);
+}
+__device__ __forceinline__ float sd_hexprism(float3 p, float hx, float hy) {
+    const float kx = -0.8660254f, ky = 0.5f, kz = 0.57735027f;
+    p = f3(fabsf(p.x), fabsf(p.y), fabsf(p.z));
+    const float m = fminf(FMA(kx, p.x, MUL(ky, p.z)), 0.f);
+    const float px = FMA(-MUL(kx, 2.f), m, p.x), pz = FMA(-MUL(ky, 2.f), m, p.z);
+    const float ex = SUB(px, CLAMP(px, MUL(-kz, hx), MUL(kz, hx))), ez = SUB(pz, hx);
+    const float dx = MUL(len2(ex, ez), copysignf(1.f, SUB(pz, hx))), dy = SUB(p.y, hy);
+    return ADD(fminf(fmaxf(dx, dy), 0.f), len2(fmaxf(dx, 0.f), fmaxf(dy, 0.f)));
+}
+
+__device__ __forceinline__ float sd_eval(int type, float3 p, float4 pm) {
+    switch (type) {
+        case P_SPHERE: return sd_sphere(p, pm.x);
+        case P_BOX: return sd_box(p, pm.x, pm.y, pm.z);
+        case P_TORUS: return sd_torus(p, pm.x, pm.y);
+        case P_CYLINDER: return sd_cylinder(p, pm.x, pm.y);
+        case P_CAPSULE: return sd_capsule(p, pm.x, pm.y);
+        case P_CONE: return sd_cone(p, pm.x, pm.y);
+        case P_RBOX: return SUB(sd_box(p, pm.x, pm.y, pm.z), pm.w);
+        case P_ELLIPSOID: return sd_ellipsoid(p, pm.x, pm.y, pm.z);
+        case P_OCTA: return sd_octahedron(p, pm.x);
+        case P_TRIPRISM: return sd_triprism(p, pm.x, pm.y);
+        case P_RCYL: return sd_rounded_cylinder(p, pm.x, pm.y, pm.z);
+        case P_RCONE: return sd_rounded_cone(p, pm.x, pm.y, pm.z);
+        case P_HEXPRISM: return sd_hexprism(p, pm.x, pm.y);
+        default: return SUB(len3(p), 1.f);
+    }
+}
+
+// leaf: local transform, displacement, distance, min-scale, annular, rounding (:594-629)
+__device__ __forceinline__ float leaf_distance(const Leaf& L, float3 pw, float time, float3& pre) {
+    float3 p = to_local(pw, L.rot, L.pos, L.scale);
+    pre = p;
+    if (L.disp == DSP_TWIST) {
+        const float c = cosf(MUL(L.dp0, p.y)), s = sinf(MUL(L.dp0, p.y));
+        p = f3(det2(c, p.x, s, p.z), p.y, FMA(s, p.x, MUL(c, p.z)));
+    } else if (L.disp == DSP_BEND) {
+        const float c = cosf(MUL(L.dp0, p.x)), s = sinf(MUL(L.dp0, p.x));
+        p = f3(det2(c, p.x, s, p.y), FMA(s, p.x, MUL(c, p.y)), p.z);
+    } else if (L.disp == DSP_SINE) {
+        p.y = FMA(sinf(FMA(p.x, L.dp0, time)), L.dp1, p.y);
+    }
+    float d = sd_eval(L.type, p, L.prm);
+    d = MUL(d, fminf(L.scale.x, fminf(L.scale.y, L.scale.z)));
+    if (L.annular > 0.f) d = SUB(fabsf(d), L.annular);
+    if (L.rounding > 0.f) d = SUB(d, L.rounding);
+    return d;
+}
+
+// mix(x, y, a) = x*(1-a) + y*a (Commons.cuh:247)
+__device__ __forceinline__ float mixf(float x, float y, float a) { return FMA(x, SUB(1.f, a), MUL(y, a)); }
+
+// running state of one point's map(); colour/id/local only tracked when ATTR
+template <bool ATTR>
+struct MapState {
+    float d;
+    float3 color;
+    int id;
+    float3 local;
+    __device__ __forceinline__ void init() {
+        d = 1e10f;
+        if (ATTR) {
+            color = f3(0.f, 0.f, 0.f);
+            id = -1;
+            local = f3(0.f, 0.f, 0.f);
+        }
+    }
+};
+
+// CSG combine (MarchingCubesKernels.cu:631-694)
+template <bool ATTR>
+__device__ __forceinline__ void combine(MapState<ATTR>& st, int op, float k, const float4* __restrict__ pr, int i,
+                                        float dp, float3 pre) {
+    float3 pc = f3(0.f, 0.f, 0.f);
+    if (ATTR) {
+        const float4 c4 = __ldg(pr + 4);
+        pc = f3(c4.x, c4.y, c4.z);
+    }
+    if (st.d == 1e10f) {
+        st.d = dp;
+        if (ATTR) { st.color = pc; st.id = i; st.local = pre; }
+        return;
+    }
+    float h;
+    switch (op) {
+        case OP_UNION:
+            if (dp < st.d) {
+                st.d = dp;
+                if (ATTR) { st.color = pc; st.id = i; st.local = pre; }
+            }
+            break;
+        case OP_SUB: {
+            const float old = st.d;
+            st.d = fmaxf(st.d, -dp);
+            if (ATTR && st.d > old) { st.color = pc; st.id = i; st.local = pre; }
+        } break;
+        case OP_INT:
+            if (dp > st.d) {
+                st.d = dp;
+                if (ATTR) { st.color = pc; st.id = i; st.local = pre; }
+            }
+            break;
+        case OP_UNION_BLEND:
+            h = CLAMP(ADD(0.5f, DIV(MUL(0.5f, SUB(st.d, dp)), k)), 0.f, 1.f);
+            st.d = FMA(-MUL(k, h), SUB(1.f, h), mixf(st.d, dp, h));
+            if (ATTR) {
+                st.color = f3(mixf(st.color.x, pc.x, h), mixf(st.color.y, pc.y, h), mixf(st.color.z, pc.z, h));
+                if (dp < st.d || h > 0.5f) { st.id = i; st.local = pre; }
+            }
+            break;
+        case OP_SUB_BLEND:
+            h = CLAMP(SUB(0.5f, DIV(MUL(0.5f, ADD(st.d, dp)), k)), 0.f, 1.f);
+            st.d = FMA(MUL(k, h), SUB(1.f, h), mixf(st.d, -dp, h));
+            if (ATTR) {
+                st.color = f3(mixf(st.color.x, pc.x, h), mixf(st.color.y, pc.y, h), mixf(st.color.z, pc.z, h));
+                if (h > 0.5f) { st.id = i; st.local = pre; }
+            }
+            break;
+        case OP_INT_BLEND:
+            h = CLAMP(SUB(0.5f, DIV(MUL(0.5f, SUB(st.d, dp)), k)), 0.f, 1.f);
+            st.d = FMA(MUL(k, h), SUB(1.f, h), mixf(st.d, dp, h));
+            if (ATTR) {
+                st.color = f3(mixf(st.color.x, pc.x, h), mixf(st.color.y, pc.y, h), mixf(st.color.z, pc.z, h));
+                if (dp > st.d || h > 0.5f) { st.id = i; st.local = pre; }
+            }
+            break;
+        default: break;
+    }
+}
+
+// intersectAABB (MarchingCubesKernels.cu:564-568): distance from p to the box, < running d
+__device__ __forceinline__ bool box_closer(float3 p, float4 a, float4 b, float dmin) {
+    const float dx = fmaxf(fmaxf(SUB(a.x, p.x), SUB(p.x, a.w)), 0.f);
+    const float dy = fmaxf(fmaxf(SUB(a.y, p.y), SUB(p.y, b.x)), 0.f);
+    const float dz = fmaxf(fmaxf(SUB(a.z, p.z), SUB(p.z, b.y)), 0.f);
+    return SQRT(FMA(dz, dz, FMA(dx, dx, MUL(dy, dy)))) < dmin;
+}
+
+// Per-launch diagnostics shared by all kernels of an extraction.
+struct Diag {
+    unsigned long long cap_hits;  // points whose search was cut by the 256-pop cap
+    int stack_overflow;           // a search needed more than 64 stack entries
+    int timeout;                  // a bounded wait gave up
+};
+
+// map() for the 32 points of a warp. Must be called by all 32 lanes together (warp-uniform control
+// flow); lanes with valid == false take part in the walk but own no point.
+template <bool ATTR>
+__device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool valid, float time, MapState<ATTR>& st,
+                                         Diag* diag) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    st.init();
+    const unsigned live = __ballot_sync(FULL, valid);
+    int iter = 0;
+    if (sc.nnodes > 0 && live) {
+        // warp stack: entry j lives in lane (j & 31) of register pair A (j < 32) or B (j >= 32)
+        int nodeA = 0, nodeB = 0;
+        unsigned maskA = 0, maskB = 0;
+        int sp = 0;
+        if (lane == 0) { nodeA = 0; maskA = live; }
+        sp = 1;
+        bool overflow = false;
+        while (sp > 0) {
+            --sp;
+            int node;
+            unsigned mask;
+            if (sp < 32) {
+                node = __shfl_sync(FULL, nodeA, sp);
+                mask = __shfl_sync(FULL, maskA, sp);
+            } else {
+                node = __shfl_sync(FULL, nodeB, sp - 32);
+                mask = __shfl_sync(FULL, maskB, sp - 32);
+            }
+            // a lane pops this node iff it pushed it and has popped fewer than MAP_CAP nodes
+            const bool pops = ((mask >> lane) & 1u) && iter < MAP_CAP;
+            if (pops) iter++;
+            // a node can only pass the prune test for a lane whose running distance is > 0
+            const unsigned alive = __ballot_sync(FULL, pops && st.d > 0.f);
+            if (alive == 0) continue;
+            const float4 na = __ldg(sc.nodes + 2 * node);
+            const float4 nb = __ldg(sc.nodes + 2 * node + 1);
+            const bool hit = ((alive >> lane) & 1u) && box_closer(p, na, nb, st.d);
+            const unsigned hm = __ballot_sync(FULL, hit);
+            if (hm == 0) continue;
+            const int left = __float_as_int(nb.z), right = __float_as_int(nb.w);
+            if (right == -1) {
+                const float4* pr = sc.prims + (size_t)left * PRIM_ROWS;
+                const Leaf L = load_leaf(pr);
+                if (hit) {
+                    float3 pre;
+                    const float dp = leaf_distance(L, p, time, pre);
+                    combine<ATTR>(st, L.op, L.pos.w, pr, left, dp, pre);
+                }
+            } else {
+                if (sp + 2 > MAP_STACK) { overflow = true; break; }
+                if (sp < 32) { if (lane == sp) { nodeA = right; maskA = hm; } }
+                else if (lane == sp - 32) { nodeB = right; maskB = hm; }
+                ++sp;
+                if (sp < 32) { if (lane == sp) { nodeA = left; maskA = hm; } }
+                else if (lane == sp - 32) { nodeB = left; maskB = hm; }
+                ++sp;
+            }
+        }
+        if (diag) {
+            const unsigned capped = __ballot_sync(FULL, valid && iter >= MAP_CAP);
+            if (lane == 0 && capped) atomicAdd(&diag->cap_hits, (unsigned long long)__popc(capped));
+            if (lane == 0 && overflow) atomicExch(&diag->stack_overflow, 1);
+        }
+    }
+    // non-union primitives: a linear pass in scene order (:703-803)
+    for (int i = sc.nbvh; i < sc.nprims; ++i) {
+        const float4* pr = sc.prims + (size_t)i * PRIM_ROWS;
+        const Leaf L = load_leaf(pr);
+        if (valid) {
+            float3 pre;
+            const float dp = leaf_distance(L, p, time, pre);
+            combine<ATTR>(st, L.op, L.pos.w, pr, i, dp, pre);
+        }
+    }
+}
+
+// computeNormal (MarchingCubesKernels.cu:814-844) for the 32 points of a warp.
+__device__ __forceinline__ float3 normal_warp(const SceneView& sc, float3 p, bool valid, float time, float cell,
+                                              Diag* diag) {
+    const float h = MUL(cell, 0.001f);
+    MapState<false> s0, sx, sy, sz;
+    map_warp<false>(sc, p, valid, time, s0, diag);
+    map_warp<false>(sc, f3(ADD(p.x, h), p.y, p.z), valid, time, sx, diag);
+    map_warp<false>(sc, f3(p.x, ADD(p.y, h), p.z), valid, time, sy, diag);
+    map_warp<false>(sc, f3(p.x, p.y, ADD(p.z, h)), valid, time, sz, diag);
+    const float3 g = f3(SUB(sx.d, s0.d), SUB(sy.d, s0.d), SUB(sz.d, s0.d));
+    const float len = SQRT(dot3(g, g));
+    if (len > 1e-6f) return f3(DIV(g.x, len), DIV(g.y, len), DIV(g.z, len));
+    return f3(0.f, 1.f, 0.f);
+}
+
+// ------------------------------------------------------------------------------------------------
+// grid geometry (Commons.cuh:190-215) and marching-cubes helpers (MarchingCubesKernels.cu:33-103)
+// ------------------------------------------------------------------------------------------------
+struct GridView {
+    int w, h, d;        // samples per axis
+    int bx, by, bz;     // blocks per axis
+    float ox, oy, oz;   // origin
+    float cell;
+};
+
+__device__ __forceinline__ float3 grid_loc(const GridView& g, int x, int y, int z) {
+    return f3(FMA((float)x, g.cell, g.ox), FMA((float)y, g.cell, g.oy), FMA((float)z, g.cell, g.oz));
+}
+__device__ __forceinline__ float edge_t(float v1, float v2) {
+    const float denom = SUB(v2, v1);
+    float t = 0.5f;
+    if (fabsf(denom) > 1e-12f) t = DIV(SUB(0.f, v1), denom);
+    t = CLAMP(t, 0.f, 1.f);
+    if (t <= 0.f) t = 1e-7f;
+    if (t >= 1.f) t = 1.f - 1e-7f;
+    return t;
+}
+__device__ __forceinline__ float3 lerp3(float3 a, float3 b, float t) {
+    const float u = SUB(1.f, t);
+    return f3(FMA(a.x, u, MUL(b.x, t)), FMA(a.y, u, MUL(b.y, t)), FMA(a.z, u, MUL(b.z, t)));
+}
+__device__ __forceinline__ float len2_3(float3 v) { return FMA(v.z, v.z, FMA(v.x, v.x, MUL(v.y, v.y))); }
+__device__ __forceinline__ bool degenerate(float3 a, float3 b, float3 c, float cell) {
+    if (!finite3(a) || !finite3(b) || !finite3(c)) return true;
+    const float me = DIV(cell, 1024.f), me2 = MUL(me, me);
+    return len2_3(sub3(b, a)) < me2 || len2_3(sub3(c, b)) < me2 || len2_3(sub3(a, c)) < me2;
+}
+
+// corner offsets and edge endpoints (MarchingCubesTables.cuh:8-17), as bit-packed constants:
+// corner c has offset (x, y, z) = bits (c*3, c*3+1, c*3+2) of kCornerBits
+constexpr uint32_t kCornerBits = (0u << 0) | (1u << 3) | (3u << 6) | (2u << 9) | (4u << 12) | (5u << 15) |
+                                 (7u << 18) | (6u << 21);
+__device__ __forceinline__ int corner_dx(int c) { return (kCornerBits >> (3 * c)) & 1; }
+__device__ __forceinline__ int corner_dy(int c) { return (kCornerBits >> (3 * c + 1)) & 1; }
+__device__ __forceinline__ int corner_dz(int c) { return (kCornerBits >> (3 * c + 2)) & 1; }
+// edge e joins corners (c0, c1): nibble e of kEdgeC0 / kEdgeC1
+constexpr uint64_t kEdgeC0 = 0x321076543210ull;
+constexpr uint64_t kEdgeC1 = 0x765447650321ull;
+__device__ __forceinline__ int edge_c0(int e) { return (int)((kEdgeC0 >> (4 * e)) & 0xF); }
+__device__ __forceinline__ int edge_c1(int e) { return (int)((kEdgeC1 >> (4 * e)) & 0xF); }
+
+}  // namespace sdfb

@@ -1,0 +1,258 @@
+/* sdfmesh_b200: B200-native (sm_100a) SDF -> mesh engine, C ABI.
+ *
+ * Drop-in boundary. The library exports, under the same unmangled names, the twelve extern "C"
+ * entry points of the reference's src/SDFMesh/Wrappers.cu:19-136 (declared by the reference's
+ * caller at CudaSDFMesh.cpp:15-29). The reference passes `SDFGrid&`; a C++ reference is a pointer at
+ * the ABI level, so they are declared here as `sdf_grid*`. A project that links this library in
+ * place of MarchingCubesKernels.cu + Wrappers.cu keeps its own CudaSDFMesh.cpp unchanged.
+ *
+ * The data types below are byte-identical to the reference's SDFPrimitive, BVHNode and SDFGrid
+ * (Commons.cuh:68-186); their sizes and field offsets are pinned by static assertions.
+ *
+ * Beside the drop-in launchers, the library has its own entry points (sdf_engine_*, sdf_extract):
+ * status codes, an explicit stream, no host synchronisation inside except the final count
+ * read-back, and a fused pipeline (scout -> block field -> count -> scan -> emit).
+ */
+#ifndef SDFMESH_B200_H
+#define SDFMESH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#define SDF_ALIGN16 alignas(16)
+#else
+#define SDF_ALIGN16 _Alignas(16)
+#endif
+
+/* ------------------------------------------------------------------------------------------------
+ * Data layout (Commons.cuh)
+ * ---------------------------------------------------------------------------------------------- */
+typedef struct sdf_float2 { float x, y; } sdf_float2;
+typedef struct SDF_ALIGN16 sdf_float4 { float x, y, z, w; } sdf_float4;
+typedef struct sdf_ushort4 { uint16_t x, y, z, w; } sdf_ushort4;
+typedef struct sdf_short4 { int16_t x, y, z, w; } sdf_short4;
+
+/* PrimitiveType (Commons.cuh:17-34) */
+enum {
+    SDF_SPHERE = 0, SDF_BOX, SDF_TORUS, SDF_CYLINDER, SDF_CAPSULE, SDF_CONE, SDF_ROUNDED_BOX,
+    SDF_ROUNDED_CYLINDER, SDF_ROUNDED_CONE, SDF_ELLIPSOID, SDF_TRIANGULAR_PRISM, SDF_OCTOHEDRON,
+    SDF_HEX_PRISM, SDF_SOLID_ANGLE, SDF_CUSTOM_FLOAT, SDF_CUSTOM_VECTOR
+};
+/* OperationType (Commons.cuh:37-44) */
+enum { SDF_UNION = 0, SDF_SUBTRACT, SDF_INTERSECT, SDF_UNION_BLEND, SDF_SUBTRACT_BLEND, SDF_INTERSECT_BLEND };
+/* DisplacementType (Commons.cuh:47-57); SINE, TWIST and BEND are the ones map() applies */
+enum { DISP_NONE = 0, DISP_SINE, DISP_TWIST, DISP_BEND, DISP_ELONGATE, DISP_ROUND, DISP_ONION, DISP_EXTRUSION,
+       DISP_REVOLUTION };
+
+/* SDFPrimitive (Commons.cuh:68-102): 160 bytes */
+typedef struct SDF_ALIGN16 sdf_primitive {
+    float rotation[4];   /* quaternion x, y, z, w */
+    float dispParams[4];
+    float position[3];
+    float blendFactor;   /* smooth-blend k */
+    float scale[3];
+    float rounding;
+    float color[3];
+    float annular;
+    float params[6];
+    int32_t type;
+    int32_t operation;
+    int32_t displacement;
+    int32_t _pad1;
+    float uvScale[2];
+    float uvOffset[2];
+    float uvRotation;
+    int32_t uvMode;
+    int32_t textureID;
+    int32_t atlasIslandID;
+    float _pad2[2];
+} sdf_primitive;
+
+/* BVHNode (Commons.cuh:104-109): leaf iff right == -1, then left = primitive index */
+typedef struct sdf_bvh_node {
+    float min[3];
+    float max[3];
+    int32_t left;
+    int32_t right;
+} sdf_bvh_node;
+
+#define SDF_BLOCK_SIZE 8
+#define SDF_BLOCK_SIZE_CUBED 512
+
+/* SDFGrid (Commons.cuh:115-186): 232 bytes, passed by reference to every launcher */
+typedef struct sdf_grid {
+    int32_t* d_activeBlocks;
+    int32_t* d_activeBlockCount;
+    int32_t maxBlocks;
+    int32_t blocksDim[3];
+    uint32_t width, height, depth; /* samples per axis */
+    float origin[3];
+    float cellSize;
+    sdf_primitive* d_primitives;
+    uint32_t numPrimitives;
+    uint32_t numBVHPrimitives;
+    sdf_bvh_node* d_bvhNodes;
+    uint32_t numBVHNodes;
+    uint32_t* d_packetVertexCounts;
+    uint32_t* d_packetVertexOffsets;
+    int32_t* d_blockToActiveId;
+    uint8_t* d_dcCornerMasks;
+    uint32_t* d_dcCellVertexOffsets;
+    sdf_ushort4* d_dcCellVertices;
+    sdf_short4* d_dcCellNormals;
+    sdf_short4* d_dcCellNormalsTmp;
+    sdf_float4* d_vertices;
+    sdf_float4* d_vertexColors;
+    uint32_t* d_indices;
+    sdf_float2* d_uvCoords;
+    int32_t* d_primitiveIDs;  /* holds float bits of the primitive index (MarchingCubesKernels.cu:1093) */
+    sdf_float4* d_normals;
+    uint32_t maxVertices;
+    uint32_t maxIndices;
+    uint32_t* d_totalVertices;
+    uint32_t* d_totalIndices;
+} sdf_grid;
+
+#ifdef __cplusplus
+static_assert(sizeof(sdf_primitive) == 160, "SDFPrimitive layout");
+static_assert(offsetof(sdf_primitive, position) == 32 && offsetof(sdf_primitive, params) == 80 &&
+              offsetof(sdf_primitive, type) == 104 && offsetof(sdf_primitive, uvScale) == 120 &&
+              offsetof(sdf_primitive, atlasIslandID) == 148, "SDFPrimitive offsets");
+static_assert(sizeof(sdf_bvh_node) == 32, "BVHNode layout");
+static_assert(sizeof(sdf_grid) == 232, "SDFGrid layout");
+static_assert(offsetof(sdf_grid, cellSize) == 56 && offsetof(sdf_grid, d_primitives) == 64 &&
+              offsetof(sdf_grid, d_packetVertexCounts) == 96 && offsetof(sdf_grid, d_vertices) == 160 &&
+              offsetof(sdf_grid, maxVertices) == 208 && offsetof(sdf_grid, d_totalIndices) == 224,
+              "SDFGrid offsets");
+#else
+_Static_assert(sizeof(sdf_primitive) == 160, "SDFPrimitive layout");
+_Static_assert(sizeof(sdf_bvh_node) == 32, "BVHNode layout");
+_Static_assert(sizeof(sdf_grid) == 232, "SDFGrid layout");
+#endif
+
+/* ------------------------------------------------------------------------------------------------
+ * Drop-in launchers: the reference's Wrappers.cu entry points. Same names, argument meaning and
+ * stream (the legacy default stream). Each checks its launch and records the first CUDA error,
+ * readable with sdf_last_error(); the reference only printf()s and carries on (Wrappers.cu:26-29).
+ * Define SDFMESH_B200_NO_LAUNCHER_DECLS when the reference's own `SDFGrid&` declarations are in
+ * scope in the same C++ translation unit.
+ * ---------------------------------------------------------------------------------------------- */
+#ifndef SDFMESH_B200_NO_LAUNCHER_DECLS
+/* Wrappers.cu:19-28  scoutActiveBlocks: active-block list (ascending block index) + count */
+void launchScoutActiveBlocks(sdf_grid* grid, float time);
+/* Wrappers.cu:30-38  countActiveBlockTriangles: per-cell vertex counts (3 x non-degenerate tris) */
+void launchCountActiveBlockTriangles(sdf_grid* grid, int numActiveBlocks, float time);
+/* Wrappers.cu:40-48  generateActiveBlockTriangles: triangle-soup emission at the scanned offsets */
+void launchGenerateActiveBlockTriangles(sdf_grid* grid, int numActiveBlocks, float time);
+/* Wrappers.cu:54-63  buildBlockToActiveMap: dense block -> active-id map (host memsets it to -1) */
+void launchBuildBlockToActiveMap(sdf_grid* grid, int numActiveBlocks);
+/* Wrappers.cu:65-73  dcMarkCells: 8-bit corner masks + has-vertex counts */
+void launchDCMarkCells(sdf_grid* grid, int numActiveBlocks, float time);
+/* Wrappers.cu:75-83  dcSolveCellVertices: Hermite data, QEF, quantised vertex + normal */
+void launchDCSolveCellVertices(sdf_grid* grid, int numActiveBlocks, float time, unsigned int maxCellVertices,
+                               float qefBlend);
+/* Wrappers.cu:85-93  dcRecomputeNormalsAtVertices: SDF gradient at the solved vertices */
+void launchDCRecomputeNormalsAtVertices(sdf_grid* grid, int numActiveBlocks, float time);
+/* Wrappers.cu:95-103 dcSmoothCellNormals: angle-gated 6-neighbour normal smoothing */
+void launchDCSmoothCellNormals(sdf_grid* grid, int numActiveBlocks, float cosAngleThreshold);
+/* Wrappers.cu:105-113 dcCountQuads: 6 vertices per owned sign-changing edge */
+void launchDCCountQuads(sdf_grid* grid, int numActiveBlocks);
+/* Wrappers.cu:115-123 dcGenerateQuads: two triangles per quad, soup layout */
+void launchDCGenerateQuads(sdf_grid* grid, int numActiveBlocks, float time);
+/* Wrappers.cu:125-130 getScanStorageSize: temp bytes for launchScan over num_items */
+void getScanStorageSize(unsigned int num_items, size_t* temp_storage_bytes);
+/* Wrappers.cu:132-136 launchScan: exclusive prefix sum of uint32 (the reference calls
+ * cub::DeviceScan::ExclusiveSum; this one is a single-pass decoupled look-back scan) */
+void launchScan(unsigned int* d_input, unsigned int* d_output, unsigned int numItems, void* d_temp_storage,
+                size_t temp_storage_bytes);
+#endif
+
+/* ------------------------------------------------------------------------------------------------
+ * Engine API (no reference counterpart; additive)
+ * ---------------------------------------------------------------------------------------------- */
+typedef enum sdf_status {
+    SDF_OK = 0,
+    SDF_ERR_INVALID = 1,   /* bad argument */
+    SDF_ERR_CUDA = 2,      /* a CUDA call failed; sdf_last_error() has the cudaError_t */
+    SDF_ERR_CAPACITY = 3,  /* output larger than the caller's buffers; counts are still exact */
+    SDF_ERR_STACK = 4,     /* BVH deeper than the 64-entry traversal stack */
+    SDF_ERR_NOMEM = 5,     /* device allocation failed */
+    SDF_ERR_TIMEOUT = 6    /* a bounded device-side wait gave up */
+} sdf_status;
+
+/* output stream mask */
+enum { SDF_OUT_COLORS = 1, SDF_OUT_INDICES = 2, SDF_OUT_UVS = 4, SDF_OUT_PRIMIDS = 8, SDF_OUT_NORMALS = 16 };
+enum { SDF_TECH_MARCHING_CUBES = 0, SDF_TECH_DUAL_CONTOURING = 1 };
+/* DC vertex solver: the reference's feature-clustering + regularised QEF, or the mass-point QEF */
+enum { SDF_DC_SOLVER_REFERENCE = 0, SDF_DC_SOLVER_MASSPOINT = 1 };
+
+typedef struct sdf_config {
+    float cell_size;
+    float bounds_min[3];
+    float bounds_max[3];
+    int32_t technique;          /* SDF_TECH_* */
+    float qef_blend;            /* 0 = cell centre, 1 = full QEF solve */
+    int32_t dc_solver;          /* SDF_DC_SOLVER_* */
+    int32_t projection_iters;   /* mass-point solver: vertex projection iterations (0 = off) */
+    int32_t adaptive_diagonal;  /* mass-point solver: split quads along the shorter diagonal */
+    float cond_threshold;       /* mass-point solver: FP64 eigensolve above this condition number */
+    uint32_t out_mask;          /* SDF_OUT_* streams to write (positions are always written) */
+} sdf_config;
+
+typedef struct sdf_outputs {
+    sdf_float4* vertices;       /* device, capacity max_vertices */
+    sdf_float4* colors;         /* optional (SDF_OUT_COLORS) */
+    uint32_t* indices;          /* optional (SDF_OUT_INDICES): identity triangle-soup indices */
+    sdf_float2* uvs;            /* optional (SDF_OUT_UVS) */
+    int32_t* primitive_ids;     /* optional (SDF_OUT_PRIMIDS), float bits as in the reference */
+    sdf_float4* normals;        /* optional (SDF_OUT_NORMALS) */
+    uint32_t max_vertices;
+} sdf_outputs;
+
+typedef struct sdf_stats {
+    int64_t total_blocks;
+    int64_t active_blocks;
+    int64_t total_vertices;     /* exact, even when larger than max_vertices */
+    int64_t written_vertices;
+    int64_t dc_cell_vertices;
+    int64_t bvh_cap_hits;       /* points whose traversal stopped at the 256-visit cap */
+    float ms_scout, ms_field, ms_scan, ms_emit, ms_total; /* filled when timing is enabled */
+} sdf_stats;
+
+typedef struct sdf_engine sdf_engine;
+
+/* Creates an engine on `device` (the current device if < 0). */
+sdf_status sdf_engine_create(sdf_engine** out, int device);
+void sdf_engine_destroy(sdf_engine* e);
+/* Grid as CudaSDFMesh::Initialize (CudaSDFMesh.cpp:90-206). */
+sdf_status sdf_engine_configure(sdf_engine* e, const sdf_config* cfg);
+/* Scene as CudaSDFMesh::UpdateBVH (CudaSDFMesh.cpp:216-249): unions first, BVH over the unions, built
+ * on the host with the reference's node order, then uploaded in the engine's compact device layout. */
+sdf_status sdf_engine_set_scene(sdf_engine* e, const sdf_primitive* prims, int count);
+/* One extraction on `stream` (a cudaStream_t, NULL = legacy default stream). The only host
+ * synchronisation is the final count read-back into *stats. */
+sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out, void* stream, sdf_stats* stats);
+/* Enables per-stage CUDA-event timing inside sdf_engine_extract (adds host syncs). */
+void sdf_engine_set_timing(sdf_engine* e, int enabled);
+/* The scene as uploaded: sorted primitives (count = numPrimitives) and BVH nodes. */
+int sdf_engine_get_bvh(sdf_engine* e, sdf_bvh_node* nodes_out, int capacity, int* num_bvh_primitives);
+/* Device pointer to the last extraction's internal arrays, for inspection: 0 active block list,
+ * 1 per-cell vertex counts (compat layout), 2 per-cell offsets, 3 DC corner masks, 4 DC cell vertex
+ * offsets, 5 DC cell vertices, 6 DC cell normals, 7 per-block vertex totals. */
+const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes);
+
+/* One-shot convenience: create, configure, set scene, extract, destroy. */
+sdf_status sdf_extract(const sdf_primitive* prims, int count, const sdf_config* cfg, float time,
+                       const sdf_outputs* out, void* stream, sdf_stats* stats);
+
+/* First CUDA error recorded by a drop-in launcher since the last call (cleared on read). */
+int sdf_last_error(void);
+/* Library version string. */
+const char* sdf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SDFMESH_B200_H */
