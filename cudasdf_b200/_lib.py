@@ -1,0 +1,133 @@
+"""ctypes binding of libsdfmesh_b200.so (include/sdfmesh_b200.h).
+
+The library is built in-tree by ``build.py`` (or ``__graft_entry__.build()``). Importing this module
+does not load it; ``lib()`` does, and raises if it is missing: there is no fallback path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsdfmesh_b200.so")
+
+SDF_OK, SDF_ERR_INVALID, SDF_ERR_CUDA, SDF_ERR_CAPACITY, SDF_ERR_STACK, SDF_ERR_NOMEM, SDF_ERR_TIMEOUT = range(7)
+STATUS_NAMES = {0: "SDF_OK", 1: "SDF_ERR_INVALID", 2: "SDF_ERR_CUDA", 3: "SDF_ERR_CAPACITY", 4: "SDF_ERR_STACK",
+                5: "SDF_ERR_NOMEM", 6: "SDF_ERR_TIMEOUT"}
+OUT_COLORS, OUT_INDICES, OUT_UVS, OUT_PRIMIDS, OUT_NORMALS = 1, 2, 4, 8, 16
+TECH_MC, TECH_DC = 0, 1
+DC_SOLVER_REFERENCE, DC_SOLVER_MASSPOINT = 0, 1
+
+
+class SdfConfig(ctypes.Structure):
+    _fields_ = [("cell_size", ctypes.c_float), ("bounds_min", ctypes.c_float * 3), ("bounds_max", ctypes.c_float * 3),
+                ("technique", ctypes.c_int32), ("qef_blend", ctypes.c_float), ("dc_solver", ctypes.c_int32),
+                ("projection_iters", ctypes.c_int32), ("adaptive_diagonal", ctypes.c_int32),
+                ("cond_threshold", ctypes.c_float), ("out_mask", ctypes.c_uint32)]
+
+
+class SdfOutputs(ctypes.Structure):
+    _fields_ = [("vertices", ctypes.c_void_p), ("colors", ctypes.c_void_p), ("indices", ctypes.c_void_p),
+                ("uvs", ctypes.c_void_p), ("primitive_ids", ctypes.c_void_p), ("normals", ctypes.c_void_p),
+                ("max_vertices", ctypes.c_uint32)]
+
+
+class SdfStats(ctypes.Structure):
+    _fields_ = [("total_blocks", ctypes.c_int64), ("active_blocks", ctypes.c_int64),
+                ("total_vertices", ctypes.c_int64), ("written_vertices", ctypes.c_int64),
+                ("dc_cell_vertices", ctypes.c_int64), ("bvh_cap_hits", ctypes.c_int64),
+                ("ms_scout", ctypes.c_float), ("ms_field", ctypes.c_float), ("ms_scan", ctypes.c_float),
+                ("ms_emit", ctypes.c_float), ("ms_total", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class SdfGrid(ctypes.Structure):
+    """The reference's SDFGrid (Commons.cuh:115-186), 232 bytes."""
+    _fields_ = [("d_activeBlocks", ctypes.c_void_p), ("d_activeBlockCount", ctypes.c_void_p),
+                ("maxBlocks", ctypes.c_int32), ("blocksDim", ctypes.c_int32 * 3),
+                ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("depth", ctypes.c_uint32),
+                ("origin", ctypes.c_float * 3), ("cellSize", ctypes.c_float),
+                ("d_primitives", ctypes.c_void_p), ("numPrimitives", ctypes.c_uint32),
+                ("numBVHPrimitives", ctypes.c_uint32), ("d_bvhNodes", ctypes.c_void_p),
+                ("numBVHNodes", ctypes.c_uint32), ("d_packetVertexCounts", ctypes.c_void_p),
+                ("d_packetVertexOffsets", ctypes.c_void_p), ("d_blockToActiveId", ctypes.c_void_p),
+                ("d_dcCornerMasks", ctypes.c_void_p), ("d_dcCellVertexOffsets", ctypes.c_void_p),
+                ("d_dcCellVertices", ctypes.c_void_p), ("d_dcCellNormals", ctypes.c_void_p),
+                ("d_dcCellNormalsTmp", ctypes.c_void_p), ("d_vertices", ctypes.c_void_p),
+                ("d_vertexColors", ctypes.c_void_p), ("d_indices", ctypes.c_void_p),
+                ("d_uvCoords", ctypes.c_void_p), ("d_primitiveIDs", ctypes.c_void_p),
+                ("d_normals", ctypes.c_void_p), ("maxVertices", ctypes.c_uint32), ("maxIndices", ctypes.c_uint32),
+                ("d_totalVertices", ctypes.c_void_p), ("d_totalIndices", ctypes.c_void_p)]
+
+
+assert ctypes.sizeof(SdfGrid) == 232
+
+# every symbol include/sdfmesh_b200.h declares
+DROPIN_SYMBOLS = ["launchScoutActiveBlocks", "launchCountActiveBlockTriangles", "launchGenerateActiveBlockTriangles",
+                  "launchBuildBlockToActiveMap", "launchDCMarkCells", "launchDCSolveCellVertices",
+                  "launchDCRecomputeNormalsAtVertices", "launchDCSmoothCellNormals", "launchDCCountQuads",
+                  "launchDCGenerateQuads", "getScanStorageSize", "launchScan"]
+ENGINE_SYMBOLS = ["sdf_engine_create", "sdf_engine_destroy", "sdf_engine_configure", "sdf_engine_set_scene",
+                  "sdf_engine_extract", "sdf_engine_set_timing", "sdf_engine_set_debug", "sdf_engine_get_bvh",
+                  "sdf_engine_buffer", "sdf_engine_read_buffer", "sdf_extract", "sdf_last_error", "sdf_version"]
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is not built; run `python -m cudasdf_b200.build` first")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i, f, u, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_uint, ctypes.c_size_t
+    G = ctypes.POINTER(SdfGrid)
+    L.launchScoutActiveBlocks.argtypes = [G, f]
+    L.launchCountActiveBlockTriangles.argtypes = [G, i, f]
+    L.launchGenerateActiveBlockTriangles.argtypes = [G, i, f]
+    L.launchBuildBlockToActiveMap.argtypes = [G, i]
+    L.launchDCMarkCells.argtypes = [G, i, f]
+    L.launchDCSolveCellVertices.argtypes = [G, i, f, u, f]
+    L.launchDCRecomputeNormalsAtVertices.argtypes = [G, i, f]
+    L.launchDCSmoothCellNormals.argtypes = [G, i, f]
+    L.launchDCCountQuads.argtypes = [G, i]
+    L.launchDCGenerateQuads.argtypes = [G, i, f]
+    L.getScanStorageSize.argtypes = [u, ctypes.POINTER(sz)]
+    L.launchScan.argtypes = [vp, vp, u, vp, sz]
+    for name in DROPIN_SYMBOLS:
+        getattr(L, name).restype = None
+    L.sdf_engine_create.argtypes = [ctypes.POINTER(vp), i]
+    L.sdf_engine_create.restype = i
+    L.sdf_engine_destroy.argtypes = [vp]
+    L.sdf_engine_destroy.restype = None
+    L.sdf_engine_configure.argtypes = [vp, ctypes.POINTER(SdfConfig)]
+    L.sdf_engine_configure.restype = i
+    L.sdf_engine_set_scene.argtypes = [vp, vp, i]
+    L.sdf_engine_set_scene.restype = i
+    L.sdf_engine_extract.argtypes = [vp, f, ctypes.POINTER(SdfOutputs), vp, ctypes.POINTER(SdfStats)]
+    L.sdf_engine_extract.restype = i
+    L.sdf_engine_set_timing.argtypes = [vp, i]
+    L.sdf_engine_set_timing.restype = None
+    L.sdf_engine_set_debug.argtypes = [vp, i]
+    L.sdf_engine_set_debug.restype = None
+    L.sdf_engine_get_bvh.argtypes = [vp, vp, i, ctypes.POINTER(i)]
+    L.sdf_engine_get_bvh.restype = i
+    L.sdf_engine_buffer.argtypes = [vp, i, ctypes.POINTER(sz)]
+    L.sdf_engine_buffer.restype = vp
+    L.sdf_engine_read_buffer.argtypes = [vp, i, vp, sz]
+    L.sdf_engine_read_buffer.restype = i
+    L.sdf_extract.argtypes = [vp, i, ctypes.POINTER(SdfConfig), f, ctypes.POINTER(SdfOutputs), vp,
+                              ctypes.POINTER(SdfStats)]
+    L.sdf_extract.restype = i
+    L.sdf_last_error.restype = i
+    L.sdf_version.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def check(status: int, what: str = "") -> None:
+    if status != SDF_OK:
+        raise RuntimeError(f"{what}: {STATUS_NAMES.get(status, status)} (cuda error {lib().sdf_last_error()})")

@@ -1,0 +1,418 @@
+// sdf_engine: the fused extraction pipeline (included at the end of sdfmesh.cu).
+//
+// Marching cubes:   scout -> compact -> block field (+ per-block vertex totals) -> scan of the block
+//                   totals -> emission from the stored fields
+// Dual contouring:  scout -> compact -> block map -> mark (+ stored fields) -> scan of has-vertex ->
+//                   solve -> count quads (+ block totals) -> scan of block totals -> quads
+// All stages run back to back on one stream; the active count stays on the device (persistent CTAs
+// read it), so the only host synchronisation is the final read-back of the counts.
+#include <chrono>
+
+namespace sdfb {
+
+// control block on the device, zeroed by one memset per extraction
+struct Ctrl {
+    int active_count;
+    unsigned tickets[12];
+    unsigned total_vertices;
+    unsigned dc_vertices;
+    unsigned pad;
+    Diag diag;
+};
+
+struct EngineImpl {
+    int device = 0;
+    sdf_config cfg;
+    bool configured = false;
+    GridView gv;
+    int nblocks = 0;
+    // scene
+    std::vector<sdf_primitive> sorted;
+    std::vector<sdf_bvh_node> nodes;
+    int nbvh = 0;
+    int depth = 0;
+    sdf_primitive* d_prims = nullptr;
+    size_t prims_cap = 0;
+    sdf_bvh_node* d_nodes = nullptr;
+    size_t nodes_cap = 0;
+    // pipeline
+    unsigned* flags = nullptr;
+    int* list = nullptr;
+    float* fields = nullptr;
+    unsigned* block_totals = nullptr;
+    unsigned* block_offsets = nullptr;
+    unsigned* packet_counts = nullptr;   // per cell: MC debug output / DC has-vertex + quad counts
+    unsigned* packet_offsets = nullptr;  // per cell: MC debug output
+    int* b2a = nullptr;
+    unsigned char* masks = nullptr;
+    unsigned* dc_voff = nullptr;
+    ushort4* dc_verts = nullptr;
+    short4* dc_norms = nullptr;
+    size_t dc_cap = 0;
+    unsigned char* ctrl_region = nullptr;  // Ctrl, then the three scan regions
+    size_t ctrl_bytes = 0;
+    size_t scanA_off = 0, scanB_off = 0, scanC_off = 0;
+    Ctrl* h_ctrl = nullptr;                // pinned read-back
+    bool timing = false;
+    int debug = 0;
+    cudaEvent_t ev[8] = {};
+    size_t packet_cap = 0;
+
+    ~EngineImpl() { release(); }
+
+    void release() {
+        void* ptrs[] = {d_prims, d_nodes, flags, list, fields, block_totals, block_offsets, packet_counts,
+                        packet_offsets, b2a, masks, dc_voff, dc_verts, dc_norms, ctrl_region};
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+        d_prims = nullptr; d_nodes = nullptr; flags = nullptr; list = nullptr; fields = nullptr;
+        block_totals = nullptr; block_offsets = nullptr; packet_counts = nullptr; packet_offsets = nullptr;
+        b2a = nullptr; masks = nullptr; dc_voff = nullptr; dc_verts = nullptr; dc_norms = nullptr;
+        ctrl_region = nullptr;
+        prims_cap = nodes_cap = dc_cap = packet_cap = 0;
+        if (h_ctrl) cudaFreeHost(h_ctrl);
+        h_ctrl = nullptr;
+        for (auto& e : ev)
+            if (e) { cudaEventDestroy(e); e = nullptr; }
+    }
+};
+
+template <class T>
+static sdf_status dev_alloc(T*& p, size_t count) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    if (count == 0) count = 1;
+    if (cudaMalloc((void**)&p, count * sizeof(T)) != cudaSuccess) {
+        cudaGetLastError();
+        p = nullptr;
+        return SDF_ERR_NOMEM;
+    }
+    return SDF_OK;
+}
+
+}  // namespace sdfb
+
+struct sdf_engine {
+    sdfb::EngineImpl impl;
+};
+
+using sdfb::EngineImpl;
+
+static sdf_status engine_ensure_packets(EngineImpl& E, size_t cells) {
+    if (E.packet_cap >= cells) return SDF_OK;
+    sdf_status s = sdfb::dev_alloc(E.packet_counts, cells);
+    if (s == SDF_OK) s = sdfb::dev_alloc(E.packet_offsets, cells);
+    if (s == SDF_OK) s = sdfb::dev_alloc(E.masks, cells);
+    if (s == SDF_OK) s = sdfb::dev_alloc(E.dc_voff, cells);
+    E.packet_cap = s == SDF_OK ? cells : 0;
+    return s;
+}
+
+extern "C" {
+
+sdf_status sdf_engine_create(sdf_engine** out, int device) {
+    if (!out) return SDF_ERR_INVALID;
+    *out = nullptr;
+    if (device >= 0 && cudaSetDevice(device) != cudaSuccess) return SDF_ERR_CUDA;
+    sdf_engine* e = new sdf_engine();
+    cudaGetDevice(&e->impl.device);
+    if (cudaMallocHost(&e->impl.h_ctrl, sizeof(sdfb::Ctrl)) != cudaSuccess) {
+        delete e;
+        return SDF_ERR_NOMEM;
+    }
+    for (auto& ev : e->impl.ev) cudaEventCreate(&ev);
+    *out = e;
+    return SDF_OK;
+}
+
+void sdf_engine_destroy(sdf_engine* e) {
+    if (!e) return;
+    cudaSetDevice(e->impl.device);
+    delete e;
+}
+
+void sdf_engine_set_timing(sdf_engine* e, int enabled) {
+    if (e) e->impl.timing = enabled != 0;
+}
+
+// debug bit 0: also write the per-cell counts/offsets of the drop-in layout (marching cubes)
+void sdf_engine_set_debug(sdf_engine* e, int flags) {
+    if (e) e->impl.debug = flags;
+}
+
+sdf_status sdf_engine_configure(sdf_engine* e, const sdf_config* cfg) {
+    if (!e || !cfg) return SDF_ERR_INVALID;
+    EngineImpl& E = e->impl;
+    cudaSetDevice(E.device);
+    if (!(cfg->cell_size > 0.f)) return SDF_ERR_INVALID;
+    float size[3];
+    for (int k = 0; k < 3; ++k) {
+        size[k] = cfg->bounds_max[k] - cfg->bounds_min[k];
+        if (!(size[k] > 0.f)) return SDF_ERR_INVALID;
+    }
+    // CudaSDFMesh::Initialize (CudaSDFMesh.cpp:107-129): samples per axis and blocks per axis
+    const unsigned w = (unsigned)ceilf(size[0] / cfg->cell_size);
+    const unsigned h = (unsigned)ceilf(size[1] / cfg->cell_size);
+    const unsigned d = (unsigned)ceilf(size[2] / cfg->cell_size);
+    if ((unsigned long long)w * h * d > 8589934592ULL) return SDF_ERR_INVALID;
+    sdfb::GridView gv;
+    gv.w = (int)w; gv.h = (int)h; gv.d = (int)d;
+    gv.bx = (int)((w + 7) / 8); gv.by = (int)((h + 7) / 8); gv.bz = (int)((d + 7) / 8);
+    gv.ox = cfg->bounds_min[0]; gv.oy = cfg->bounds_min[1]; gv.oz = cfg->bounds_min[2];
+    gv.cell = cfg->cell_size;
+    const long long nb = (long long)gv.bx * gv.by * gv.bz;
+    if (nb * 512 >= (1LL << 32)) return SDF_ERR_INVALID;  // packed cell indices are 32-bit
+    const bool same_grid = E.configured && E.nblocks == (int)nb;
+    E.cfg = *cfg;
+    E.gv = gv;
+    E.configured = true;
+    if (same_grid) return SDF_OK;
+    E.nblocks = (int)nb;
+    sdf_status s = SDF_OK;
+    if (s == SDF_OK) s = sdfb::dev_alloc(E.flags, nb);
+    if (s == SDF_OK) s = sdfb::dev_alloc(E.list, nb);
+    if (s == SDF_OK) s = sdfb::dev_alloc(E.block_totals, nb);
+    if (s == SDF_OK) s = sdfb::dev_alloc(E.block_offsets, nb);
+    if (s == SDF_OK) s = sdfb::dev_alloc(E.b2a, nb);
+    if (s == SDF_OK) s = sdfb::dev_alloc(E.fields, (size_t)nb * sdfb::FIELD_STRIDE);
+    if (s != SDF_OK) return s;
+    // control block + scan regions (word 0 of a region is its ticket)
+    const size_t tA = sdfb::scan_tiles((unsigned)nb) + 1;
+    const size_t tC = sdfb::scan_tiles((unsigned)(nb * 512)) + 1;
+    E.scanA_off = (sizeof(sdfb::Ctrl) + 255) & ~size_t(255);
+    E.scanB_off = E.scanA_off + tA * 8;
+    E.scanC_off = E.scanB_off + tA * 8;
+    E.ctrl_bytes = E.scanC_off + tC * 8;
+    s = sdfb::dev_alloc(E.ctrl_region, E.ctrl_bytes);
+    // per-cell buffers are allocated on first use
+    E.packet_cap = 0;
+    return s;
+}
+
+sdf_status sdf_engine_set_scene(sdf_engine* e, const sdf_primitive* prims, int count) {
+    if (!e || count < 0 || (count > 0 && !prims)) return SDF_ERR_INVALID;
+    EngineImpl& E = e->impl;
+    cudaSetDevice(E.device);
+    E.nbvh = sdfb::prepare_scene(prims, count, E.sorted, E.nodes);
+    E.depth = sdfb::bvh_depth(E.nodes);
+    if (E.depth + 1 > sdfb::MAP_STACK) return SDF_ERR_STACK;
+    if (E.prims_cap < E.sorted.size()) {
+        if (sdfb::dev_alloc(E.d_prims, E.sorted.size() * 2) != SDF_OK) return SDF_ERR_NOMEM;
+        E.prims_cap = E.sorted.size() * 2;
+    }
+    if (E.nodes_cap < E.nodes.size()) {
+        if (sdfb::dev_alloc(E.d_nodes, E.nodes.size() * 2) != SDF_OK) return SDF_ERR_NOMEM;
+        E.nodes_cap = E.nodes.size() * 2;
+    }
+    if (!E.sorted.empty() &&
+        cudaMemcpy(E.d_prims, E.sorted.data(), E.sorted.size() * sizeof(sdf_primitive), cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+        return SDF_ERR_CUDA;
+    if (!E.nodes.empty() &&
+        cudaMemcpy(E.d_nodes, E.nodes.data(), E.nodes.size() * sizeof(sdf_bvh_node), cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+        return SDF_ERR_CUDA;
+    return SDF_OK;
+}
+
+int sdf_engine_get_bvh(sdf_engine* e, sdf_bvh_node* nodes_out, int capacity, int* num_bvh_primitives) {
+    if (!e) return -1;
+    EngineImpl& E = e->impl;
+    if (num_bvh_primitives) *num_bvh_primitives = E.nbvh;
+    if (nodes_out)
+        for (int i = 0; i < (int)E.nodes.size() && i < capacity; ++i) nodes_out[i] = E.nodes[i];
+    return (int)E.nodes.size();
+}
+
+sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out, void* stream_ptr, sdf_stats* stats) {
+    using namespace sdfb;
+    if (!e || !out || !out->vertices) return SDF_ERR_INVALID;
+    EngineImpl& E = e->impl;
+    if (!E.configured) return SDF_ERR_INVALID;
+    cudaSetDevice(E.device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream_ptr);
+    const sdf_config& C = E.cfg;
+    const bool dc = C.technique == SDF_TECH_DUAL_CONTOURING;
+    if (dc || (E.debug & 1)) {
+        const sdf_status s = engine_ensure_packets(E, (size_t)E.nblocks * 512);
+        if (s != SDF_OK) return s;
+    }
+    if (dc) {
+        const size_t want = std::min<size_t>((size_t)E.nblocks * 512, (size_t)1 << 28);
+        if (E.dc_cap < want) {
+            if (dev_alloc(E.dc_verts, want) != SDF_OK || dev_alloc(E.dc_norms, want) != SDF_OK) return SDF_ERR_NOMEM;
+            E.dc_cap = want;
+        }
+    }
+    cudaGetLastError();
+    auto t0 = std::chrono::high_resolution_clock::now();
+    Ctrl* ctrl = reinterpret_cast<Ctrl*>(E.ctrl_region);
+    unsigned long long* scanA = reinterpret_cast<unsigned long long*>(E.ctrl_region + E.scanA_off);
+    unsigned long long* scanB = reinterpret_cast<unsigned long long*>(E.ctrl_region + E.scanB_off);
+    unsigned long long* scanC = reinterpret_cast<unsigned long long*>(E.ctrl_region + E.scanC_off);
+    // only the parts of the scan regions this extraction can touch need zeroing
+    const size_t zero_bytes = dc ? E.ctrl_bytes : E.scanC_off;
+    record(cudaMemsetAsync(E.ctrl_region, 0, zero_bytes, st));
+    if (E.timing) cudaEventRecord(E.ev[0], st);
+
+    SceneView sv;
+    sv.prims = reinterpret_cast<const float4*>(E.d_prims);
+    sv.nodes = reinterpret_cast<const float4*>(E.d_nodes);
+    sv.nprims = (int)E.sorted.size();
+    sv.nbvh = E.nbvh;
+    sv.nnodes = (int)E.nodes.size();
+    const GridView gv = E.gv;
+    Diag* diag = &ctrl->diag;
+    const int nb = E.nblocks;
+    run_scout_compact(gv, sv, time, E.flags, scanA, E.list, &ctrl->active_count, diag, st);
+    if (E.timing) cudaEventRecord(E.ev[1], st);
+    ActiveView av{E.list, &ctrl->active_count, nb};
+    MeshOut mo;
+    mo.verts = reinterpret_cast<float4*>(out->vertices);
+    mo.colors = reinterpret_cast<float4*>(out->colors);
+    mo.indices = out->indices;
+    mo.uvs = reinterpret_cast<float2*>(out->uvs);
+    mo.primids = out->primitive_ids;
+    mo.normals = reinterpret_cast<float4*>(out->normals);
+    mo.maxV = out->max_vertices;
+    unsigned mask = C.out_mask;
+    if (!out->colors) mask &= ~OUT_COLORS;
+    if (!out->indices) mask &= ~OUT_INDICES;
+    if (!out->uvs) mask &= ~OUT_UVS;
+    if (!out->primitive_ids) mask &= ~OUT_PRIMIDS;
+    if (!out->normals) mask &= ~OUT_NORMALS;
+
+    if (!dc) {
+        k_mc_field<<<persistent_grid(k_mc_field, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(
+            gv, sv, time, av, E.fields, E.block_totals, (E.debug & 1) ? E.packet_counts : nullptr, &ctrl->tickets[0],
+            diag);
+        check_launch();
+        if (E.timing) cudaEventRecord(E.ev[2], st);
+        k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)nb)), SCAN_THREADS, 0, st>>>(
+            E.block_totals, E.block_offsets, 0, &ctrl->active_count, 1, scan_state(scanB), &ctrl->total_vertices, diag);
+        check_launch();
+        if (E.timing) cudaEventRecord(E.ev[3], st);
+        k_mc_emit<<<persistent_grid(k_mc_emit, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(
+            gv, sv, time, av, E.fields, E.block_offsets, nullptr, (E.debug & 1) ? E.packet_offsets : nullptr, mo, mask,
+            &ctrl->tickets[1], diag);
+        check_launch();
+        if (E.timing) cudaEventRecord(E.ev[4], st);
+    } else {
+        DcBuffers B;
+        B.block_to_active = E.b2a;
+        B.masks = E.masks;
+        B.vert_offsets = E.dc_voff;
+        B.cell_verts = E.dc_verts;
+        B.cell_normals = E.dc_norms;
+        B.cell_normals_tmp = nullptr;
+        B.counts = E.packet_counts;
+        B.offsets = E.packet_offsets;
+        record(cudaMemsetAsync(E.b2a, 0xFF, (size_t)nb * sizeof(int), st));
+        k_dc_block_map<<<(nb + 255) / 256, 256, 0, st>>>(E.list, &ctrl->active_count, nb, nb, E.b2a);
+        check_launch();
+        k_dc_mark<<<persistent_grid(k_dc_mark, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(gv, sv, time, av, E.fields, B,
+                                                                                      &ctrl->tickets[0], diag);
+        check_launch();
+        const unsigned ncells_max = (unsigned)nb * 512u;
+        k_exclusive_scan<<<std::max(1u, scan_tiles(ncells_max)), SCAN_THREADS, 0, st>>>(
+            E.packet_counts, E.dc_voff, 0, &ctrl->active_count, 512, scan_state(scanC), &ctrl->dc_vertices, diag);
+        check_launch();
+        if (E.timing) cudaEventRecord(E.ev[2], st);
+        DcSolveParams sp;
+        sp.max_cell_vertices = (unsigned)E.dc_cap;
+        sp.qef_blend = C.qef_blend;
+        sp.solver = C.dc_solver;
+        sp.projection_iters = C.dc_solver == SDF_DC_SOLVER_MASSPOINT ? C.projection_iters : 0;
+        sp.cond_threshold = C.cond_threshold > 0.f ? C.cond_threshold : 1e4f;
+        const size_t solve_smem = sizeof(SolveSmem);
+        k_dc_solve<<<persistent_grid(k_dc_solve, BLK_THREADS, nb, solve_smem), BLK_THREADS, solve_smem, st>>>(
+            gv, sv, time, av, E.fields, B, sp, &ctrl->tickets[1], diag);
+        check_launch();
+        if (E.timing) cudaEventRecord(E.ev[3], st);
+        k_dc_count_quads<<<nb, 512, 0, st>>>(gv, av, B, E.packet_counts, E.block_totals);
+        check_launch();
+        k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)nb)), SCAN_THREADS, 0, st>>>(
+            E.block_totals, E.block_offsets, 0, &ctrl->active_count, 1, scan_state(scanB), &ctrl->total_vertices, diag);
+        check_launch();
+        DcQuadParams qp;
+        qp.adaptive_diagonal = (C.dc_solver == SDF_DC_SOLVER_MASSPOINT) ? C.adaptive_diagonal : 0;
+        const size_t quad_smem = sizeof(QuadSmem);
+        k_dc_quads<<<persistent_grid(k_dc_quads, BLK_THREADS, nb, quad_smem), BLK_THREADS, quad_smem, st>>>(
+            gv, sv, time, av, B, nullptr, E.packet_counts, E.block_offsets, mo, mask, qp, &ctrl->tickets[2], diag);
+        check_launch();
+        if (E.timing) cudaEventRecord(E.ev[4], st);
+    }
+    record(cudaMemcpyAsync(E.h_ctrl, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+    const cudaError_t err = cudaStreamSynchronize(st);
+    auto t1 = std::chrono::high_resolution_clock::now();
+    if (err != cudaSuccess) {
+        record(err);
+        return SDF_ERR_CUDA;
+    }
+    const Ctrl& h = *E.h_ctrl;
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->total_blocks = nb;
+        stats->active_blocks = h.active_count;
+        stats->total_vertices = h.total_vertices;
+        stats->written_vertices = std::min<int64_t>(h.total_vertices, out->max_vertices);
+        stats->dc_cell_vertices = h.dc_vertices;
+        stats->bvh_cap_hits = (int64_t)h.diag.cap_hits;
+        stats->ms_total = std::chrono::duration<float, std::milli>(t1 - t0).count();
+        if (E.timing) {
+            cudaEventElapsedTime(&stats->ms_scout, E.ev[0], E.ev[1]);
+            cudaEventElapsedTime(&stats->ms_field, E.ev[1], E.ev[2]);
+            cudaEventElapsedTime(&stats->ms_scan, E.ev[2], E.ev[3]);
+            cudaEventElapsedTime(&stats->ms_emit, E.ev[3], E.ev[4]);
+        }
+    }
+    if (h.diag.timeout) return SDF_ERR_TIMEOUT;
+    if (h.diag.stack_overflow) return SDF_ERR_STACK;
+    if (h.total_vertices > out->max_vertices || (dc && h.dc_vertices > E.dc_cap)) return SDF_ERR_CAPACITY;
+    return SDF_OK;
+}
+
+const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes) {
+    if (!e) return nullptr;
+    EngineImpl& E = e->impl;
+    const size_t cells = (size_t)E.nblocks * 512;
+    const void* p = nullptr;
+    size_t b = 0;
+    switch (which) {
+        case 0: p = E.list; b = (size_t)E.nblocks * 4; break;
+        case 1: p = E.packet_counts; b = E.packet_cap ? cells * 4 : 0; break;
+        case 2: p = E.packet_offsets; b = E.packet_cap ? cells * 4 : 0; break;
+        case 3: p = E.masks; b = E.packet_cap ? cells : 0; break;
+        case 4: p = E.dc_voff; b = E.packet_cap ? cells * 4 : 0; break;
+        case 5: p = E.dc_verts; b = E.dc_cap * 8; break;
+        case 6: p = E.dc_norms; b = E.dc_cap * 8; break;
+        case 7: p = E.block_totals; b = (size_t)E.nblocks * 4; break;
+        case 8: p = E.fields; b = (size_t)E.nblocks * sdfb::FIELD_STRIDE * 4; break;
+        default: break;
+    }
+    if (bytes) *bytes = b;
+    return p;
+}
+
+sdf_status sdf_engine_read_buffer(sdf_engine* e, int which, void* host_dst, size_t bytes) {
+    size_t have = 0;
+    const void* p = sdf_engine_buffer(e, which, &have);
+    if (!p || !host_dst || bytes > have) return SDF_ERR_INVALID;
+    cudaSetDevice(e->impl.device);
+    if (cudaDeviceSynchronize() != cudaSuccess) return SDF_ERR_CUDA;
+    return cudaMemcpy(host_dst, p, bytes, cudaMemcpyDeviceToHost) == cudaSuccess ? SDF_OK : SDF_ERR_CUDA;
+}
+
+sdf_status sdf_extract(const sdf_primitive* prims, int count, const sdf_config* cfg, float time,
+                       const sdf_outputs* out, void* stream, sdf_stats* stats) {
+    sdf_engine* e = nullptr;
+    sdf_status s = sdf_engine_create(&e, -1);
+    if (s != SDF_OK) return s;
+    s = sdf_engine_configure(e, cfg);
+    if (s == SDF_OK) s = sdf_engine_set_scene(e, prims, count);
+    if (s == SDF_OK) s = sdf_engine_extract(e, time, out, stream, stats);
+    sdf_engine_destroy(e);
+    return s;
+}
+
+}  // extern "C"

@@ -1,0 +1,457 @@
+// Marching-cubes stages for sm_100a: scout, compaction, block field + count, emission.
+//
+// Work decomposition. One thread block (CTA) owns one active 8^3 block at a time and evaluates
+// the block's 9^3 = 729 corner samples once, into shared memory, with warp-coherent map() calls
+// (23 warps' worth of 32 samples). The reference evaluates map() 8 times per cell in the count
+// kernel and 8 times again in the emit kernel (MarchingCubesKernels.cu:936-950, 987-1001), i.e.
+// 8192 evaluations per active block per pass; here a block costs 729. Every sample value equals
+// the reference's value at that grid point bit for bit (same point, same arithmetic), so case
+// codes, counts and vertex positions are unchanged.
+//
+// The CTAs are persistent: each claims active blocks from an atomic ticket until the device-side
+// active count is exhausted, so no host read-back is needed between stages.
+#pragma once
+
+#include "mc_cases.inc"
+#include "scan.cuh"
+#include "sdf_device.cuh"
+#include "uv.cuh"
+
+namespace sdfb {
+
+constexpr int BLK_THREADS = 256;           // 8 warps per CTA
+constexpr int FIELD_N = 729;               // 9^3 samples of one block incl. the +1 halo
+constexpr int FIELD_STRIDE = 736;          // padded to a multiple of 16 floats (64 B rows)
+constexpr int FIELD_CHUNKS = (FIELD_N + 31) / 32;
+constexpr int MAX_BLOCK_TRIS = 512 * 5;    // upper bound of triangles in one block
+
+// marching-cubes case table (re-encoded reference table, see gen_mc_cases.py)
+__constant__ unsigned long long c_mcCases[256] = {SDF_MC_CASE_WORDS};
+
+struct ActiveView {
+    const int* list;       // active block linear indices, ascending
+    const int* count_dev;  // device-side active count
+    int cap;               // host-side bound (numActiveBlocks of the drop-in launchers)
+};
+
+struct MeshOut {
+    float4* verts;
+    float4* colors;
+    unsigned* indices;
+    float2* uvs;
+    int* primids;
+    float4* normals;
+    unsigned maxV;
+};
+
+enum { OUT_COLORS = 1, OUT_INDICES = 2, OUT_UVS = 4, OUT_PRIMIDS = 8, OUT_NORMALS = 16 };
+
+__device__ __forceinline__ int active_count(const ActiveView& av) {
+    int n = av.count_dev ? *av.count_dev : av.cap;
+    return n < av.cap ? n : av.cap;
+}
+
+__device__ __forceinline__ void block_coord(const GridView& g, int lin, int& bx, int& by, int& bz) {
+    bx = lin % g.bx;
+    const int t = lin / g.bx;
+    by = t % g.by;
+    bz = t / g.by;
+}
+
+// claims the next work item for the whole CTA; returns -1 when done
+__device__ __forceinline__ int claim(unsigned* ticket, int n, int* s_item) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int a = (int)atomicAdd(ticket, 1u);
+        *s_item = a < n ? a : -1;
+    }
+    __syncthreads();
+    return *s_item;
+}
+
+// 9^3 samples of block `lin` into s_field (index (z*9 + y)*9 + x); samples outside the grid are 0 and
+// never read by an in-bounds cell
+__device__ __forceinline__ void eval_block_field(const GridView& g, const SceneView& sc, float time, int lin,
+                                                 float* s_field, Diag* diag) {
+    int bx, by, bz;
+    block_coord(g, lin, bx, by, bz);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (int chunk = warp; chunk < FIELD_CHUNKS; chunk += nwarps) {
+        const int s = chunk * 32 + lane;
+        const int sx = s % 9, sy = (s / 9) % 9, sz = s / 81;
+        const int gx = bx * 8 + sx, gy = by * 8 + sy, gz = bz * 8 + sz;
+        const bool valid = s < FIELD_N && gx < g.w && gy < g.h && gz < g.d;
+        const float3 p = grid_loc(g, gx, gy, gz);
+        MapState<false> st;
+        map_warp<false>(sc, p, valid, time, st, diag);
+        if (s < FIELD_N) s_field[s] = valid ? st.d : 0.f;
+    }
+}
+
+__device__ __forceinline__ int fidx(int x, int y, int z) { return (z * 9 + y) * 9 + x; }
+
+// case code and corner values of the cell at local (lx, ly, lz)
+__device__ __forceinline__ int cell_case(const float* f, int lx, int ly, int lz, float cv[8]) {
+    int code = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        cv[i] = f[fidx(lx + corner_dx(i), ly + corner_dy(i), lz + corner_dz(i))];
+        if (cv[i] > 0.f) code |= 1 << i;
+    }
+    return code;
+}
+
+// interpEdgePoint (MarchingCubesKernels.cu:60-81)
+__device__ __forceinline__ float3 edge_point(const GridView& g, int x, int y, int z, const float cv[8], int e) {
+    const int c1 = edge_c0(e), c2 = edge_c1(e);
+    const float t = edge_t(cv[c1], cv[c2]);
+    const float3 p1 = grid_loc(g, x + corner_dx(c1), y + corner_dy(c1), z + corner_dz(c1));
+    const float3 p2 = grid_loc(g, x + corner_dx(c2), y + corner_dy(c2), z + corner_dz(c2));
+    return lerp3(p1, p2, t);
+}
+
+__device__ __forceinline__ void tri_points(const GridView& g, int x, int y, int z, const float cv[8],
+                                           unsigned long long word, int k, float3 v[3]) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) v[j] = edge_point(g, x, y, z, cv, (int)((word >> (4 + 4 * (3 * k + j))) & 0xF));
+}
+
+// bit k set iff triangle k of the case is non-degenerate (countActiveBlockTriangles, :952-967)
+__device__ __forceinline__ unsigned cell_valid_mask(const GridView& g, int x, int y, int z, const float cv[8],
+                                                    unsigned long long word) {
+    const int nt = (int)(word & 0xF);
+    unsigned m = 0;
+    for (int k = 0; k < nt; ++k) {
+        float3 v[3];
+        tri_points(g, x, y, z, cv, word, k, v);
+        if (!degenerate(v[0], v[1], v[2], g.cell)) m |= 1u << k;
+    }
+    return m;
+}
+
+struct CellInfo {
+    int x, y, z, lx, ly, lz;
+    bool oob;
+};
+
+__device__ __forceinline__ CellInfo cell_info(const GridView& g, int bx, int by, int bz, int tid) {
+    CellInfo c;
+    c.lz = tid >> 6;
+    c.ly = (tid >> 3) & 7;
+    c.lx = tid & 7;
+    c.x = bx * 8 + c.lx;
+    c.y = by * 8 + c.ly;
+    c.z = bz * 8 + c.lz;
+    c.oob = c.x >= g.w - 1 || c.y >= g.h - 1 || c.z >= g.d - 1;  // outOfBounds (Commons.cuh:204-207)
+    return c;
+}
+
+// ------------------------------------------------------------------------------------------------
+// scout (MarchingCubesKernels.cu:850-889). Warps take 4x4x2 bricks of blocks so the 32 block
+// centres of a warp are spatially close and their BVH walks coincide; the result is a 0/1 flag per
+// linear block index, compacted in index order afterwards.
+// ------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(BLK_THREADS) k_scout(GridView g, SceneView sc, float time, unsigned* flags,
+                                                       Diag* diag) {
+    const int lane = threadIdx.x & 31;
+    const int warp_global = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int nbx = (g.bx + 3) >> 2, nby = (g.by + 3) >> 2, nbz = (g.bz + 1) >> 1;
+    if (warp_global >= nbx * nby * nbz) return;
+    const int wx = warp_global % nbx, t = warp_global / nbx, wy = t % nby, wz = t / nby;
+    const int bx = wx * 4 + (lane & 3), by = wy * 4 + ((lane >> 2) & 3), bz = wz * 2 + (lane >> 4);
+    const bool valid = bx < g.bx && by < g.by && bz < g.bz;
+    const float3 c = f3(FMA(ADD((float)(bx * 8), 4.f), g.cell, g.ox), FMA(ADD((float)(by * 8), 4.f), g.cell, g.oy),
+                        FMA(ADD((float)(bz * 8), 4.f), g.cell, g.oz));
+    MapState<false> st;
+    map_warp<false>(sc, c, valid, time, st, diag);
+    const float r = MUL(8 * 0.5f * 1.73205f + 2.0f, g.cell);
+    if (valid) flags[bx + g.bx * (by + g.by * bz)] = fabsf(st.d) <= r ? 1u : 0u;
+}
+
+// ------------------------------------------------------------------------------------------------
+// block field + per-cell counts
+// ------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(BLK_THREADS) k_mc_field(GridView g, SceneView sc, float time, ActiveView av,
+                                                          float* __restrict__ fields_out,
+                                                          unsigned* __restrict__ block_totals,
+                                                          unsigned* __restrict__ packet_counts, unsigned* ticket,
+                                                          Diag* diag) {
+    __shared__ __align__(16) float s_field[FIELD_STRIDE];
+    __shared__ unsigned s_red[BLK_THREADS / 32];
+    __shared__ int s_item;
+    const int n = active_count(av);
+    for (;;) {
+        const int a = claim(ticket, n, &s_item);
+        if (a < 0) break;
+        const int lin = av.list[a];
+        eval_block_field(g, sc, time, lin, s_field, diag);
+        if (threadIdx.x < FIELD_STRIDE - FIELD_N) s_field[FIELD_N + threadIdx.x] = 0.f;
+        __syncthreads();
+        if (fields_out) {
+            float4* dst = reinterpret_cast<float4*>(fields_out + (size_t)a * FIELD_STRIDE);
+            const float4* src = reinterpret_cast<const float4*>(s_field);
+            for (int i = threadIdx.x; i < FIELD_STRIDE / 4; i += blockDim.x) dst[i] = src[i];
+        }
+        int bx, by, bz;
+        block_coord(g, lin, bx, by, bz);
+        unsigned cnt[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int tid = 2 * threadIdx.x + h;
+            const CellInfo c = cell_info(g, bx, by, bz, tid);
+            cnt[h] = 0;
+            if (!c.oob) {
+                float cv[8];
+                const int code = cell_case(s_field, c.lx, c.ly, c.lz, cv);
+                const unsigned long long word = c_mcCases[code];
+                cnt[h] = 3u * __popc(cell_valid_mask(g, c.x, c.y, c.z, cv, word));
+            }
+        }
+        if (packet_counts)
+            *reinterpret_cast<uint2*>(packet_counts + (size_t)a * 512 + 2 * threadIdx.x) = make_uint2(cnt[0], cnt[1]);
+        if (block_totals) {
+            unsigned v = cnt[0] + cnt[1];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                unsigned s = 0;
+                for (int w = 0; w < BLK_THREADS / 32; ++w) s += s_red[w];
+                block_totals[a] = s;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// emission (generateActiveBlockTriangles, MarchingCubesKernels.cu:972-1110)
+// ------------------------------------------------------------------------------------------------
+struct EmitSmem {
+    float field[FIELD_STRIDE];
+    unsigned warp_sums[BLK_THREADS / 32];
+    unsigned short tri_cell[MAX_BLOCK_TRIS];  // (cell << 3) | triangle slot
+    unsigned tri_out[MAX_BLOCK_TRIS];         // first output vertex of the triangle
+    int ntri;
+    int item;
+};
+
+// writes the triangle-list attributes: colour / primitive id / uv from map() at the triangle
+// centre (one warp-coherent call per 32 triangles), normals from computeNormal at each vertex
+__device__ void emit_attributes(const GridView& g, const SceneView& sc, float time, int bx, int by, int bz,
+                                EmitSmem& S, const MeshOut& out, unsigned mask, Diag* diag) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const int ntri = S.ntri;
+    if (mask & (OUT_COLORS | OUT_PRIMIDS | OUT_UVS)) {
+        for (int base = warp * 32; base < ntri; base += nwarps * 32) {
+            const int i = base + lane;
+            const bool valid = i < ntri;
+            float3 v[3] = {f3(0.f, 0.f, 0.f), f3(0.f, 0.f, 0.f), f3(0.f, 0.f, 0.f)};
+            unsigned w = 0;
+            if (valid) {
+                const int tid = S.tri_cell[i] >> 3, k = S.tri_cell[i] & 7;
+                const CellInfo c = cell_info(g, bx, by, bz, tid);
+                float cv[8];
+                const int code = cell_case(S.field, c.lx, c.ly, c.lz, cv);
+                tri_points(g, c.x, c.y, c.z, cv, c_mcCases[code], k, v);
+                w = S.tri_out[i];
+            }
+            const float3 ctr = f3(DIV(ADD(ADD(v[0].x, v[1].x), v[2].x), 3.f), DIV(ADD(ADD(v[0].y, v[1].y), v[2].y), 3.f),
+                                  DIV(ADD(ADD(v[0].z, v[1].z), v[2].z), 3.f));
+            MapState<true> st;
+            map_warp<true>(sc, ctr, valid, time, st, diag);
+            if (valid) {
+                if ((mask & OUT_COLORS) && out.colors) {
+                    const float4 c4 = make_float4(st.color.x, st.color.y, st.color.z, 1.f);
+                    out.colors[w] = c4;
+                    out.colors[w + 1] = c4;
+                    out.colors[w + 2] = c4;
+                }
+                if ((mask & OUT_PRIMIDS) && out.primids) {
+                    const int bits = __float_as_int((float)st.id);
+                    out.primids[w] = bits;
+                    out.primids[w + 1] = bits;
+                    out.primids[w + 2] = bits;
+                }
+                if ((mask & OUT_UVS) && out.uvs) {
+                    float2 uv[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+                    if (st.id >= 0 && st.id < sc.nprims) {
+                        const float4* pr = sc.prims + (size_t)st.id * PRIM_ROWS;
+                        const float4 rot = __ldg(pr + 0), pos = __ldg(pr + 2), scl = __ldg(pr + 3);
+                        float3 lp[3];
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) lp[j] = to_local(v[j], rot, pos, scl);
+                        triangle_uvs(lp, load_uv_params(pr), uv);
+                    }
+                    out.uvs[w] = uv[0];
+                    out.uvs[w + 1] = uv[1];
+                    out.uvs[w + 2] = uv[2];
+                }
+            }
+        }
+    }
+    if ((mask & OUT_NORMALS) && out.normals) {
+        const int nv = ntri * 3;
+        for (int base = warp * 32; base < nv; base += nwarps * 32) {
+            const int i = base + lane;
+            const bool valid = i < nv;
+            float3 p = f3(0.f, 0.f, 0.f);
+            unsigned w = 0;
+            if (valid) {
+                const int t = i / 3, j = i - 3 * t;
+                const int tid = S.tri_cell[t] >> 3, k = S.tri_cell[t] & 7;
+                const CellInfo c = cell_info(g, bx, by, bz, tid);
+                float cv[8];
+                const int code = cell_case(S.field, c.lx, c.ly, c.lz, cv);
+                float3 v[3];
+                tri_points(g, c.x, c.y, c.z, cv, c_mcCases[code], k, v);
+                p = v[j];
+                w = S.tri_out[t] + j;
+            }
+            const float3 nrm = normal_warp(sc, p, valid, time, g.cell, diag);
+            if (valid) out.normals[w] = make_float4(nrm.x, nrm.y, nrm.z, 0.f);
+        }
+    }
+}
+
+// Modes: FIELD_FROM (fields_in != nullptr: load the stored field; else evaluate it) and OFFSETS_FROM
+// (packet_offsets_in != nullptr: per-cell offsets of the drop-in layout; else block_offsets + an
+// in-block scan).
+__global__ void __launch_bounds__(BLK_THREADS) k_mc_emit(GridView g, SceneView sc, float time, ActiveView av,
+                                                         const float* __restrict__ fields_in,
+                                                         const unsigned* __restrict__ block_offsets,
+                                                         const unsigned* __restrict__ packet_offsets_in,
+                                                         unsigned* __restrict__ packet_offsets_out, MeshOut out,
+                                                         unsigned mask, unsigned* ticket, Diag* diag) {
+    __shared__ __align__(16) EmitSmem S;
+    const int n = active_count(av);
+    const bool attrs = (mask & (OUT_COLORS | OUT_PRIMIDS | OUT_UVS | OUT_NORMALS)) != 0;
+    for (;;) {
+        const int a = claim(ticket, n, &S.item);
+        if (a < 0) break;
+        const int lin = av.list[a];
+        if (fields_in) {
+            const float4* src = reinterpret_cast<const float4*>(fields_in + (size_t)a * FIELD_STRIDE);
+            float4* dst = reinterpret_cast<float4*>(S.field);
+            for (int i = threadIdx.x; i < FIELD_STRIDE / 4; i += blockDim.x) dst[i] = __ldcs(src + i);
+        } else {
+            eval_block_field(g, sc, time, lin, S.field, diag);
+        }
+        __syncthreads();
+        int bx, by, bz;
+        block_coord(g, lin, bx, by, bz);
+        CellInfo c[2];
+        float cv[2][8];
+        unsigned long long word[2];
+        unsigned vm[2], cnt[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            c[h] = cell_info(g, bx, by, bz, 2 * threadIdx.x + h);
+            vm[h] = 0;
+            word[h] = 0;
+            if (!c[h].oob) {
+                const int code = cell_case(S.field, c[h].lx, c[h].ly, c[h].lz, cv[h]);
+                word[h] = c_mcCases[code];
+                vm[h] = cell_valid_mask(g, c[h].x, c[h].y, c[h].z, cv[h], word[h]);
+            }
+            cnt[h] = 3u * __popc(vm[h]);
+        }
+        unsigned local_total;
+        const unsigned local = block_exclusive<BLK_THREADS>(cnt[0] + cnt[1], S.warp_sums, &local_total);
+        unsigned off[2];
+        if (packet_offsets_in) {
+            const uint2 o = *reinterpret_cast<const uint2*>(packet_offsets_in + (size_t)a * 512 + 2 * threadIdx.x);
+            off[0] = o.x;
+            off[1] = o.y;
+        } else {
+            off[0] = block_offsets[a] + local;
+            off[1] = off[0] + cnt[0];
+        }
+        if (packet_offsets_out)
+            *reinterpret_cast<uint2*>(packet_offsets_out + (size_t)a * 512 + 2 * threadIdx.x) = make_uint2(off[0], off[1]);
+        if (threadIdx.x == 0) S.ntri = 0;
+        __syncthreads();
+        unsigned tslot = local / 3;  // this thread's first slot in the block triangle list
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (c[h].oob) continue;
+            unsigned w = off[h];
+            const int nt = (int)(word[h] & 0xF);
+            for (int k = 0; k < nt; ++k) {
+                if (!((vm[h] >> k) & 1u)) continue;
+                if ((unsigned long long)w + 2 >= out.maxV) break;  // the reference's capacity stop (:1020)
+                float3 v[3];
+                tri_points(g, c[h].x, c[h].y, c[h].z, cv[h], word[h], k, v);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) out.verts[w + j] = make_float4(v[j].x, v[j].y, v[j].z, 1.f);
+                if ((mask & OUT_INDICES) && out.indices) {
+                    out.indices[w] = w;
+                    out.indices[w + 1] = w + 1;
+                    out.indices[w + 2] = w + 2;
+                }
+                if (attrs) {
+                    S.tri_cell[tslot] = (unsigned short)(((2 * threadIdx.x + h) << 3) | k);
+                    S.tri_out[tslot] = w;
+                    atomicAdd(&S.ntri, 1);
+                }
+                ++tslot;
+                w += 3;
+            }
+        }
+        if (attrs) {
+            __syncthreads();
+            // slots are dense except when the capacity stop dropped triangles; S.ntri counts them,
+            // and dropped slots only occur at the end of the output, i.e. the tail of the list
+            emit_attributes(g, sc, time, bx, by, bz, S, out, mask, diag);
+        }
+    }
+}
+
+// active list from the 0/1 flags: out[prefix(i)] = i where flags[i] != 0 (same look-back scan)
+__global__ void __launch_bounds__(SCAN_THREADS) k_compact(const unsigned* __restrict__ flags, unsigned n,
+                                                          int* __restrict__ list, int* __restrict__ count,
+                                                          ScanState st, Diag* diag) {
+    __shared__ unsigned s_warp[SCAN_THREADS / 32];
+    __shared__ unsigned s_pfx;
+    __shared__ int s_tile;
+    if (threadIdx.x == 0) s_tile = (int)atomicAdd(st.ticket, 1u);
+    __syncthreads();
+    const int tile = s_tile;
+    const unsigned base = (unsigned)tile * SCAN_TILE;
+    if (base >= n && tile != 0) return;
+    uint4 v[SCAN_ROUNDS];
+    unsigned tsum[SCAN_ROUNDS], pre[SCAN_ROUNDS], rtot[SCAN_ROUNDS];
+#pragma unroll
+    for (int r = 0; r < SCAN_ROUNDS; ++r) {
+        const unsigned i0 = base + (unsigned)r * (SCAN_THREADS * 4) + threadIdx.x * 4;
+        if (i0 + 3 < n) {
+            v[r] = *reinterpret_cast<const uint4*>(flags + i0);
+        } else {
+            v[r].x = i0 < n ? flags[i0] : 0u;
+            v[r].y = i0 + 1 < n ? flags[i0 + 1] : 0u;
+            v[r].z = i0 + 2 < n ? flags[i0 + 2] : 0u;
+            v[r].w = i0 + 3 < n ? flags[i0 + 3] : 0u;
+        }
+        tsum[r] = v[r].x + v[r].y + v[r].z + v[r].w;
+    }
+#pragma unroll
+    for (int r = 0; r < SCAN_ROUNDS; ++r) pre[r] = block_exclusive<SCAN_THREADS>(tsum[r], s_warp, &rtot[r]);
+    unsigned agg = 0;
+#pragma unroll
+    for (int r = 0; r < SCAN_ROUNDS; ++r) agg += rtot[r];
+    const unsigned tile_pfx = tile_lookback(st, tile, agg, &s_pfx, diag);
+    unsigned carry = tile_pfx;
+#pragma unroll
+    for (int r = 0; r < SCAN_ROUNDS; ++r) {
+        const unsigned i0 = base + (unsigned)r * (SCAN_THREADS * 4) + threadIdx.x * 4;
+        unsigned p = carry + pre[r];
+        if (v[r].x) list[p++] = (int)i0;
+        if (v[r].y) list[p++] = (int)(i0 + 1);
+        if (v[r].z) list[p++] = (int)(i0 + 2);
+        if (v[r].w) list[p++] = (int)(i0 + 3);
+        carry += rtot[r];
+    }
+    if (threadIdx.x == 0 && base + SCAN_TILE >= n) *count = (int)(tile_pfx + agg);
+}
+
+}  // namespace sdfb

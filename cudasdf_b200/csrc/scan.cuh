@@ -119,21 +119,25 @@ __device__ __forceinline__ unsigned tile_lookback(const ScanState& st, int tile,
     return r;
 }
 
-// out[i] = sum(in[0..i)), i < n. n is read from *n_dev when n_dev != nullptr (device-side count),
+// out[i] = sum(in[0..i)), i < n. n is (*n_dev) * n_mult when n_dev != nullptr (a device-side count),
 // else n_host. If `total` is set, the grand total is written there by the last tile.
 __global__ void __launch_bounds__(SCAN_THREADS) k_exclusive_scan(const unsigned* __restrict__ in,
                                                                  unsigned* __restrict__ out, unsigned n_host,
-                                                                 const int* __restrict__ n_dev, ScanState st,
-                                                                 unsigned* total, Diag* diag) {
+                                                                 const int* __restrict__ n_dev, unsigned n_mult,
+                                                                 ScanState st, unsigned* total, Diag* diag) {
     __shared__ unsigned s_warp[SCAN_THREADS / 32];
     __shared__ unsigned s_pfx;
     __shared__ int s_tile;
-    const unsigned n = n_dev ? (unsigned)max(*n_dev, 0) : n_host;
+    const unsigned n = n_dev ? (unsigned)max(*n_dev, 0) * n_mult : n_host;
     if (threadIdx.x == 0) s_tile = (int)atomicAdd(st.ticket, 1u);
     __syncthreads();
     const int tile = s_tile;
     const unsigned base = (unsigned)tile * SCAN_TILE;
     if (base >= n && tile != 0) return;
+    if (n == 0) {
+        if (total && threadIdx.x == 0) *total = 0;
+        return;
+    }
     // load: round r covers items [base + r*1024, +1024), 4 per thread
     uint4 v[SCAN_ROUNDS];
     unsigned tsum[SCAN_ROUNDS];

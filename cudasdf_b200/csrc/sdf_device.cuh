@@ -45,10 +45,13 @@ __device__ __forceinline__ float3 scl3(float3 a, float s) { return f3(MUL(s, a.x
 // a.x*b.x + a.y*b.y + a.z*b.z
 __device__ __forceinline__ float dot3(float3 a, float3 b) { return FMA(a.z, b.z, FMA(a.x, b.x, MUL(a.y, b.y))); }
 __device__ __forceinline__ float len3(float3 a) { return SQRT(dot3(a, a)); }
+// length(float2) with the first square fused (len2) or the second (len2b)
 __device__ __forceinline__ float len2(float x, float y) { return SQRT(FMA(x, x, MUL(y, y))); }
-// a*b - c*d
+__device__ __forceinline__ float len2b(float x, float y) { return SQRT(FMA(y, y, MUL(x, x))); }
+// a*b - c*d with the first product fused
 __device__ __forceinline__ float det2(float a, float b, float c, float d) { return FMA(a, b, -MUL(c, d)); }
-__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+// cross3 (MarchingCubesKernels.cu:21-27) as the DC kernels compute it: first product fused
+__device__ __forceinline__ float3 cross_ff(float3 a, float3 b) {
     return f3(det2(a.y, b.z, a.z, b.y), det2(a.z, b.x, a.x, b.z), det2(a.x, b.y, a.y, b.x));
 }
 __device__ __forceinline__ bool finite3(float3 v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z); }
@@ -108,15 +111,16 @@ __device__ __forceinline__ Leaf load_leaf(const float4* __restrict__ pr) {
     return L;
 }
 
-// rotateVector with u = q.xyz, s = q.w (Commons.cuh:264-273)
+// rotateVector with u = q.xyz, s = q.w (Commons.cuh:264-273):
+// 2*dot(u,v)*u + (s*s - dot(u,u))*v + 2*s*cross(u,v); the inline cross fuses its second product
 __device__ __forceinline__ float3 rotate(float3 v, float ux, float uy, float uz, float s) {
     const float3 u = f3(ux, uy, uz);
-    const float a = MUL(2.0f, dot3(u, v));
+    const float a = MUL(2.0f, FMA(u.z, v.z, FMA(u.y, v.y, MUL(u.x, v.x))));
     const float b = FMA(s, s, -dot3(u, u));
     const float c = MUL(2.0f, s);
-    const float3 cr = cross3(u, v);
-    return f3(FMA(c, cr.x, FMA(a, u.x, MUL(b, v.x))), FMA(c, cr.y, FMA(a, u.y, MUL(b, v.y))),
-              FMA(c, cr.z, FMA(a, u.z, MUL(b, v.z))));
+    const float3 cr = f3(FMA(-u.z, v.y, MUL(u.y, v.z)), FMA(-u.x, v.z, MUL(u.z, v.x)), FMA(-u.y, v.x, MUL(u.x, v.y)));
+    return f3(FMA(c, cr.x, FMA(b, v.x, MUL(a, u.x))), FMA(c, cr.y, FMA(b, v.y, MUL(a, u.y))),
+              FMA(c, cr.z, FMA(b, v.z, MUL(a, u.z))));
 }
 // world -> primitive local: subtract position, conjugate rotation, divide by scale
 __device__ __forceinline__ float3 to_local(float3 pw, float4 rot, float4 pos, float4 scale) {
@@ -132,11 +136,11 @@ __device__ __forceinline__ float sd_box(float3 p, float bx, float by, float bz) 
     return ADD(len3(f3(fmaxf(qx, 0.f), fmaxf(qy, 0.f), fmaxf(qz, 0.f))), fminf(fmaxf(qx, fmaxf(qy, qz)), 0.f));
 }
 __device__ __forceinline__ float sd_torus(float3 p, float r1, float r2) {
-    return SUB(len2(SUB(len2(p.x, p.z), r1), p.y), r2);
+    return SUB(len2b(SUB(len2(p.x, p.z), r1), p.y), r2);
 }
 __device__ __forceinline__ float sd_cylinder(float3 p, float h, float r) {
     const float dx = SUB(fabsf(len2(p.x, p.z)), r), dy = SUB(fabsf(p.y), h);
-    return ADD(fminf(fmaxf(dx, dy), 0.f), len3(f3(fmaxf(dx, 0.f), fmaxf(dy, 0.f), 0.f)));
+    return ADD(fminf(fmaxf(dx, dy), 0.f), len2b(fmaxf(dx, 0.f), fmaxf(dy, 0.f)));
 }
 __device__ __forceinline__ float sd_capsule(float3 p, float h, float r) {
     p.y = SUB(p.y, CLAMP(p.y, 0.f, h));
@@ -174,22 +178,22 @@ __device__ __forceinline__ float sd_rounded_cone(float3 p, float h, float r1, fl
     const float b = DIV(SUB(r1, r2), h);
     const float a = SQRT(FMA(-b, b, 1.f));
     const float k = FMA(qx, -b, MUL(qy, a));
-    if (k < 0.f) return SUB(len2(qx, qy), r1);
-    if (k > MUL(a, h)) return SUB(len2(qx, SUB(qy, h)), r2);
+    if (k < 0.f) return SUB(len2b(qx, qy), r1);
+    if (k > MUL(a, h)) return SUB(len2b(qx, SUB(qy, h)), r2);
     return SUB(FMA(qx, a, MUL(qy, b)), r1);
 }
 __device__ __forceinline__ float sd_rounded_cylinder(float3 p, float h, float r1, float r2) {
     const float dx = ADD(FMA(-2.f, r1, len2(p.x, p.z)), r2), dy = SUB(fabsf(p.y), h);
-    return SUB(ADD(fminf(fmaxf(dx, dy), 0.f), len2(fmaxf(dx, 0.f), fmaxf(dy, 0.f))), r2);
+    return SUB(ADD(fminf(fmaxf(dx, dy), 0.f), len2b(fmaxf(dx, 0.f), fmaxf(dy, 0.f))), r2);
 }
 __device__ __forceinline__ float sd_hexprism(float3 p, float hx, float hy) {
     const float kx = -0.8660254f, ky = 0.5f, kz = 0.57735027f;
     p = f3(fabsf(p.x), fabsf(p.y), fabsf(p.z));
-    const float m = fminf(FMA(kx, p.x, MUL(ky, p.z)), 0.f);
+    const float m = fminf(FMA(ky, p.z, MUL(kx, p.x)), 0.f);
     const float px = FMA(-MUL(kx, 2.f), m, p.x), pz = FMA(-MUL(ky, 2.f), m, p.z);
     const float ex = SUB(px, CLAMP(px, MUL(-kz, hx), MUL(kz, hx))), ez = SUB(pz, hx);
-    const float dx = MUL(len2(ex, ez), copysignf(1.f, SUB(pz, hx))), dy = SUB(p.y, hy);
-    return ADD(fminf(fmaxf(dx, dy), 0.f), len2(fmaxf(dx, 0.f), fmaxf(dy, 0.f)));
+    const float dx = MUL(len2b(ex, ez), copysignf(1.f, SUB(pz, hx))), dy = SUB(p.y, hy);
+    return ADD(fminf(fmaxf(dx, dy), 0.f), len2b(fmaxf(dx, 0.f), fmaxf(dy, 0.f)));
 }
 
 __device__ __forceinline__ float sd_eval(int type, float3 p, float4 pm) {
@@ -217,10 +221,10 @@ __device__ __forceinline__ float leaf_distance(const Leaf& L, float3 pw, float t
     pre = p;
     if (L.disp == DSP_TWIST) {
         const float c = cosf(MUL(L.dp0, p.y)), s = sinf(MUL(L.dp0, p.y));
-        p = f3(det2(c, p.x, s, p.z), p.y, FMA(s, p.x, MUL(c, p.z)));
+        p = f3(det2(c, p.x, s, p.z), p.y, FMA(c, p.z, MUL(s, p.x)));
     } else if (L.disp == DSP_BEND) {
         const float c = cosf(MUL(L.dp0, p.x)), s = sinf(MUL(L.dp0, p.x));
-        p = f3(det2(c, p.x, s, p.y), FMA(s, p.x, MUL(c, p.y)), p.z);
+        p = f3(det2(c, p.x, s, p.y), FMA(c, p.y, MUL(s, p.x)), p.z);
     } else if (L.disp == DSP_SINE) {
         p.y = FMA(sinf(FMA(p.x, L.dp0, time)), L.dp1, p.y);
     }
@@ -231,8 +235,10 @@ __device__ __forceinline__ float leaf_distance(const Leaf& L, float3 pw, float t
     return d;
 }
 
-// mix(x, y, a) = x*(1-a) + y*a (Commons.cuh:247)
-__device__ __forceinline__ float mixf(float x, float y, float a) { return FMA(x, SUB(1.f, a), MUL(y, a)); }
+// mix(x, y, a) = x*(1-a) + y*a (Commons.cuh:247). Inside map()'s blends the union / intersect
+// blends and the colour mix fuse y*a, the subtract blend fuses x*(1-a).
+__device__ __forceinline__ float mix_fy(float x, float y, float a) { return FMA(y, a, MUL(x, SUB(1.f, a))); }
+__device__ __forceinline__ float mix_fx(float x, float y, float a) { return FMA(x, SUB(1.f, a), MUL(y, a)); }
 
 // running state of one point's map(); colour/id/local only tracked when ATTR
 template <bool ATTR>
@@ -286,25 +292,25 @@ __device__ __forceinline__ void combine(MapState<ATTR>& st, int op, float k, con
             break;
         case OP_UNION_BLEND:
             h = CLAMP(ADD(0.5f, DIV(MUL(0.5f, SUB(st.d, dp)), k)), 0.f, 1.f);
-            st.d = FMA(-MUL(k, h), SUB(1.f, h), mixf(st.d, dp, h));
+            st.d = FMA(-MUL(k, h), SUB(1.f, h), mix_fy(st.d, dp, h));
             if (ATTR) {
-                st.color = f3(mixf(st.color.x, pc.x, h), mixf(st.color.y, pc.y, h), mixf(st.color.z, pc.z, h));
+                st.color = f3(mix_fy(st.color.x, pc.x, h), mix_fy(st.color.y, pc.y, h), mix_fy(st.color.z, pc.z, h));
                 if (dp < st.d || h > 0.5f) { st.id = i; st.local = pre; }
             }
             break;
         case OP_SUB_BLEND:
             h = CLAMP(SUB(0.5f, DIV(MUL(0.5f, ADD(st.d, dp)), k)), 0.f, 1.f);
-            st.d = FMA(MUL(k, h), SUB(1.f, h), mixf(st.d, -dp, h));
+            st.d = FMA(MUL(k, h), SUB(1.f, h), mix_fx(st.d, -dp, h));
             if (ATTR) {
-                st.color = f3(mixf(st.color.x, pc.x, h), mixf(st.color.y, pc.y, h), mixf(st.color.z, pc.z, h));
+                st.color = f3(mix_fy(st.color.x, pc.x, h), mix_fy(st.color.y, pc.y, h), mix_fy(st.color.z, pc.z, h));
                 if (h > 0.5f) { st.id = i; st.local = pre; }
             }
             break;
         case OP_INT_BLEND:
             h = CLAMP(SUB(0.5f, DIV(MUL(0.5f, SUB(st.d, dp)), k)), 0.f, 1.f);
-            st.d = FMA(MUL(k, h), SUB(1.f, h), mixf(st.d, dp, h));
+            st.d = FMA(MUL(k, h), SUB(1.f, h), mix_fy(st.d, dp, h));
             if (ATTR) {
-                st.color = f3(mixf(st.color.x, pc.x, h), mixf(st.color.y, pc.y, h), mixf(st.color.z, pc.z, h));
+                st.color = f3(mix_fy(st.color.x, pc.x, h), mix_fy(st.color.y, pc.y, h), mix_fy(st.color.z, pc.z, h));
                 if (dp > st.d || h > 0.5f) { st.id = i; st.local = pre; }
             }
             break;
@@ -322,9 +328,10 @@ __device__ __forceinline__ bool box_closer(float3 p, float4 a, float4 b, float d
 
 // Per-launch diagnostics shared by all kernels of an extraction.
 struct Diag {
-    unsigned long long cap_hits;  // points whose search was cut by the 256-pop cap
-    int stack_overflow;           // a search needed more than 64 stack entries
-    int timeout;                  // a bounded wait gave up
+    unsigned long long cap_hits;    // points whose search was cut by the 256-pop cap
+    unsigned long long fp64_cells;  // mass-point DC cells solved with the FP64 eigensolve
+    int stack_overflow;             // a search needed more than 64 stack entries
+    int timeout;                    // a bounded wait gave up
 };
 
 // map() for the 32 points of a warp. Must be called by all 32 lanes together (warp-uniform control
@@ -441,6 +448,7 @@ __device__ __forceinline__ float edge_t(float v1, float v2) {
     if (t >= 1.f) t = 1.f - 1e-7f;
     return t;
 }
+// lerp3 (:48-54) as inlined in interpEdgePoint and the DC solve: a*(1-t) fused
 __device__ __forceinline__ float3 lerp3(float3 a, float3 b, float t) {
     const float u = SUB(1.f, t);
     return f3(FMA(a.x, u, MUL(b.x, t)), FMA(a.y, u, MUL(b.y, t)), FMA(a.z, u, MUL(b.z, t)));

@@ -1,0 +1,128 @@
+"""Python front end of the fused engine (sdf_engine_* in include/sdfmesh_b200.h).
+
+Device memory comes from torch (the caller's CUDA allocator); every kernel is the library's own.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+from .scenes import PRIM_DTYPE
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class MeshBuffers:
+    """Output streams in the reference's VBO/EBO layout (triangle soup)."""
+
+    def __init__(self, max_vertices: int, out_mask: int, device="cuda"):
+        import torch
+        self.max_vertices = int(max_vertices)
+        self.out_mask = int(out_mask)
+        n = max(self.max_vertices, 1)
+        self.vertices = torch.empty((n, 4), dtype=torch.float32, device=device)
+        self.colors = torch.empty((n, 4), dtype=torch.float32, device=device) if out_mask & L.OUT_COLORS else None
+        self.indices = torch.empty((n,), dtype=torch.int32, device=device) if out_mask & L.OUT_INDICES else None
+        self.uvs = torch.empty((n, 2), dtype=torch.float32, device=device) if out_mask & L.OUT_UVS else None
+        self.primitive_ids = torch.empty((n,), dtype=torch.int32, device=device) if out_mask & L.OUT_PRIMIDS else None
+        self.normals = torch.empty((n, 4), dtype=torch.float32, device=device) if out_mask & L.OUT_NORMALS else None
+
+    def c_struct(self) -> L.SdfOutputs:
+        o = L.SdfOutputs()
+        o.vertices = self.vertices.data_ptr()
+        o.colors = self.colors.data_ptr() if self.colors is not None else None
+        o.indices = self.indices.data_ptr() if self.indices is not None else None
+        o.uvs = self.uvs.data_ptr() if self.uvs is not None else None
+        o.primitive_ids = self.primitive_ids.data_ptr() if self.primitive_ids is not None else None
+        o.normals = self.normals.data_ptr() if self.normals is not None else None
+        o.max_vertices = self.max_vertices
+        return o
+
+
+def make_config(cell_size: float, bounds_min=(-1.0, -1.0, -1.0), bounds_max=(1.0, 1.0, 1.0), technique=L.TECH_MC,
+                qef_blend=1.0, dc_solver=L.DC_SOLVER_REFERENCE, projection_iters=0, adaptive_diagonal=0,
+                cond_threshold=1e4, out_mask=L.OUT_INDICES) -> L.SdfConfig:
+    c = L.SdfConfig()
+    c.cell_size = float(np.float32(cell_size))
+    for k in range(3):
+        c.bounds_min[k] = float(bounds_min[k])
+        c.bounds_max[k] = float(bounds_max[k])
+    c.technique = int(technique)
+    c.qef_blend = float(qef_blend)
+    c.dc_solver = int(dc_solver)
+    c.projection_iters = int(projection_iters)
+    c.adaptive_diagonal = int(adaptive_diagonal)
+    c.cond_threshold = float(cond_threshold)
+    c.out_mask = int(out_mask)
+    return c
+
+
+class Engine:
+    """One engine instance: grid configuration, uploaded scene, reusable device buffers."""
+
+    def __init__(self, device: int = -1):
+        self._lib = L.lib()
+        h = ctypes.c_void_p()
+        L.check(self._lib.sdf_engine_create(ctypes.byref(h), int(device)), "sdf_engine_create")
+        self.h = h
+        self.config = None
+
+    def close(self):
+        if self.h:
+            self._lib.sdf_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def configure(self, cfg: L.SdfConfig):
+        L.check(self._lib.sdf_engine_configure(self.h, ctypes.byref(cfg)), "sdf_engine_configure")
+        self.config = cfg
+
+    def set_scene(self, prims: np.ndarray):
+        p = np.ascontiguousarray(prims, dtype=PRIM_DTYPE)
+        L.check(self._lib.sdf_engine_set_scene(self.h, p.ctypes.data, len(p)), "sdf_engine_set_scene")
+
+    def set_timing(self, on: bool):
+        self._lib.sdf_engine_set_timing(self.h, 1 if on else 0)
+
+    def set_debug(self, flags: int):
+        self._lib.sdf_engine_set_debug(self.h, int(flags))
+
+    def extract(self, out: MeshBuffers, time: float = 0.0, stream=None, allow_capacity=False) -> dict:
+        st = L.SdfStats()
+        o = out.c_struct()
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        rc = self._lib.sdf_engine_extract(self.h, float(time), ctypes.byref(o), sp, ctypes.byref(st))
+        if not (allow_capacity and rc == L.SDF_ERR_CAPACITY):
+            L.check(rc, "sdf_engine_extract")
+        d = st.as_dict()
+        d["status"] = rc
+        return d
+
+    def bvh(self):
+        nb = ctypes.c_int(0)
+        n = self._lib.sdf_engine_get_bvh(self.h, None, 0, ctypes.byref(nb))
+        nodes = np.zeros(max(n, 0), dtype=[("min", "<f4", 3), ("max", "<f4", 3), ("left", "<i4"), ("right", "<i4")])
+        if n > 0:
+            self._lib.sdf_engine_get_bvh(self.h, nodes.ctypes.data, n, ctypes.byref(nb))
+        return nodes, nb.value
+
+    def buffer(self, which: int, dtype, count: int) -> np.ndarray:
+        """Copies `count` elements of an internal device array (see sdf_engine_buffer) to the host."""
+        nbytes = ctypes.c_size_t(0)
+        self._lib.sdf_engine_buffer(self.h, int(which), ctypes.byref(nbytes))
+        dt = np.dtype(dtype)
+        count = min(int(count), nbytes.value // dt.itemsize)
+        out = np.zeros(count, dt)
+        if count:
+            L.check(self._lib.sdf_engine_read_buffer(self.h, int(which), out.ctypes.data, out.nbytes),
+                    "sdf_engine_read_buffer")
+        return out

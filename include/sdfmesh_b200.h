@@ -30,7 +30,7 @@ extern "C" {
  * Data layout (Commons.cuh)
  * ---------------------------------------------------------------------------------------------- */
 typedef struct sdf_float2 { float x, y; } sdf_float2;
-typedef struct SDF_ALIGN16 sdf_float4 { float x, y, z, w; } sdf_float4;
+typedef struct sdf_float4 { SDF_ALIGN16 float x; float y, z, w; } sdf_float4;
 typedef struct sdf_ushort4 { uint16_t x, y, z, w; } sdf_ushort4;
 typedef struct sdf_short4 { int16_t x, y, z, w; } sdf_short4;
 
@@ -47,8 +47,8 @@ enum { DISP_NONE = 0, DISP_SINE, DISP_TWIST, DISP_BEND, DISP_ELONGATE, DISP_ROUN
        DISP_REVOLUTION };
 
 /* SDFPrimitive (Commons.cuh:68-102): 160 bytes */
-typedef struct SDF_ALIGN16 sdf_primitive {
-    float rotation[4];   /* quaternion x, y, z, w */
+typedef struct sdf_primitive {
+    SDF_ALIGN16 float rotation[4]; /* quaternion x, y, z, w */
     float dispParams[4];
     float position[3];
     float blendFactor;   /* smooth-blend k */
@@ -234,14 +234,19 @@ sdf_status sdf_engine_set_scene(sdf_engine* e, const sdf_primitive* prims, int c
 /* One extraction on `stream` (a cudaStream_t, NULL = legacy default stream). The only host
  * synchronisation is the final count read-back into *stats. */
 sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out, void* stream, sdf_stats* stats);
-/* Enables per-stage CUDA-event timing inside sdf_engine_extract (adds host syncs). */
+/* Enables per-stage CUDA-event timing inside sdf_engine_extract. */
 void sdf_engine_set_timing(sdf_engine* e, int enabled);
+/* Debug outputs: bit 0 also writes the per-cell vertex counts/offsets of the drop-in layout in
+ * marching-cubes mode (readable through sdf_engine_buffer 1 and 2). */
+void sdf_engine_set_debug(sdf_engine* e, int flags);
 /* The scene as uploaded: sorted primitives (count = numPrimitives) and BVH nodes. */
 int sdf_engine_get_bvh(sdf_engine* e, sdf_bvh_node* nodes_out, int capacity, int* num_bvh_primitives);
 /* Device pointer to the last extraction's internal arrays, for inspection: 0 active block list,
  * 1 per-cell vertex counts (compat layout), 2 per-cell offsets, 3 DC corner masks, 4 DC cell vertex
  * offsets, 5 DC cell vertices, 6 DC cell normals, 7 per-block vertex totals. */
 const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes);
+/* Copies the first `bytes` bytes of an internal array (ids as for sdf_engine_buffer) to host memory. */
+sdf_status sdf_engine_read_buffer(sdf_engine* e, int which, void* host_dst, size_t bytes);
 
 /* One-shot convenience: create, configure, set scene, extract, destroy. */
 sdf_status sdf_extract(const sdf_primitive* prims, int count, const sdf_config* cfg, float time,
