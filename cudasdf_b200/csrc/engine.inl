@@ -57,18 +57,20 @@ struct EngineImpl {
     int debug = 0;
     cudaEvent_t ev[8] = {};
     size_t packet_cap = 0;
+    Diag* eval_diag = nullptr;
 
     ~EngineImpl() { release(); }
 
     void release() {
         void* ptrs[] = {d_prims, d_nodes, flags, list, fields, block_totals, block_offsets, packet_counts,
-                        packet_offsets, b2a, masks, dc_voff, dc_verts, dc_norms, ctrl_region};
+                        packet_offsets, b2a, masks, dc_voff, dc_verts, dc_norms, ctrl_region, eval_diag};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         d_prims = nullptr; d_nodes = nullptr; flags = nullptr; list = nullptr; fields = nullptr;
         block_totals = nullptr; block_offsets = nullptr; packet_counts = nullptr; packet_offsets = nullptr;
         b2a = nullptr; masks = nullptr; dc_voff = nullptr; dc_verts = nullptr; dc_norms = nullptr;
         ctrl_region = nullptr;
+        eval_diag = nullptr;
         prims_cap = nodes_cap = dc_cap = packet_cap = 0;
         if (h_ctrl) cudaFreeHost(h_ctrl);
         h_ctrl = nullptr;
@@ -392,6 +394,28 @@ const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes) {
     }
     if (bytes) *bytes = b;
     return p;
+}
+
+sdf_status sdf_engine_eval(sdf_engine* e, const float* d_points, int n, float time, float* d_out, void* stream) {
+    using namespace sdfb;
+    if (!e || n < 0 || (n > 0 && (!d_points || !d_out))) return SDF_ERR_INVALID;
+    if (n == 0) return SDF_OK;
+    EngineImpl& E = e->impl;
+    cudaSetDevice(E.device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!E.eval_diag && cudaMalloc(&E.eval_diag, sizeof(Diag)) != cudaSuccess) return SDF_ERR_NOMEM;
+    record(cudaMemsetAsync(E.eval_diag, 0, sizeof(Diag), st));
+    SceneView sv;
+    sv.prims = reinterpret_cast<const float4*>(E.d_prims);
+    sv.nodes = reinterpret_cast<const float4*>(E.d_nodes);
+    sv.nprims = (int)E.sorted.size();
+    sv.nbvh = E.nbvh;
+    sv.nnodes = (int)E.nodes.size();
+    const int warps = (n + 31) / 32;
+    const int blocks = std::min((warps + 7) / 8, num_sms() * 8);
+    k_eval_points<<<blocks, BLK_THREADS, 0, st>>>(sv, d_points, n, time, d_out, E.eval_diag);
+    const cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? SDF_OK : SDF_ERR_CUDA;
 }
 
 sdf_status sdf_engine_read_buffer(sdf_engine* e, int which, void* host_dst, size_t bytes) {

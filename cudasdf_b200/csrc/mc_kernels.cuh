@@ -407,6 +407,26 @@ __global__ void __launch_bounds__(BLK_THREADS) k_mc_emit(GridView g, SceneView s
     }
 }
 
+// map() at arbitrary points: out[8*i ..] = distance, colour xyz, primitive id (as float), local xyz.
+// Points are taken 32 per warp in input order, so spatially sorted input keeps the walks coherent.
+__global__ void __launch_bounds__(BLK_THREADS) k_eval_points(SceneView sc, const float* __restrict__ pts, int n,
+                                                             float time, float* __restrict__ out, Diag* diag) {
+    const int warps_total = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n; base += warps_total * 32) {
+        const int i = base + lane;
+        const bool valid = i < n;
+        const float3 p = valid ? f3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]) : f3(0.f, 0.f, 0.f);
+        MapState<true> st;
+        map_warp<true>(sc, p, valid, time, st, diag);
+        if (valid) {
+            float* o = out + 8 * (size_t)i;
+            o[0] = st.d; o[1] = st.color.x; o[2] = st.color.y; o[3] = st.color.z;
+            o[4] = (float)st.id; o[5] = st.local.x; o[6] = st.local.y; o[7] = st.local.z;
+        }
+    }
+}
+
 // active list from the 0/1 flags: out[prefix(i)] = i where flags[i] != 0 (same look-back scan)
 __global__ void __launch_bounds__(SCAN_THREADS) k_compact(const unsigned* __restrict__ flags, unsigned n,
                                                           int* __restrict__ list, int* __restrict__ count,

@@ -107,6 +107,16 @@ class Engine:
         d["status"] = rc
         return d
 
+    def eval(self, points, time: float = 0.0, stream=None):
+        """map() at device points (torch float32 (n, 3)); returns a (n, 8) device tensor."""
+        import torch
+        pts = points.contiguous()
+        out = torch.empty((pts.shape[0], 8), dtype=torch.float32, device=pts.device)
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        L.check(self._lib.sdf_engine_eval(self.h, ctypes.c_void_p(pts.data_ptr()), int(pts.shape[0]), float(time),
+                                          ctypes.c_void_p(out.data_ptr()), sp), "sdf_engine_eval")
+        return out
+
     def bvh(self):
         nb = ctypes.c_int(0)
         n = self._lib.sdf_engine_get_bvh(self.h, None, 0, ctypes.byref(nb))

@@ -248,6 +248,11 @@ const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes);
 /* Copies the first `bytes` bytes of an internal array (ids as for sdf_engine_buffer) to host memory. */
 sdf_status sdf_engine_read_buffer(sdf_engine* e, int which, void* host_dst, size_t bytes);
 
+/* The composite SDF of the current scene (the reference's map(), MarchingCubesKernels.cu:570-808) at n
+ * device points (x, y, z floats). d_out receives 8 floats per point: distance, colour r g b, primitive
+ * index (as a float), local position x y z. Asynchronous on `stream`. */
+sdf_status sdf_engine_eval(sdf_engine* e, const float* d_points, int n, float time, float* d_out, void* stream);
+
 /* One-shot convenience: create, configure, set scene, extract, destroy. */
 sdf_status sdf_extract(const sdf_primitive* prims, int count, const sdf_config* cfg, float time,
                        const sdf_outputs* out, void* stream, sdf_stats* stats);
