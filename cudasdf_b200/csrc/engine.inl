@@ -418,6 +418,65 @@ sdf_status sdf_engine_eval(sdf_engine* e, const float* d_points, int n, float ti
     return err == cudaSuccess ? SDF_OK : SDF_ERR_CUDA;
 }
 
+sdf_status sdf_engine_count_work(sdf_engine* e, unsigned long long out[4]) {
+    using namespace sdfb;
+    if (!e || !out) return SDF_ERR_INVALID;
+    EngineImpl& E = e->impl;
+    if (!E.configured) return SDF_ERR_INVALID;
+    cudaSetDevice(E.device);
+    Ctrl* ctrl = reinterpret_cast<Ctrl*>(E.ctrl_region);
+    unsigned long long* scanA = reinterpret_cast<unsigned long long*>(E.ctrl_region + E.scanA_off);
+    record(cudaMemsetAsync(E.ctrl_region, 0, E.scanC_off, 0));
+    SceneView sv;
+    sv.prims = reinterpret_cast<const float4*>(E.d_prims);
+    sv.nodes = reinterpret_cast<const float4*>(E.d_nodes);
+    sv.nprims = (int)E.sorted.size();
+    sv.nbvh = E.nbvh;
+    sv.nnodes = (int)E.nodes.size();
+    run_scout_compact(E.gv, sv, 0.f, E.flags, scanA, E.list, &ctrl->active_count, &ctrl->diag, 0);
+    record(cudaMemsetAsync(&ctrl->diag, 0, sizeof(Diag), 0));
+    ActiveView av{E.list, &ctrl->active_count, E.nblocks};
+    k_mc_field_count<<<persistent_grid(k_mc_field_count, BLK_THREADS, E.nblocks), BLK_THREADS>>>(
+        E.gv, sv, 0.f, av, nullptr, nullptr, nullptr, &ctrl->tickets[0], &ctrl->diag);
+    check_launch();
+    Ctrl h;
+    if (cudaMemcpy(&h, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost) != cudaSuccess) return SDF_ERR_CUDA;
+    out[0] = h.diag.node_pops;
+    out[1] = h.diag.leaf_evals;
+    out[2] = h.diag.points;
+    out[3] = (unsigned long long)h.active_count;
+    return SDF_OK;
+}
+
+sdf_status sdf_measure_fp32_peak(double* tflops) {
+    using namespace sdfb;
+    if (!tflops) return SDF_ERR_INVALID;
+    float* dummy = nullptr;
+    if (cudaMalloc(&dummy, 256 * sizeof(float)) != cudaSuccess) return SDF_ERR_NOMEM;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = num_sms() * 8, iters = 4096;
+    k_fma_peak<<<blocks, 256>>>(dummy, iters, 0.9999f, 1e-7f);  // warm-up
+    float best = 1e30f;
+    for (int r = 0; r < 3; ++r) {
+        cudaEventRecord(a);
+        k_fma_peak<<<blocks, 256>>>(dummy, iters, 0.9999f, 1e-7f);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        best = std::min(best, ms);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(dummy);
+    if (cudaGetLastError() != cudaSuccess) return SDF_ERR_CUDA;
+    const double flops = 2.0 * 8 * 16 * (double)iters * blocks * 256;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return SDF_OK;
+}
+
 sdf_status sdf_engine_read_buffer(sdf_engine* e, int which, void* host_dst, size_t bytes) {
     size_t have = 0;
     const void* p = sdf_engine_buffer(e, which, &have);

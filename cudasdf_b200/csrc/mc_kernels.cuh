@@ -71,6 +71,7 @@ __device__ __forceinline__ int claim(unsigned* ticket, int n, int* s_item) {
 
 // 9^3 samples of block `lin` into s_field (index (z*9 + y)*9 + x); samples outside the grid are 0 and
 // never read by an in-bounds cell
+template <bool COUNT = false>
 __device__ __forceinline__ void eval_block_field(const GridView& g, const SceneView& sc, float time, int lin,
                                                  float* s_field, Diag* diag) {
     int bx, by, bz;
@@ -83,7 +84,7 @@ __device__ __forceinline__ void eval_block_field(const GridView& g, const SceneV
         const bool valid = s < FIELD_N && gx < g.w && gy < g.h && gz < g.d;
         const float3 p = grid_loc(g, gx, gy, gz);
         MapState<false> st;
-        map_warp<false>(sc, p, valid, time, st, diag);
+        map_warp<false, COUNT>(sc, p, valid, time, st, diag);
         if (s < FIELD_N) s_field[s] = valid ? st.d : 0.f;
     }
 }
@@ -171,7 +172,8 @@ __global__ void __launch_bounds__(BLK_THREADS) k_scout(GridView g, SceneView sc,
 // ------------------------------------------------------------------------------------------------
 // block field + per-cell counts
 // ------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(BLK_THREADS) k_mc_field(GridView g, SceneView sc, float time, ActiveView av,
+template <bool COUNT>
+__global__ void __launch_bounds__(BLK_THREADS) k_mc_field_t(GridView g, SceneView sc, float time, ActiveView av,
                                                           float* __restrict__ fields_out,
                                                           unsigned* __restrict__ block_totals,
                                                           unsigned* __restrict__ packet_counts, unsigned* ticket,
@@ -184,7 +186,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_mc_field(GridView g, SceneView 
         const int a = claim(ticket, n, &s_item);
         if (a < 0) break;
         const int lin = av.list[a];
-        eval_block_field(g, sc, time, lin, s_field, diag);
+        eval_block_field<COUNT>(g, sc, time, lin, s_field, diag);
         if (threadIdx.x < FIELD_STRIDE - FIELD_N) s_field[FIELD_N + threadIdx.x] = 0.f;
         __syncthreads();
         if (fields_out) {
@@ -222,6 +224,25 @@ __global__ void __launch_bounds__(BLK_THREADS) k_mc_field(GridView g, SceneView 
             }
         }
     }
+}
+
+// the block-field kernel, and its work-counting twin (counting runs only)
+static constexpr auto k_mc_field = k_mc_field_t<false>;
+static constexpr auto k_mc_field_count = k_mc_field_t<true>;
+
+// FP32 FMA throughput probe: 8 independent FMA chains per thread, no memory traffic in the loop
+__global__ void __launch_bounds__(256) k_fma_peak(float* out, int iters, float a, float b) {
+    float x0 = threadIdx.x * 1e-7f, x1 = x0 + 1e-7f, x2 = x0 + 2e-7f, x3 = x0 + 3e-7f;
+    float x4 = x0 + 4e-7f, x5 = x0 + 5e-7f, x6 = x0 + 6e-7f, x7 = x0 + 7e-7f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            x0 = __fmaf_rn(x0, a, b); x1 = __fmaf_rn(x1, a, b); x2 = __fmaf_rn(x2, a, b); x3 = __fmaf_rn(x3, a, b);
+            x4 = __fmaf_rn(x4, a, b); x5 = __fmaf_rn(x5, a, b); x6 = __fmaf_rn(x6, a, b); x7 = __fmaf_rn(x7, a, b);
+        }
+    }
+    const float r = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+    if (r == 12345.f) out[threadIdx.x] = r;  // keeps the chains live
 }
 
 // ------------------------------------------------------------------------------------------------

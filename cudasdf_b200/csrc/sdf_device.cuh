@@ -180,7 +180,7 @@ __device__ __forceinline__ float sd_rounded_cone(float3 p, float h, float r1, fl
     const float k = FMA(qx, -b, MUL(qy, a));
     if (k < 0.f) return SUB(len2b(qx, qy), r1);
     if (k > MUL(a, h)) return SUB(len2b(qx, SUB(qy, h)), r2);
-    return SUB(FMA(qx, a, MUL(qy, b)), r1);
+    return SUB(FMA(qy, b, MUL(qx, a)), r1);
 }
 __device__ __forceinline__ float sd_rounded_cylinder(float3 p, float h, float r1, float r2) {
     const float dx = ADD(FMA(-2.f, r1, len2(p.x, p.z)), r2), dy = SUB(fabsf(p.y), h);
@@ -330,15 +330,19 @@ __device__ __forceinline__ bool box_closer(float3 p, float4 a, float4 b, float d
 struct Diag {
     unsigned long long cap_hits;    // points whose search was cut by the 256-pop cap
     unsigned long long fp64_cells;  // mass-point DC cells solved with the FP64 eigensolve
+    unsigned long long node_pops;   // work counters (counting runs only): per-point popped nodes,
+    unsigned long long leaf_evals;  //   per-point primitive evaluations,
+    unsigned long long points;      //   evaluated points
     int stack_overflow;             // a search needed more than 64 stack entries
     int timeout;                    // a bounded wait gave up
 };
 
 // map() for the 32 points of a warp. Must be called by all 32 lanes together (warp-uniform control
 // flow); lanes with valid == false take part in the walk but own no point.
-template <bool ATTR>
+template <bool ATTR, bool COUNT = false>
 __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool valid, float time, MapState<ATTR>& st,
                                          Diag* diag) {
+    unsigned long long cnt_pops = 0, cnt_leaves = 0;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     st.init();
@@ -366,6 +370,7 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
             // a lane pops this node iff it pushed it and has popped fewer than MAP_CAP nodes
             const bool pops = ((mask >> lane) & 1u) && iter < MAP_CAP;
             if (pops) iter++;
+            if (COUNT) cnt_pops += __popc(__ballot_sync(FULL, pops));
             // a node can only pass the prune test for a lane whose running distance is > 0
             const unsigned alive = __ballot_sync(FULL, pops && st.d > 0.f);
             if (alive == 0) continue;
@@ -378,6 +383,7 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
             if (right == -1) {
                 const float4* pr = sc.prims + (size_t)left * PRIM_ROWS;
                 const Leaf L = load_leaf(pr);
+                if (COUNT) cnt_leaves += __popc(hm);
                 if (hit) {
                     float3 pre;
                     const float dp = leaf_distance(L, p, time, pre);
@@ -398,6 +404,12 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
             if (lane == 0 && capped) atomicAdd(&diag->cap_hits, (unsigned long long)__popc(capped));
             if (lane == 0 && overflow) atomicExch(&diag->stack_overflow, 1);
         }
+    }
+    if (COUNT && diag && lane == 0) {
+        const unsigned nlive = __popc(live);
+        atomicAdd(&diag->node_pops, cnt_pops);
+        atomicAdd(&diag->leaf_evals, cnt_leaves + (unsigned long long)nlive * (sc.nprims - sc.nbvh));
+        atomicAdd(&diag->points, (unsigned long long)nlive);
     }
     // non-union primitives: a linear pass in scene order (:703-803)
     for (int i = sc.nbvh; i < sc.nprims; ++i) {

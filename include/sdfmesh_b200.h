@@ -253,6 +253,13 @@ sdf_status sdf_engine_read_buffer(sdf_engine* e, int which, void* host_dst, size
  * index (as a float), local position x y z. Asynchronous on `stream`. */
 sdf_status sdf_engine_eval(sdf_engine* e, const float* d_points, int n, float time, float* d_out, void* stream);
 
+/* Work counters of one extraction's block-field stage (a separate, slower counting run):
+ * out[0] BVH nodes popped per point (summed), out[1] primitive evaluations, out[2] points,
+ * out[3] active blocks. */
+sdf_status sdf_engine_count_work(sdf_engine* e, unsigned long long out[4]);
+/* FP32 FMA throughput of the current device in TFLOP/s, measured by a short FMA-loop kernel. */
+sdf_status sdf_measure_fp32_peak(double* tflops);
+
 /* One-shot convenience: create, configure, set scene, extract, destroy. */
 sdf_status sdf_extract(const sdf_primitive* prims, int count, const sdf_config* cfg, float time,
                        const sdf_outputs* out, void* stream, sdf_stats* stats);

@@ -56,6 +56,7 @@ def lib():
         L.or_result_free.argtypes = [vp]
         L.or_scout_range.argtypes = [ctypes.POINTER(_Scene), ctypes.POINTER(_Grid), f, i64, i64, i]
         L.or_scout_range.restype = i64
+        L.or_scout_flags.argtypes = [ctypes.POINTER(_Scene), ctypes.POINTER(_Grid), f, vp, i, vp, i]
         L.or_mc_blocks.argtypes = [ctypes.POINTER(_Scene), ctypes.POINTER(_Grid), f, vp, i, i]
         L.or_mc_blocks.restype = i64
         L.or_exclusive_scan.argtypes = [vp, vp, i64]
@@ -154,6 +155,14 @@ def run(scene: Scene, grid: _Grid, time: float = 0.0, technique: int = 0, qef_bl
 def scout_range(scene: Scene, grid: _Grid, b0: int, b1: int, time: float = 0.0, nthreads: int = 0) -> int:
     return int(lib().or_scout_range(ctypes.byref(scene._c), ctypes.byref(grid), float(time), int(b0), int(b1),
                                     int(nthreads)))
+
+
+def scout_flags(scene: Scene, grid: _Grid, blocks: np.ndarray, time: float = 0.0, nthreads: int = 0) -> np.ndarray:
+    b = np.ascontiguousarray(blocks, np.int32)
+    out = np.zeros(len(b), np.uint8)
+    lib().or_scout_flags(ctypes.byref(scene._c), ctypes.byref(grid), float(time), b.ctypes.data, len(b),
+                         out.ctypes.data, int(nthreads))
+    return out.astype(bool)
 
 
 def mc_blocks(scene: Scene, grid: _Grid, blocks: np.ndarray, time: float = 0.0, nthreads: int = 0) -> int:

@@ -130,7 +130,8 @@ static float sd_rounded_cone(v3 p, float h, float r1, float r2) {
     float k = fmaf(qx, -b, qy * a);
     if (k < 0.0f) return len2b(qx, qy) - r1;
     if (k > a * h) return len2b(qx, qy - h) - r2;
-    return fmaf(qx, a, qy * b) - r1;
+    /* inside map() the reference's build fuses q.y*b here (a standalone call fuses q.x*a) */
+    return fmaf(qy, b, qx * a) - r1;
 }
 static float sd_rounded_cylinder(v3 p, float h, float r1, float r2) {
     float dx = fmaf(-2.0f, r1, len2(p.x, p.z)) + r2, dy = fabsf(p.y) - h;
@@ -1289,6 +1290,13 @@ int64_t or_scout_range(const OrScene* s, const OrGridDesc* g, float time, int64_
 #pragma omp parallel for schedule(dynamic, 256) reduction(+ : n)
     for (int64_t b = b0; b < b1; ++b) n += scout_block(s, g, time, b);
     return n;
+}
+
+void or_scout_flags(const OrScene* s, const OrGridDesc* g, float time, const int32_t* blocks, int n, uint8_t* flags,
+                    int nthreads) {
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int i = 0; i < n; ++i) flags[i] = (uint8_t)scout_block(s, g, time, blocks[i]);
 }
 
 int64_t or_mc_blocks(const OrScene* s, const OrGridDesc* g, float time, const int32_t* blocks, int nblocks,

@@ -94,6 +94,9 @@ void or_result_free(OrResult* r);
 
 /* scout only, over blocks [b0, b1) (CPU-baseline sampling); returns active count */
 int64_t or_scout_range(const OrScene* s, const OrGridDesc* g, float time, int64_t b0, int64_t b1, int nthreads);
+/* scout decisions for a list of blocks */
+void or_scout_flags(const OrScene* s, const OrGridDesc* g, float time, const int32_t* blocks, int n, uint8_t* flags,
+                    int nthreads);
 /* marching cubes count+generate over a given list of active blocks (CPU-baseline sampling) */
 int64_t or_mc_blocks(const OrScene* s, const OrGridDesc* g, float time, const int32_t* blocks, int nblocks,
                      int nthreads);

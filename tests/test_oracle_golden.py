@@ -19,6 +19,9 @@ PROBE_IDS = {"sd": 0, "xform": 1, "twist": 2, "bend": 3, "sine": 4, "edget": 7, 
              "interp": 10, "degen": 11, "solve3": 12, "qefreg": 13, "qef": 14, "encv": 15, "decv": 16,
              "encn": 17, "decn": 18, "aabb": 19}
 TRIG_PROBES = {"sd5", "twist", "bend", "sine"}  # CUDA sinf/cosf inside
+# The rounded cone's last product pair contracts one way when the reference's sdRoundedCone is
+# inlined into map() and the other way when called alone (the probe); the oracle follows map().
+CONTEXT_PROBES = {"sd8"}
 
 
 def bits_equal(a, b):
@@ -47,6 +50,8 @@ def test_function_probe(name):
     out = O.probe(PROBE_IDS[base], inp)[:, :ref.shape[1]]
     if name in TRIG_PROBES:
         np.testing.assert_allclose(out, ref, rtol=2e-5, atol=2e-6)
+    elif name in CONTEXT_PROBES:
+        np.testing.assert_allclose(out, ref, rtol=3e-7, atol=1e-7)
     else:
         eq = bits_equal(out, ref)
         assert eq.all(), f"{name}: {(~eq.all(1)).sum()} of {len(inp)} records differ from the reference"
@@ -68,10 +73,9 @@ def test_bvh_and_map(name):
     ref = G[name + "_map"]
     # primitive ids and local positions never depend on a transcendental result's last bits here
     assert (out[:, 4] == ref[:, 4]).all()
-    trig = name in ("showcase", "single5") or name == "single8"
+    trig = name in ("showcase", "single5")
     if trig:
-        # showcase: twist/sine displacement; single5: cone (sinf/cosf); single8: rounded cone whose
-        # branch test k < 0 sits on a rounding boundary for a few points
+        # showcase: twist displacement; single5: cone (sinf/cosf)
         np.testing.assert_allclose(out[:, 0], ref[:, 0], rtol=1e-4, atol=2e-6)
     else:
         eq = bits_equal(out, ref)
