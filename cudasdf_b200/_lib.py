@@ -71,7 +71,7 @@ DROPIN_SYMBOLS = ["launchScoutActiveBlocks", "launchCountActiveBlockTriangles", 
                   "launchDCGenerateQuads", "getScanStorageSize", "launchScan"]
 ENGINE_SYMBOLS = ["sdf_engine_create", "sdf_engine_destroy", "sdf_engine_configure", "sdf_engine_set_scene",
                   "sdf_engine_extract", "sdf_engine_set_timing", "sdf_engine_set_debug", "sdf_engine_get_bvh",
-                  "sdf_engine_buffer", "sdf_engine_read_buffer", "sdf_engine_eval", "sdf_engine_count_work", "sdf_measure_fp32_peak", "sdf_extract", "sdf_last_error", "sdf_version"]
+                  "sdf_engine_buffer", "sdf_engine_read_buffer", "sdf_engine_eval", "sdf_engine_eval_distance", "sdf_engine_eval_normals", "sdf_engine_count_work", "sdf_measure_fp32_peak", "sdf_extract", "sdf_last_error", "sdf_version"]
 
 _lib = None
 
@@ -122,6 +122,10 @@ def lib():
     L.sdf_measure_fp32_peak.argtypes = [vp]
     L.sdf_measure_fp32_peak.restype = i
     L.sdf_engine_eval.argtypes = [vp, vp, i, f, vp, vp]
+    L.sdf_engine_eval_distance.argtypes = [vp, vp, i, f, vp, vp]
+    L.sdf_engine_eval_distance.restype = i
+    L.sdf_engine_eval_normals.argtypes = [vp, vp, i, f, f, vp, vp]
+    L.sdf_engine_eval_normals.restype = i
     L.sdf_engine_eval.restype = i
     L.sdf_engine_read_buffer.argtypes = [vp, i, vp, sz]
     L.sdf_engine_read_buffer.restype = i

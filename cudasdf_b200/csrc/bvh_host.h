@@ -52,14 +52,20 @@ inline void primitive_box(const sdf_primitive& p, HostV3& mn, HostV3& mx) {
     }
 }
 
-inline int build_node(int* idx, int count, const std::vector<sdf_primitive>& prims, std::vector<sdf_bvh_node>& nodes) {
+struct HostBox {
+    HostV3 mn, mx;
+};
+
+// The recursion of buildBVHRecursive. The reference recomputes getPrimitiveAABB for every primitive
+// at every level (twice); the box is a pure function of the primitive, so it is computed once per
+// primitive here and looked up, which gives the same nodes in O(n) box evaluations.
+inline int build_node(int* idx, int count, const std::vector<HostBox>& boxes, std::vector<sdf_bvh_node>& nodes) {
     sdf_bvh_node node;
     node.min[0] = node.min[1] = node.min[2] = 1e10f;
     node.max[0] = node.max[1] = node.max[2] = -1e10f;
     HostV3 cc = hv(0.f, 0.f, 0.f);
     for (int i = 0; i < count; ++i) {
-        HostV3 a, b;
-        primitive_box(prims[idx[i]], a, b);
+        const HostV3 a = boxes[idx[i]].mn, b = boxes[idx[i]].mx;
         node.min[0] = fminf(node.min[0], a.x); node.min[1] = fminf(node.min[1], a.y); node.min[2] = fminf(node.min[2], a.z);
         node.max[0] = fmaxf(node.max[0], b.x); node.max[1] = fmaxf(node.max[1], b.y); node.max[2] = fmaxf(node.max[2], b.z);
         cc = hv(cc.x + (a.x + b.x) * 0.5f, cc.y + (a.y + b.y) * 0.5f, cc.z + (a.z + b.z) * 0.5f);
@@ -79,8 +85,7 @@ inline int build_node(int* idx, int count, const std::vector<sdf_primitive>& pri
     const float split = axis == 0 ? cc.x : (axis == 1 ? cc.y : cc.z);
     int mid = 0;
     for (int i = 0; i < count; ++i) {
-        HostV3 a, b;
-        primitive_box(prims[idx[i]], a, b);
+        const HostV3 a = boxes[idx[i]].mn, b = boxes[idx[i]].mx;
         const float c = axis == 0 ? (a.x + b.x) * 0.5f : (axis == 1 ? (a.y + b.y) * 0.5f : (a.z + b.z) * 0.5f);
         if (c < split) {
             const int t = idx[i];
@@ -92,8 +97,8 @@ inline int build_node(int* idx, int count, const std::vector<sdf_primitive>& pri
     if (mid == 0 || mid == count) mid = count / 2;
     const int cur = (int)nodes.size();
     nodes.push_back(node);
-    const int l = build_node(idx, mid, prims, nodes);
-    const int r = build_node(idx + mid, count - mid, prims, nodes);
+    const int l = build_node(idx, mid, boxes, nodes);
+    const int r = build_node(idx + mid, count - mid, boxes, nodes);
     nodes[cur].left = l;
     nodes[cur].right = r;
     return cur;
@@ -111,10 +116,12 @@ inline int prepare_scene(const sdf_primitive* in, int n, std::vector<sdf_primiti
     for (int i = 0; i < n; ++i)
         if (!(in[i].operation == SDF_UNION || in[i].operation == SDF_UNION_BLEND)) sorted.push_back(in[i]);
     if (nu > 0) {
+        std::vector<HostBox> boxes(nu);
+        for (int i = 0; i < nu; ++i) primitive_box(sorted[i], boxes[i].mn, boxes[i].mx);
         std::vector<int> idx(nu);
         for (int i = 0; i < nu; ++i) idx[i] = i;
         nodes.reserve(2 * nu);
-        build_node(idx.data(), nu, sorted, nodes);
+        build_node(idx.data(), nu, boxes, nodes);
     }
     return nu;
 }

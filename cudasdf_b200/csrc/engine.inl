@@ -396,6 +396,47 @@ const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes) {
     return p;
 }
 
+static sdfb::SceneView engine_scene_view(EngineImpl& E) {
+    sdfb::SceneView sv;
+    sv.prims = reinterpret_cast<const float4*>(E.d_prims);
+    sv.nodes = reinterpret_cast<const float4*>(E.d_nodes);
+    sv.nprims = (int)E.sorted.size();
+    sv.nbvh = E.nbvh;
+    sv.nnodes = (int)E.nodes.size();
+    return sv;
+}
+
+sdf_status sdf_engine_eval_normals(sdf_engine* e, const float* d_points, int n, float time, float cell,
+                                   float* d_out, void* stream) {
+    using namespace sdfb;
+    if (!e || n < 0 || (n > 0 && (!d_points || !d_out))) return SDF_ERR_INVALID;
+    if (n == 0) return SDF_OK;
+    EngineImpl& E = e->impl;
+    cudaSetDevice(E.device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!E.eval_diag && cudaMalloc(&E.eval_diag, sizeof(Diag)) != cudaSuccess) return SDF_ERR_NOMEM;
+    const int warps = (n + 31) / 32;
+    const int blocks = std::min((warps + 7) / 8, num_sms() * 8);
+    k_eval_normals<<<blocks, BLK_THREADS, 0, st>>>(engine_scene_view(E), d_points, n, time, cell, d_out,
+                                                   E.eval_diag);
+    return cudaGetLastError() == cudaSuccess ? SDF_OK : SDF_ERR_CUDA;
+}
+
+sdf_status sdf_engine_eval_distance(sdf_engine* e, const float* d_points, int n, float time, float* d_out,
+                                    void* stream) {
+    using namespace sdfb;
+    if (!e || n < 0 || (n > 0 && (!d_points || !d_out))) return SDF_ERR_INVALID;
+    if (n == 0) return SDF_OK;
+    EngineImpl& E = e->impl;
+    cudaSetDevice(E.device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!E.eval_diag && cudaMalloc(&E.eval_diag, sizeof(Diag)) != cudaSuccess) return SDF_ERR_NOMEM;
+    const int warps = (n + 31) / 32;
+    const int blocks = std::min((warps + 7) / 8, num_sms() * 8);
+    k_eval_distance<<<blocks, BLK_THREADS, 0, st>>>(engine_scene_view(E), d_points, n, time, d_out, E.eval_diag);
+    return cudaGetLastError() == cudaSuccess ? SDF_OK : SDF_ERR_CUDA;
+}
+
 sdf_status sdf_engine_eval(sdf_engine* e, const float* d_points, int n, float time, float* d_out, void* stream) {
     using namespace sdfb;
     if (!e || n < 0 || (n > 0 && (!d_points || !d_out))) return SDF_ERR_INVALID;

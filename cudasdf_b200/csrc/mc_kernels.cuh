@@ -448,6 +448,41 @@ __global__ void __launch_bounds__(BLK_THREADS) k_eval_points(SceneView sc, const
     }
 }
 
+// distance only (no colour / id / local position tracking) at arbitrary points
+__global__ void __launch_bounds__(BLK_THREADS) k_eval_distance(SceneView sc, const float* __restrict__ pts, int n,
+                                                               float time, float* __restrict__ out, Diag* diag) {
+    const int warps_total = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n; base += warps_total * 32) {
+        const int i = base + lane;
+        const bool valid = i < n;
+        const float3 p = valid ? f3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]) : f3(0.f, 0.f, 0.f);
+        MapState<false> st;
+        map_warp<false>(sc, p, valid, time, st, diag);
+        if (valid) out[i] = st.d;
+    }
+}
+
+// computeNormal at arbitrary points: out[3*i ..] = unit gradient (central differences of map(),
+// step 0.001 cell, as the reference's computeNormal)
+__global__ void __launch_bounds__(BLK_THREADS) k_eval_normals(SceneView sc, const float* __restrict__ pts, int n,
+                                                              float time, float cell, float* __restrict__ out,
+                                                              Diag* diag) {
+    const int warps_total = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < n; base += warps_total * 32) {
+        const int i = base + lane;
+        const bool valid = i < n;
+        const float3 p = valid ? f3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]) : f3(0.f, 0.f, 0.f);
+        const float3 nrm = normal_warp(sc, p, valid, time, cell, diag);
+        if (valid) {
+            out[3 * (size_t)i] = nrm.x;
+            out[3 * (size_t)i + 1] = nrm.y;
+            out[3 * (size_t)i + 2] = nrm.z;
+        }
+    }
+}
+
 // active list from the 0/1 flags: out[prefix(i)] = i where flags[i] != 0 (same look-back scan)
 __global__ void __launch_bounds__(SCAN_THREADS) k_compact(const unsigned* __restrict__ flags, unsigned n,
                                                           int* __restrict__ list, int* __restrict__ count,

@@ -318,12 +318,23 @@ __device__ __forceinline__ void combine(MapState<ATTR>& st, int op, float k, con
     }
 }
 
-// intersectAABB (MarchingCubesKernels.cu:564-568): distance from p to the box, < running d
+// intersectAABB (MarchingCubesKernels.cu:564-568): sqrt_rn(|p - box|^2) < running d.
+// The same decision without the square root in all but boundary cases: with D = dmin^2 rounded,
+// dd < D(1 - 2^-20) implies sqrt_rn(dd) < dmin, and dd > D(1 + 2^-20) implies sqrt_rn(dd) > dmin
+// (the two roundings of D and of the square root are each within 2^-24 relative, far inside the
+// 2^-20 margin); in between, and when dmin^2 could under- or overflow, the square root decides.
 __device__ __forceinline__ bool box_closer(float3 p, float4 a, float4 b, float dmin) {
     const float dx = fmaxf(fmaxf(SUB(a.x, p.x), SUB(p.x, a.w)), 0.f);
     const float dy = fmaxf(fmaxf(SUB(a.y, p.y), SUB(p.y, b.x)), 0.f);
     const float dz = fmaxf(fmaxf(SUB(a.z, p.z), SUB(p.z, b.y)), 0.f);
-    return SQRT(FMA(dz, dz, FMA(dx, dx, MUL(dy, dy)))) < dmin;
+    const float dd = FMA(dz, dz, FMA(dx, dx, MUL(dy, dy)));
+    if (!(dmin > 0.f)) return false;  // sqrt_rn(dd) >= 0; NaN compares false
+    if (dmin >= 1e-18f && dmin <= 1e18f) {
+        const float d2 = MUL(dmin, dmin);
+        if (dd < MUL(d2, 0x1.ffffep-1f)) return true;   // 1 - 2^-20
+        if (dd > MUL(d2, 0x1.00001p+0f)) return false;  // 1 + 2^-20
+    }
+    return SQRT(dd) < dmin;
 }
 
 // Per-launch diagnostics shared by all kernels of an extraction.

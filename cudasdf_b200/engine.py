@@ -117,6 +117,28 @@ class Engine:
                                           ctypes.c_void_p(out.data_ptr()), sp), "sdf_engine_eval")
         return out
 
+    def eval_distance(self, points, time: float = 0.0, stream=None):
+        """Distance only at device points (torch float32 (n, 3)); returns a (n,) device tensor."""
+        import torch
+        pts = points.contiguous()
+        out = torch.empty((pts.shape[0],), dtype=torch.float32, device=pts.device)
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        L.check(self._lib.sdf_engine_eval_distance(self.h, ctypes.c_void_p(pts.data_ptr()), int(pts.shape[0]),
+                                                   float(time), ctypes.c_void_p(out.data_ptr()), sp),
+                "sdf_engine_eval_distance")
+        return out
+
+    def eval_normals(self, points, cell: float, time: float = 0.0, stream=None):
+        """computeNormal at device points (torch float32 (n, 3)); returns a (n, 3) device tensor."""
+        import torch
+        pts = points.contiguous()
+        out = torch.empty((pts.shape[0], 3), dtype=torch.float32, device=pts.device)
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        L.check(self._lib.sdf_engine_eval_normals(self.h, ctypes.c_void_p(pts.data_ptr()), int(pts.shape[0]),
+                                                  float(time), float(cell), ctypes.c_void_p(out.data_ptr()), sp),
+                "sdf_engine_eval_normals")
+        return out
+
     def bvh(self):
         nb = ctypes.c_int(0)
         n = self._lib.sdf_engine_get_bvh(self.h, None, 0, ctypes.byref(nb))

@@ -252,6 +252,13 @@ sdf_status sdf_engine_read_buffer(sdf_engine* e, int which, void* host_dst, size
  * device points (x, y, z floats). d_out receives 8 floats per point: distance, colour r g b, primitive
  * index (as a float), local position x y z. Asynchronous on `stream`. */
 sdf_status sdf_engine_eval(sdf_engine* e, const float* d_points, int n, float time, float* d_out, void* stream);
+/* Distance only (no attributes) at n device points: 1 float per point. */
+sdf_status sdf_engine_eval_distance(sdf_engine* e, const float* d_points, int n, float time, float* d_out,
+                                    void* stream);
+/* The reference's computeNormal (MarchingCubesKernels.cu:814-844) at n device points: 3 floats per
+ * point, finite differences of the composite SDF with step 0.001 * cell. */
+sdf_status sdf_engine_eval_normals(sdf_engine* e, const float* d_points, int n, float time, float cell,
+                                   float* d_out, void* stream);
 
 /* Work counters of one extraction's block-field stage (a separate, slower counting run):
  * out[0] BVH nodes popped per point (summed), out[1] primitive evaluations, out[2] points,

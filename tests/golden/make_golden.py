@@ -224,8 +224,8 @@ def gen_map_probes(rng) -> dict:
 
 
 def run_pipeline(prims, res, technique, out_mask, t=0.0, qef_blend=1.0, max_vertices=50_000_000,
-                 full=True, dc_normal_passes=False) -> dict:
-    mesh = R.RefMesh(S.cell_size_for(res), max_vertices=max_vertices)
+                 full=True, dc_normal_passes=False, cell=None, bmin=S.BOUNDS_MIN, bmax=S.BOUNDS_MAX) -> dict:
+    mesh = R.RefMesh(cell if cell is not None else S.cell_size_for(res), bmin, bmax, max_vertices=max_vertices)
     mesh.set_primitives(prims)
     st = mesh.run(t, technique, qef_blend, out_mask, sort_active=True)
     nA = st["activeUsed"]
@@ -282,13 +282,50 @@ def run_pipeline(prims, res, technique, out_mask, t=0.0, qef_blend=1.0, max_vert
     return d
 
 
+def mixed_scene_notrig(seed, n):
+    """Every primitive type without transcendentals (the cone calls sinf/cosf), every operation,
+    annular/rounding shells; no displacement."""
+    rng = np.random.default_rng(seed)
+    p = S.random_scene(n, seed, size_range=(0.08, 0.35), center_range=0.6)
+    types = [t for t in range(15) if t != S.SDF_CONE]
+    p["type"] = rng.choice(types, n)
+    p["operation"] = rng.choice([0, 0, 3, 3, 1, 2, 4, 5], n)
+    p["operation"][0] = S.SDF_UNION
+    p["blendFactor"] = rng.uniform(0.02, 0.2, n)
+    p["params"] = rng.uniform(0.2, 0.9, (n, 6))
+    p["params"][:, 2] = np.where(p["type"] == S.SDF_ROUNDED_CONE, rng.uniform(0.05, 0.15, n), p["params"][:, 2])
+    p["annular"] = np.where(rng.random(n) < 0.2, rng.uniform(0, 0.03, n), 0)
+    p["rounding"] = np.where(rng.random(n) < 0.2, rng.uniform(0, 0.03, n), 0)
+    return p
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
     ap.add_argument("--skip-full", action="store_true", help="skip the full-size digests")
+    ap.add_argument("--only-odd", action="store_true", help="only the non-power-of-two grid fixtures")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     t0 = time.time()
+    # grids whose cell size is not a power of two and whose origin is not -1: here the products
+    # i * cellSize round, so these pin how grid points are formed
+    odd_bmin, odd_bmax = (-1.1, -1.05, -1.0), (1.1, 1.0, 1.05)
+    odd_cell = float(np.float32(2.2) / np.float32(50))
+    notrig = mixed_scene_notrig(21, 48)
+    odd = [
+        ("mc_c2_odd50", S.config_scene(2), 0, R.OUT_ALL, 0.0),
+        ("dc_c2_odd50", S.config_scene(2), 1, R.OUT_ALL, 0.0),
+        ("mc_mixed_odd50", notrig, 0, R.OUT_ALL, 0.0),
+        ("dc_mixed_odd50", notrig, 1, R.OUT_ALL, 0.0),
+    ]
+    for name, prims, tech, mask, t in odd:
+        d = run_pipeline(prims, 50, tech, mask, t, cell=odd_cell, bmin=odd_bmin, bmax=odd_bmax)
+        np.savez_compressed(os.path.join(args.out, name + ".npz"), prims=prims, res=np.int32(50),
+                            technique=np.int32(tech), out_mask=np.int32(mask), time=np.float32(t),
+                            cell=np.float32(odd_cell), bmin=np.float32(odd_bmin), bmax=np.float32(odd_bmax), **d)
+        print(name, json.loads(d["stats"]), time.time() - t0, flush=True)
+    if args.only_odd:
+        return
     rng = np.random.Generator(np.random.PCG64(S.SEED_BASE + 100))
     np.savez_compressed(os.path.join(args.out, "probes.npz"), **gen_probes(rng))
     print("probes", time.time() - t0, flush=True)

@@ -26,13 +26,14 @@ def exclusive_scan(x):
     return out.astype(np.uint32)
 
 
-def engine_run(prims, res, technique, out_mask, time=0.0, max_vertices=None, debug=True, **cfg_kw):
+def engine_run(prims, res, technique, out_mask, time=0.0, max_vertices=None, debug=True, cell=None,
+               bmin=(-1.0, -1.0, -1.0), bmax=(1.0, 1.0, 1.0), **cfg_kw):
     from cudasdf_b200 import _lib as L
     from cudasdf_b200 import scenes as S
     from cudasdf_b200.engine import Engine, MeshBuffers, make_config
-    cell = S.cell_size_for(res)
+    cell = S.cell_size_for(res) if cell is None else cell
     eng = Engine()
-    eng.configure(make_config(cell, technique=technique, out_mask=out_mask, **cfg_kw))
+    eng.configure(make_config(cell, bmin, bmax, technique=technique, out_mask=out_mask, **cfg_kw))
     eng.set_debug(1 if debug else 0)
     eng.set_scene(prims)
     buf = MeshBuffers(max_vertices or 4_000_000, out_mask)
@@ -66,14 +67,15 @@ def engine_run(prims, res, technique, out_mask, time=0.0, max_vertices=None, deb
     return r
 
 
-def dropin_run(prims, res, technique, out_mask, time=0.0, max_vertices=4_000_000, max_active=1 << 30):
+def dropin_run(prims, res, technique, out_mask, time=0.0, max_vertices=4_000_000, max_active=1 << 30, cell=None,
+               bmin=(-1.0, -1.0, -1.0), bmax=(1.0, 1.0, 1.0)):
     import torch
 
     from cudasdf_b200 import _lib as L
     from cudasdf_b200 import scenes as S
     from cudasdf_b200.dropin import CudaSDFMesh
     mesh = CudaSDFMesh(max_active_blocks=max_active, max_vertices=max_vertices)
-    mesh.Initialize(S.cell_size_for(res), S.BOUNDS_MIN, S.BOUNDS_MAX)
+    mesh.Initialize(S.cell_size_for(res) if cell is None else cell, bmin, bmax)
     for p in prims:
         mesh.AddPrimitive(p)
     n = max_vertices

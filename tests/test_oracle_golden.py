@@ -92,12 +92,16 @@ def run_fixture(name, nthreads=0):
     G = load(name)
     sc = O.Scene(G["prims"])
     res = int(G["res"])
-    g = O.make_grid(float(np.float32(2.0) / np.float32(res)))
+    if "cell" in G.files:
+        g = O.make_grid(float(G["cell"]), tuple(G["bmin"]), tuple(G["bmax"]))
+    else:
+        g = O.make_grid(float(np.float32(2.0) / np.float32(res)))
     r = O.run(sc, g, float(G["time"]), int(G["technique"]), 1.0, int(G["out_mask"]), nthreads=nthreads)
     return G, r
 
 
-BITEXACT_PIPELINES = ["mc_sphere64", "mc_sphere128", "mc_c2_64", "dc_sphere64", "dc_c2_64", "dc_c3_128"]
+BITEXACT_PIPELINES = ["mc_sphere64", "mc_sphere128", "mc_c2_64", "dc_sphere64", "dc_c2_64", "dc_c3_128",
+                      "mc_c2_odd50", "dc_c2_odd50"]
 TRIG_PIPELINES = ["mc_showcase64", "dc_showcase64"]
 
 
