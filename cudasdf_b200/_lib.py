@@ -69,6 +69,7 @@ DROPIN_SYMBOLS = ["launchScoutActiveBlocks", "launchCountActiveBlockTriangles", 
                   "launchBuildBlockToActiveMap", "launchDCMarkCells", "launchDCSolveCellVertices",
                   "launchDCRecomputeNormalsAtVertices", "launchDCSmoothCellNormals", "launchDCCountQuads",
                   "launchDCGenerateQuads", "getScanStorageSize", "launchScan"]
+STATIC_SCOUT_SYMBOLS = ["sdf_scout_active_blocks_static", "sdf_scout_static_max_blocks"]
 ENGINE_SYMBOLS = ["sdf_engine_create", "sdf_engine_destroy", "sdf_engine_configure", "sdf_engine_set_scene",
                   "sdf_engine_extract", "sdf_engine_set_timing", "sdf_engine_set_debug", "sdf_engine_get_bvh",
                   "sdf_engine_buffer", "sdf_engine_read_buffer", "sdf_engine_eval", "sdf_engine_eval_distance", "sdf_engine_eval_normals", "sdf_engine_count_work", "sdf_measure_fp32_peak", "sdf_extract", "sdf_last_error", "sdf_version"]
@@ -132,6 +133,9 @@ def lib():
     L.sdf_extract.argtypes = [vp, i, ctypes.POINTER(SdfConfig), f, ctypes.POINTER(SdfOutputs), vp,
                               ctypes.POINTER(SdfStats)]
     L.sdf_extract.restype = i
+    L.sdf_scout_active_blocks_static.argtypes = [G, f]
+    L.sdf_scout_active_blocks_static.restype = i
+    L.sdf_scout_static_max_blocks.restype = u
     L.sdf_last_error.restype = i
     L.sdf_version.restype = ctypes.c_char_p
     _lib = L

@@ -346,3 +346,4 @@ const char* sdf_version(void) { return "sdfmesh_b200 0.1 (sm_100a)"; }
 }  // extern "C"
 
 #include "engine.inl"
+#include "noalloc.inl"

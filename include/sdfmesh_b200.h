@@ -271,6 +271,19 @@ sdf_status sdf_measure_fp32_peak(double* tflops);
 sdf_status sdf_extract(const sdf_primitive* prims, int count, const sdf_config* cfg, float time,
                        const sdf_outputs* out, void* stream, sdf_stats* stats);
 
+/* The active-block scout of launchScoutActiveBlocks without any device allocation (this entry point
+ * has no counterpart in the reference). For callers that must not let a library call cudaMalloc /
+ * cudaFree - a per-frame render loop or plugin host that forbids device allocation (both calls
+ * synchronise the device and can fail under the host's fixed memory budget), or an application that
+ * owns every allocation through its own allocator. Its working memory is one static device array of
+ * the library (a little over 4 MiB, held by every device that loads the library until exit).
+ * Limit: sdf_scout_static_max_blocks() 8^3 blocks (1,048,576); larger grids return SDF_ERR_CAPACITY.
+ * The first call on a device looks up the array's device address with that device current; make it
+ * before any stream capture there. Calls share the array: calls that overlap on the GPU race.
+ * Runs on the legacy default stream, like launchScoutActiveBlocks; same outputs. */
+sdf_status sdf_scout_active_blocks_static(sdf_grid* grid, float time);
+unsigned int sdf_scout_static_max_blocks(void);
+
 /* First CUDA error recorded by a drop-in launcher since the last call (cleared on read). */
 int sdf_last_error(void);
 /* Library version string. */
