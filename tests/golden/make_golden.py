@@ -282,6 +282,19 @@ def run_pipeline(prims, res, technique, out_mask, t=0.0, qef_blend=1.0, max_vert
     return d
 
 
+def single_type_scene(t, n, seed):
+    rng = np.random.default_rng(seed)
+    p = S.random_scene(n, seed, size_range=(0.1, 0.35), center_range=0.6)
+    p["type"] = t
+    p["operation"] = rng.choice([S.SDF_UNION, S.SDF_UNION_BLEND], n)
+    p["blendFactor"] = rng.uniform(0.02, 0.2, n)
+    prm = sd_params(rng, t, n)
+    p["params"] = prm
+    p["annular"] = np.where(rng.random(n) < 0.25, rng.uniform(0, 0.03, n), 0)
+    p["rounding"] = np.where(rng.random(n) < 0.25, rng.uniform(0, 0.03, n), 0)
+    return p
+
+
 def mixed_scene_notrig(seed, n):
     """Every primitive type without transcendentals (the cone calls sinf/cosf), every operation,
     annular/rounding shells; no displacement."""
@@ -304,9 +317,21 @@ def main():
     ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
     ap.add_argument("--skip-full", action="store_true", help="skip the full-size digests")
     ap.add_argument("--only-odd", action="store_true", help="only the non-power-of-two grid fixtures")
+    ap.add_argument("--only-types", action="store_true", help="only the per-primitive-type fixtures")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     t0 = time.time()
+    # one marching-cubes run per primitive type: union scenes of that type only, random transforms,
+    # annular / rounding shells on some primitives (pins the per-type arithmetic inside the reference's
+    # 8-corner evaluation, which can contract differently than a lone map() call)
+    for t in list(range(0, 13)) + [14]:
+        prims = single_type_scene(t, 24, S.SEED_BASE + 300 + t)
+        d = run_pipeline(prims, 48, 0, R.OUT_ALL, 0.0)
+        np.savez_compressed(os.path.join(args.out, f"mc_type{t}_48.npz"), prims=prims, res=np.int32(48),
+                            technique=np.int32(0), out_mask=np.int32(R.OUT_ALL), time=np.float32(0.0), **d)
+        print(f"mc_type{t}_48", json.loads(d["stats"])["totalVertices"], time.time() - t0, flush=True)
+    if args.only_types:
+        return
     # grids whose cell size is not a power of two and whose origin is not -1: here the products
     # i * cellSize round, so these pin how grid points are formed
     odd_bmin, odd_bmax = (-1.1, -1.05, -1.0), (1.1, 1.0, 1.05)
