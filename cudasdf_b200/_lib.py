@@ -37,7 +37,24 @@ class SdfStats(ctypes.Structure):
                 ("total_vertices", ctypes.c_int64), ("written_vertices", ctypes.c_int64),
                 ("dc_cell_vertices", ctypes.c_int64), ("bvh_cap_hits", ctypes.c_int64),
                 ("ms_scout", ctypes.c_float), ("ms_field", ctypes.c_float), ("ms_scan", ctypes.c_float),
-                ("ms_emit", ctypes.c_float), ("ms_total", ctypes.c_float)]
+                ("ms_emit", ctypes.c_float), ("ms_total", ctypes.c_float), ("scouted_blocks", ctypes.c_int64)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class SurrogateConfig(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_int32), ("validation", ctypes.c_int32), ("steps", ctypes.c_int32),
+                ("batch", ctypes.c_int32), ("lr", ctypes.c_float), ("freq_sigma", ctypes.c_float),
+                ("surface_sigma", ctypes.c_float), ("clamp", ctypes.c_float), ("surface_res", ctypes.c_int32),
+                ("slack_cells", ctypes.c_float), ("time", ctypes.c_float), ("seed", ctypes.c_uint32)]
+
+
+class SurrogateStats(ctypes.Structure):
+    _fields_ = [("final_loss", ctypes.c_float), ("eps_max", ctypes.c_float), ("eps_cert", ctypes.c_float),
+                ("margin", ctypes.c_float),
+                ("surface_points", ctypes.c_int32), ("ms_samples", ctypes.c_float), ("ms_train", ctypes.c_float),
+                ("ms_certify", ctypes.c_float)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -69,6 +86,9 @@ DROPIN_SYMBOLS = ["launchScoutActiveBlocks", "launchCountActiveBlockTriangles", 
                   "launchBuildBlockToActiveMap", "launchDCMarkCells", "launchDCSolveCellVertices",
                   "launchDCRecomputeNormalsAtVertices", "launchDCSmoothCellNormals", "launchDCCountQuads",
                   "launchDCGenerateQuads", "getScanStorageSize", "launchScan"]
+SURROGATE_SYMBOLS = ["sdf_surrogate_default_config", "sdf_surrogate_train", "sdf_surrogate_enable",
+                     "sdf_surrogate_audit", "sdf_surrogate_num_params", "sdf_surrogate_set_params",
+                     "sdf_surrogate_get_params", "sdf_surrogate_forward", "sdf_surrogate_gradient"]
 STATIC_SCOUT_SYMBOLS = ["sdf_scout_active_blocks_static", "sdf_scout_static_max_blocks"]
 ENGINE_SYMBOLS = ["sdf_engine_create", "sdf_engine_destroy", "sdf_engine_configure", "sdf_engine_set_scene",
                   "sdf_engine_extract", "sdf_engine_set_timing", "sdf_engine_set_debug", "sdf_engine_get_bvh",
@@ -133,6 +153,24 @@ def lib():
     L.sdf_extract.argtypes = [vp, i, ctypes.POINTER(SdfConfig), f, ctypes.POINTER(SdfOutputs), vp,
                               ctypes.POINTER(SdfStats)]
     L.sdf_extract.restype = i
+    L.sdf_surrogate_default_config.argtypes = [ctypes.POINTER(SurrogateConfig)]
+    L.sdf_surrogate_default_config.restype = None
+    L.sdf_surrogate_train.argtypes = [vp, ctypes.POINTER(SurrogateConfig), ctypes.POINTER(SurrogateStats)]
+    L.sdf_surrogate_train.restype = i
+    L.sdf_surrogate_enable.argtypes = [vp, i]
+    L.sdf_surrogate_enable.restype = i
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    L.sdf_surrogate_audit.argtypes = [vp, f, i64p, i64p, i64p]
+    L.sdf_surrogate_audit.restype = i
+    L.sdf_surrogate_num_params.restype = i
+    L.sdf_surrogate_set_params.argtypes = [vp, vp, vp, vp]
+    L.sdf_surrogate_set_params.restype = i
+    L.sdf_surrogate_get_params.argtypes = [vp, vp, vp, vp]
+    L.sdf_surrogate_get_params.restype = i
+    L.sdf_surrogate_forward.argtypes = [vp, vp, i, vp, vp]
+    L.sdf_surrogate_forward.restype = i
+    L.sdf_surrogate_gradient.argtypes = [vp, vp, vp, i, vp, vp]
+    L.sdf_surrogate_gradient.restype = i
     L.sdf_scout_active_blocks_static.argtypes = [G, f]
     L.sdf_scout_active_blocks_static.restype = i
     L.sdf_scout_static_max_blocks.restype = u

@@ -20,6 +20,49 @@ struct Ctrl {
     Diag diag;
 };
 
+// learned-surrogate state of an engine (device parameters, optimiser moments, work buffers)
+struct SurrogateState {
+    float* theta = nullptr;
+    float* m1 = nullptr;
+    float* m2 = nullptr;
+    __nv_bfloat16* wbf = nullptr;
+    float* freq = nullptr;
+    float* partial = nullptr;       // per-CTA gradient partials
+    int partial_rows = 0;
+    float* loss_partial = nullptr;
+    float* grad = nullptr;
+    int* error = nullptr;
+    float* coarse_f = nullptr;      // f_net at the coarse block centres
+    size_t coarse_cap = 0;
+    unsigned long long* counters = nullptr;  // audit counters
+    float io[7] = {0.f, 0.f, 0.f, 1.f, 1.f, 1.f, 0.25f};
+    bool has_params = false;
+    bool certified = false;
+    bool enabled = false;
+    float eps = 0.f;
+    float slack_cells = 2.f;
+
+    ~SurrogateState() {
+        void* ptrs[] = {theta, m1, m2, wbf, freq, partial, loss_partial, grad, error, coarse_f, counters};
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+    }
+    sur::NetView view() const {
+        sur::NetView v;
+        v.theta = theta;
+        v.wbf = wbf;
+        v.freq = freq;
+        v.cx = io[0]; v.cy = io[1]; v.cz = io[2];
+        v.sx = io[3]; v.sy = io[4]; v.sz = io[5];
+        v.clamp = io[6];
+        return v;
+    }
+};
+
+// coarse blocks of the culled scout: 4 x 4 x 4 blocks of 8^3 cells (32^3 cells), two scout bricks
+constexpr int SUR_SPAN_BLOCKS = 4;
+constexpr int SUR_SPAN_CELLS = 8 * SUR_SPAN_BLOCKS;
+
 struct EngineImpl {
     int device = 0;
     sdf_config cfg;
@@ -58,6 +101,8 @@ struct EngineImpl {
     cudaEvent_t ev[8] = {};
     size_t packet_cap = 0;
     Diag* eval_diag = nullptr;
+    std::vector<sdf_primitive> scene;  // the primitives as given (the surrogate's surface run uses them)
+    SurrogateState* sur = nullptr;
 
     ~EngineImpl() { release(); }
 
@@ -76,6 +121,8 @@ struct EngineImpl {
         h_ctrl = nullptr;
         for (auto& e : ev)
             if (e) { cudaEventDestroy(e); e = nullptr; }
+        delete sur;
+        sur = nullptr;
     }
 };
 
@@ -108,6 +155,63 @@ static sdf_status engine_ensure_packets(EngineImpl& E, size_t cells) {
     if (s == SDF_OK) s = sdfb::dev_alloc(E.dc_voff, cells);
     E.packet_cap = s == SDF_OK ? cells : 0;
     return s;
+}
+
+// the grid-dependent part K of the cull margin: coarse half-diagonal + scout radius + slack
+static float surrogate_reach(const EngineImpl& E, float slack_cells) {
+    using namespace sdfb;
+    const float cell = E.gv.cell;
+    const float r_scout = (8 * 0.5f * 1.73205f + 2.0f) * cell;
+    return 0.5f * (float)SUR_SPAN_CELLS * 1.7320508f * cell + r_scout + slack_cells * cell;
+}
+
+static float surrogate_margin(const EngineImpl& E) { return E.sur->eps + surrogate_reach(E, E.sur->slack_cells); }
+
+static void coarse_dims(const EngineImpl& E, int& cx, int& cy, int& cz) {
+    using namespace sdfb;
+    cx = (E.gv.bx + SUR_SPAN_BLOCKS - 1) / SUR_SPAN_BLOCKS;
+    cy = (E.gv.by + SUR_SPAN_BLOCKS - 1) / SUR_SPAN_BLOCKS;
+    cz = (E.gv.bz + SUR_SPAN_BLOCKS - 1) / SUR_SPAN_BLOCKS;
+}
+
+// f_net at the coarse block centres into E.sur->coarse_f
+static sdf_status surrogate_coarse_eval(EngineImpl& E, cudaStream_t st) {
+    using namespace sdfb;
+    SurrogateState& S = *E.sur;
+    int cx, cy, cz;
+    coarse_dims(E, cx, cy, cz);
+    const size_t nc = (size_t)cx * cy * cz;
+    if (S.coarse_cap < nc) {
+        if (dev_alloc(S.coarse_f, nc) != SDF_OK) return SDF_ERR_NOMEM;
+        S.coarse_cap = nc;
+    }
+    sur::CoarseCentres cc;
+    cc.ox = E.gv.ox; cc.oy = E.gv.oy; cc.oz = E.gv.oz; cc.cell = E.gv.cell;
+    cc.cx = cx; cc.cy = cy; cc.cz = cz; cc.span = SUR_SPAN_CELLS;
+    cc.n = (int)nc;
+    const size_t smem = sizeof(sur::InferSmem);
+    const int tiles = (int)((nc + sur::TILE - 1) / sur::TILE);
+    sur::k_sur_infer<sur::CoarseCentres><<<persistent_grid(sur::k_sur_infer<sur::CoarseCentres>, sur::TILE, tiles, smem),
+                                      sur::TILE, smem, st>>>(S.view(), cc, S.coarse_f, S.error);
+    check_launch();
+    return SDF_OK;
+}
+
+// the scout of run_scout_compact, skipping the coarse blocks the surrogate culls
+static void run_culled_scout_compact(EngineImpl& E, const sdfb::SceneView& sv, float time, unsigned long long* status,
+                                     sdfb::Ctrl* ctrl, cudaStream_t st) {
+    using namespace sdfb;
+    const GridView& gv = E.gv;
+    surrogate_coarse_eval(E, st);
+    const int nbricks = ((gv.bx + 3) / 4) * ((gv.by + 3) / 4) * ((gv.bz + 1) / 2);
+    const int warps_per_cta = BLK_THREADS / 32;
+    k_scout_t<true><<<(nbricks + warps_per_cta - 1) / warps_per_cta, BLK_THREADS, 0, st>>>(
+        gv, sv, time, E.flags, &ctrl->diag, E.sur->coarse_f, surrogate_margin(E));
+    check_launch();
+    const unsigned tiles = scan_tiles((unsigned)E.nblocks);
+    k_compact<<<std::max(1u, tiles), SCAN_THREADS, 0, st>>>(E.flags, (unsigned)E.nblocks, E.list, &ctrl->active_count,
+                                                          scan_state(status), &ctrl->diag);
+    check_launch();
 }
 
 extern "C" {
@@ -195,8 +299,16 @@ sdf_status sdf_engine_set_scene(sdf_engine* e, const sdf_primitive* prims, int c
     if (!e || count < 0 || (count > 0 && !prims)) return SDF_ERR_INVALID;
     EngineImpl& E = e->impl;
     cudaSetDevice(E.device);
-    E.nbvh = sdfb::prepare_scene(prims, count, E.sorted, E.nodes);
-    E.depth = sdfb::bvh_depth(E.nodes);
+    // an unchanged scene (byte-identical primitives) keeps its host BVH and its trained surrogate; the
+    // upload below still runs
+    const bool same = count > 0 && E.scene.size() == (size_t)count && E.d_prims &&
+                      memcmp(E.scene.data(), prims, (size_t)count * sizeof(sdf_primitive)) == 0;
+    if (!same) {
+        E.scene.assign(prims, prims + count);
+        if (E.sur) E.sur->certified = E.sur->enabled = false;  // a new scene needs a new surrogate
+        E.nbvh = sdfb::prepare_scene(prims, count, E.sorted, E.nodes);
+        E.depth = sdfb::bvh_depth(E.nodes);
+    }
     if (E.depth + 1 > sdfb::MAP_STACK) return SDF_ERR_STACK;
     if (E.prims_cap < E.sorted.size()) {
         if (sdfb::dev_alloc(E.d_prims, E.sorted.size() * 2) != SDF_OK) return SDF_ERR_NOMEM;
@@ -266,7 +378,11 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
     const GridView gv = E.gv;
     Diag* diag = &ctrl->diag;
     const int nb = E.nblocks;
-    run_scout_compact(gv, sv, time, E.flags, scanA, E.list, &ctrl->active_count, diag, st);
+    const bool culled = E.sur && E.sur->enabled;
+    if (culled)
+        run_culled_scout_compact(E, sv, time, scanA, ctrl, st);
+    else
+        run_scout_compact(gv, sv, time, E.flags, scanA, E.list, &ctrl->active_count, diag, st);
     if (E.timing) cudaEventRecord(E.ev[1], st);
     ActiveView av{E.list, &ctrl->active_count, nb};
     MeshOut mo;
@@ -360,6 +476,7 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
         stats->written_vertices = std::min<int64_t>(h.total_vertices, out->max_vertices);
         stats->dc_cell_vertices = h.dc_vertices;
         stats->bvh_cap_hits = (int64_t)h.diag.cap_hits;
+        stats->scouted_blocks = culled ? (int64_t)h.diag.scouted : (int64_t)nb;
         stats->ms_total = std::chrono::duration<float, std::milli>(t1 - t0).count();
         if (E.timing) {
             cudaEventElapsedTime(&stats->ms_scout, E.ev[0], E.ev[1]);

@@ -152,8 +152,13 @@ __device__ __forceinline__ CellInfo cell_info(const GridView& g, int bx, int by,
 // centres of a warp are spatially close and their BVH walks coincide; the result is a 0/1 flag per
 // linear block index, compacted in index order afterwards.
 // ------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(BLK_THREADS) k_scout(GridView g, SceneView sc, float time, unsigned* flags,
-                                                       Diag* diag) {
+// CULL: the brick lies in coarse block (wx, wy, wz / 2) of 4 x 4 x 4 blocks (32^3 cells); when the
+// surrogate's value at that coarse block's centre exceeds `margin` in magnitude, the brick's blocks
+// are marked inactive without evaluating the scene.
+template <bool CULL>
+__global__ void __launch_bounds__(BLK_THREADS) k_scout_t(GridView g, SceneView sc, float time, unsigned* flags,
+                                                         Diag* diag, const float* __restrict__ coarse_f,
+                                                         float margin) {
     const int lane = threadIdx.x & 31;
     const int warp_global = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int nbx = (g.bx + 3) >> 2, nby = (g.by + 3) >> 2, nbz = (g.bz + 1) >> 1;
@@ -161,6 +166,15 @@ __global__ void __launch_bounds__(BLK_THREADS) k_scout(GridView g, SceneView sc,
     const int wx = warp_global % nbx, t = warp_global / nbx, wy = t % nby, wz = t / nby;
     const int bx = wx * 4 + (lane & 3), by = wy * 4 + ((lane >> 2) & 3), bz = wz * 2 + (lane >> 4);
     const bool valid = bx < g.bx && by < g.by && bz < g.bz;
+    if (CULL) {
+        const float fc = coarse_f[wx + nbx * (wy + nby * (wz >> 1))];
+        if (fabsf(fc) > margin) {
+            if (valid) flags[bx + g.bx * (by + g.by * bz)] = 0u;
+            return;
+        }
+        const unsigned v = __ballot_sync(0xffffffffu, valid);
+        if (lane == 0) atomicAdd(&diag->scouted, (unsigned long long)__popc(v));
+    }
     const float3 c = f3(FMA(ADD((float)(bx * 8), 4.f), g.cell, g.ox), FMA(ADD((float)(by * 8), 4.f), g.cell, g.oy),
                         FMA(ADD((float)(bz * 8), 4.f), g.cell, g.oz));
     MapState<false> st;

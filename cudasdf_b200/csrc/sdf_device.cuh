@@ -344,6 +344,7 @@ struct Diag {
     unsigned long long node_pops;   // work counters (counting runs only): per-point popped nodes,
     unsigned long long leaf_evals;  //   per-point primitive evaluations,
     unsigned long long points;      //   evaluated points
+    unsigned long long scouted;     // blocks the surrogate-culled scout evaluated exactly
     int stack_overflow;             // a search needed more than 64 stack entries
     int timeout;                    // a bounded wait gave up
 };

@@ -17,6 +17,7 @@
 #include "bvh_host.h"
 #include "mc_kernels.cuh"
 #include "dc_kernels.cuh"
+#include "surrogate.cuh"
 
 namespace sdfb {
 
@@ -140,7 +141,8 @@ static void run_scout_compact(const GridView& gv, const SceneView& sv, float tim
     const int nblocks = gv.bx * gv.by * gv.bz;
     const int nbricks = ((gv.bx + 3) / 4) * ((gv.by + 3) / 4) * ((gv.bz + 1) / 2);
     const int warps_per_cta = BLK_THREADS / 32;
-    k_scout<<<(nbricks + warps_per_cta - 1) / warps_per_cta, BLK_THREADS, 0, stream>>>(gv, sv, time, flags, diag);
+    k_scout_t<false><<<(nbricks + warps_per_cta - 1) / warps_per_cta, BLK_THREADS, 0, stream>>>(gv, sv, time, flags, diag,
+                                                                                          nullptr, 0.f);
     check_launch();
     const unsigned tiles = scan_tiles((unsigned)nblocks);
     record(cudaMemsetAsync(status, 0, (tiles + 1) * sizeof(unsigned long long), stream));
@@ -346,4 +348,5 @@ const char* sdf_version(void) { return "sdfmesh_b200 0.1 (sm_100a)"; }
 }  // extern "C"
 
 #include "engine.inl"
+#include "surrogate.inl"
 #include "noalloc.inl"

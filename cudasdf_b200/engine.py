@@ -139,6 +139,67 @@ class Engine:
                 "sdf_engine_eval_normals")
         return out
 
+    # ---- learned surrogate (sdf_surrogate_* in include/sdfmesh_b200.h) ----
+    @staticmethod
+    def surrogate_config(**overrides) -> L.SurrogateConfig:
+        c = L.SurrogateConfig()
+        L.lib().sdf_surrogate_default_config(ctypes.byref(c))
+        for k, v in overrides.items():
+            setattr(c, k, v)
+        return c
+
+    def surrogate_train(self, cfg: L.SurrogateConfig = None) -> dict:
+        cfg = cfg or self.surrogate_config()
+        st = L.SurrogateStats()
+        L.check(self._lib.sdf_surrogate_train(self.h, ctypes.byref(cfg), ctypes.byref(st)), "sdf_surrogate_train")
+        return st.as_dict()
+
+    def surrogate_enable(self, on: bool):
+        L.check(self._lib.sdf_surrogate_enable(self.h, 1 if on else 0), "sdf_surrogate_enable")
+
+    def surrogate_audit(self, time: float = 0.0) -> dict:
+        v, c, n = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        L.check(self._lib.sdf_surrogate_audit(self.h, float(time), ctypes.byref(v), ctypes.byref(c), ctypes.byref(n)),
+                "sdf_surrogate_audit")
+        return {"violations": v.value, "culled_coarse": c.value, "coarse_blocks": n.value}
+
+    def surrogate_set_params(self, theta, freq, io):
+        th = np.ascontiguousarray(theta, np.float32)
+        fr = np.ascontiguousarray(freq, np.float32)
+        iv = np.ascontiguousarray(io, np.float32)
+        assert th.size == self._lib.sdf_surrogate_num_params() and fr.size == 96 and iv.size == 7
+        L.check(self._lib.sdf_surrogate_set_params(self.h, th.ctypes.data, fr.ctypes.data, iv.ctypes.data),
+                "sdf_surrogate_set_params")
+
+    def surrogate_get_params(self):
+        th = np.zeros(self._lib.sdf_surrogate_num_params(), np.float32)
+        fr = np.zeros(96, np.float32)
+        iv = np.zeros(7, np.float32)
+        L.check(self._lib.sdf_surrogate_get_params(self.h, th.ctypes.data, fr.ctypes.data, iv.ctypes.data),
+                "sdf_surrogate_get_params")
+        return th, fr.reshape(32, 3), iv
+
+    def surrogate_forward(self, points, stream=None):
+        """f_net at device points (torch float32 (n, 3)); returns a (n,) device tensor."""
+        import torch
+        pts = points.contiguous()
+        out = torch.empty((pts.shape[0],), dtype=torch.float32, device=pts.device)
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        L.check(self._lib.sdf_surrogate_forward(self.h, ctypes.c_void_p(pts.data_ptr()), int(pts.shape[0]),
+                                                ctypes.c_void_p(out.data_ptr()), sp), "sdf_surrogate_forward")
+        return out
+
+    def surrogate_gradient(self, points, targets):
+        """Gradient of the mean squared error over device samples (no update): (grad numpy, loss)."""
+        pts = points.contiguous()
+        tg = targets.contiguous()
+        g = np.zeros(self._lib.sdf_surrogate_num_params(), np.float32)
+        loss = ctypes.c_float()
+        L.check(self._lib.sdf_surrogate_gradient(self.h, ctypes.c_void_p(pts.data_ptr()), ctypes.c_void_p(tg.data_ptr()),
+                                                 int(pts.shape[0]), g.ctypes.data, ctypes.byref(loss)),
+                "sdf_surrogate_gradient")
+        return g, loss.value
+
     def bvh(self):
         nb = ctypes.c_int(0)
         n = self._lib.sdf_engine_get_bvh(self.h, None, 0, ctypes.byref(nb))

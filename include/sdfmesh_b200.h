@@ -219,6 +219,7 @@ typedef struct sdf_stats {
     int64_t dc_cell_vertices;
     int64_t bvh_cap_hits;       /* points whose traversal stopped at the 256-visit cap */
     float ms_scout, ms_field, ms_scan, ms_emit, ms_total; /* filled when timing is enabled */
+    int64_t scouted_blocks;     /* blocks whose centre the exact scout evaluated (all, unless culled) */
 } sdf_stats;
 
 typedef struct sdf_engine sdf_engine;
@@ -283,6 +284,71 @@ sdf_status sdf_extract(const sdf_primitive* prims, int count, const sdf_config* 
  * Runs on the legacy default stream, like launchScoutActiveBlocks; same outputs. */
 sdf_status sdf_scout_active_blocks_static(sdf_grid* grid, float time);
 unsigned int sdf_scout_static_max_blocks(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Learned surrogate culling (no counterpart in the reference). A Fourier-feature MLP
+ * (3 -> 32 frequencies -> 64 features -> 4 x 64 SiLU -> 1; BF16 weights, FP32 accumulation) is trained
+ * on the GPU by the library's own tensor-core forward/backward kernels on samples of the current
+ * scene's exact distance (targets clamped to +-clamp). With
+ *     K = 16 * sqrt(3) * cell + r_scout + slack_cells * cell,
+ * r_scout = (8 * 0.5 * 1.73205 + 2) * cell the scout's own radius (MarchingCubesKernels.cu:874), the
+ * certified error eps is the smallest value such that every held-out sample with |f_net| > eps + K
+ * has |f_net - clamp(f)| <= eps (errors where the network is near zero never cull anything, so they do
+ * not enter), and the cull margin is eps + K.
+ * With culling enabled, sdf_engine_extract skips the exact scout inside every coarse block of
+ * 32^3 cells (4 x 4 x 4 blocks) whose centre has |f_net| > margin; every kept block runs the exact path, so
+ * the mesh is the plain extraction's whenever no culled coarse block holds an active block, which
+ * sdf_surrogate_audit checks against a full exact scout.
+ * --------------------------------------------------------------------------------------------- */
+typedef struct sdf_surrogate_config {
+    int32_t samples;            /* training samples (half uniform in the bounds, half near the surface) */
+    int32_t validation;         /* held-out samples for the certificate */
+    int32_t steps;              /* Adam steps */
+    int32_t batch;              /* samples per step */
+    float lr;                   /* peak learning rate (cosine decay to 2 %) */
+    float freq_sigma;           /* standard deviation of the Fourier frequencies (unit: per half extent) */
+    float surface_sigma;        /* standard deviation of the offsets around surface points */
+    float clamp;                /* distance targets are clamped to [-clamp, clamp] */
+    int32_t surface_res;        /* resolution of the coarse marching-cubes run that supplies surface points */
+    float slack_cells;          /* extra cull margin, in cells */
+    float time;                 /* scene time the samples are taken at */
+    uint32_t seed;
+} sdf_surrogate_config;
+
+typedef struct sdf_surrogate_stats {
+    float final_loss;           /* mean squared error of the last step */
+    float eps_max;              /* max |f_net - clamp(f)| over all held-out samples */
+    float eps_cert;             /* the certified error used by the margin (see above) */
+    float margin;               /* cull threshold at the configured grid (eps_cert + K) */
+    int32_t surface_points;     /* vertices of the coarse run */
+    float ms_samples, ms_train, ms_certify;
+} sdf_surrogate_stats;
+
+/* Fills *cfg with the defaults (2,000,000 samples, 262,144 held out, 1,500 steps of 65,536, lr 2e-3,
+ * frequencies N(0, 2^2), surface offsets N(0, 0.01^2), clamp 0.25, surface run at 128 samples per
+ * axis, 2 cells of slack, time 0, seed 1). */
+void sdf_surrogate_default_config(sdf_surrogate_config* cfg);
+/* Trains the surrogate for the current scene and grid and certifies it; synchronous. */
+sdf_status sdf_surrogate_train(sdf_engine* e, const sdf_surrogate_config* cfg, sdf_surrogate_stats* stats);
+/* Turns surrogate culling in sdf_engine_extract on or off (SDF_ERR_INVALID if not trained). */
+sdf_status sdf_surrogate_enable(sdf_engine* e, int enabled);
+/* Exact audit: a full exact scout at `time`; *violations = exact-active blocks inside culled coarse
+ * blocks (0 means the culled extraction equals the plain one), *culled = culled coarse blocks,
+ * *coarse = all coarse blocks. Synchronous. */
+sdf_status sdf_surrogate_audit(sdf_engine* e, float time, int64_t* violations, int64_t* culled, int64_t* coarse);
+/* Number of trainable parameters (hidden W[4][64][64] out x in, b[4][64], w5[64], b5). */
+int sdf_surrogate_num_params(void);
+/* Parameters: theta (sdf_surrogate_num_params() floats, the order above), freq (32 x 3 floats) and
+ * io = {centre x, y, z, scale x, y, z, clamp}; features use (p - centre) * scale. */
+sdf_status sdf_surrogate_set_params(sdf_engine* e, const float* theta, const float* freq, const float io[7]);
+sdf_status sdf_surrogate_get_params(sdf_engine* e, float* theta, float* freq, float io[7]);
+/* f_net at n device points (x, y, z floats) into d_out (n floats). Asynchronous on `stream`. */
+sdf_status sdf_surrogate_forward(sdf_engine* e, const float* d_points, int n, float* d_out, void* stream);
+/* One forward + backward pass over n device samples (points, targets) without an update: writes the
+ * gradient of mean((f_net - clamp(target))^2) into h_grad (num_params floats, host) and the loss into
+ * *h_loss. Synchronous. */
+sdf_status sdf_surrogate_gradient(sdf_engine* e, const float* d_points, const float* d_targets, int n, float* h_grad,
+                                  float* h_loss);
 
 /* First CUDA error recorded by a drop-in launcher since the last call (cleared on read). */
 int sdf_last_error(void);

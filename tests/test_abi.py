@@ -13,7 +13,7 @@ HEADER = os.path.join(ROOT, "include", "sdfmesh_b200.h")
 def declared_functions():
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\**\s+\**([A-Za-z_][A-Za-z0-9_]*)\s*\(", text, re.M)
+    names = re.findall(r"^\s*(?:const\s+)?(?:unsigned\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\**\s+\**([A-Za-z_][A-Za-z0-9_]*)\s*\(", text, re.M)
     return sorted(set(n for n in names if n not in ("if", "return")))
 
 
@@ -33,7 +33,8 @@ def test_library_exports_every_declared_symbol():
     L = _lib.lib()
     missing = [n for n in declared_functions() if not hasattr(L, n)]
     assert not missing, missing
-    assert set(_lib.DROPIN_SYMBOLS + _lib.ENGINE_SYMBOLS) <= set(declared_functions())
+    assert set(_lib.DROPIN_SYMBOLS + _lib.ENGINE_SYMBOLS + _lib.SURROGATE_SYMBOLS +
+               _lib.STATIC_SCOUT_SYMBOLS) <= set(declared_functions())
     assert L.sdf_version().startswith(b"sdfmesh_b200")
 
 
@@ -47,13 +48,24 @@ def test_struct_layouts_match_reference():
 
 
 def test_header_compiles_as_c():
+    """The header is plain C11, and its structs have the sizes the Python bindings assume."""
     import subprocess
     import tempfile
-    src = '#include "sdfmesh_b200.h"\nint main(void){ sdf_grid g; (void)g; return sizeof(sdf_primitive) == 160 ? 0 : 1; }\n'
+
+    from cudasdf_b200 import _lib
+    structs = {"sdf_config": _lib.SdfConfig, "sdf_outputs": _lib.SdfOutputs, "sdf_stats": _lib.SdfStats,
+               "sdf_surrogate_config": _lib.SurrogateConfig, "sdf_surrogate_stats": _lib.SurrogateStats,
+               "sdf_grid": _lib.SdfGrid}
+    body = "".join(f'printf("%zu\\n", sizeof({n}));' for n in structs)
+    src = ('#include <stdio.h>\n#include "sdfmesh_b200.h"\n'
+           'int main(void){ if (sizeof(sdf_primitive) != 160) return 1; ' + body + ' return 0; }\n')
     with tempfile.TemporaryDirectory() as d:
         c = os.path.join(d, "t.c")
         open(c, "w").write(src)
         r = subprocess.run(["/usr/bin/gcc", "-std=c11", "-Wall", "-I", os.path.dirname(HEADER), c, "-o",
                             os.path.join(d, "t")], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
-        assert subprocess.run([os.path.join(d, "t")]).returncode == 0
+        out = subprocess.run([os.path.join(d, "t")], capture_output=True, text=True)
+        assert out.returncode == 0
+        sizes = [int(x) for x in out.stdout.split()]
+        assert sizes == [ctypes.sizeof(t) for t in structs.values()], dict(zip(structs, sizes))
