@@ -228,12 +228,14 @@ def count_work(eng, buf, res):
     import ctypes
 
     from cudasdf_b200 import _lib as L
-    c = (ctypes.c_ulonglong * 4)()
+    c = (ctypes.c_ulonglong * 8)()
     rc = L.lib().sdf_engine_count_work(eng.h, ctypes.byref(c))
     if rc != 0:
         return None
     return {"field_node_visits": int(c[0]), "field_leaf_evals": int(c[1]), "field_points": int(c[2]),
-            "field_ms": None}
+            "warp_pops": int(c[4]), "warp_box_tests": int(c[5]), "warp_leaf_steps": int(c[6]),
+            "lane_efficiency_pops": int(c[0]) / max(32 * int(c[4]), 1),
+            "lane_efficiency_leaves": int(c[1]) / max(32 * int(c[6]), 1)}
 
 
 def cpu_baseline(args):

@@ -401,9 +401,12 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
     if (!out->normals) mask &= ~OUT_NORMALS;
 
     if (!dc) {
-        k_mc_field<<<persistent_grid(k_mc_field, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(
-            gv, sv, time, av, E.fields, E.block_totals, (E.debug & 1) ? E.packet_counts : nullptr, &ctrl->tickets[0],
-            diag);
+        k_field_own<false><<<persistent_grid(k_field_own<false>, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(
+            gv, sv, time, av, E.fields, E.b2a, &ctrl->tickets[0], diag);
+        check_launch();
+        k_field_halo<false><<<persistent_grid(k_field_halo<false>, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(
+            gv, sv, time, av, E.fields, E.b2a, E.flags, E.block_totals, (E.debug & 1) ? E.packet_counts : nullptr,
+            &ctrl->tickets[3], diag);
         check_launch();
         if (E.timing) cudaEventRecord(E.ev[2], st);
         k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)nb)), SCAN_THREADS, 0, st>>>(
@@ -576,7 +579,7 @@ sdf_status sdf_engine_eval(sdf_engine* e, const float* d_points, int n, float ti
     return err == cudaSuccess ? SDF_OK : SDF_ERR_CUDA;
 }
 
-sdf_status sdf_engine_count_work(sdf_engine* e, unsigned long long out[4]) {
+sdf_status sdf_engine_count_work(sdf_engine* e, unsigned long long out[8]) {
     using namespace sdfb;
     if (!e || !out) return SDF_ERR_INVALID;
     EngineImpl& E = e->impl;
@@ -594,8 +597,11 @@ sdf_status sdf_engine_count_work(sdf_engine* e, unsigned long long out[4]) {
     run_scout_compact(E.gv, sv, 0.f, E.flags, scanA, E.list, &ctrl->active_count, &ctrl->diag, 0);
     record(cudaMemsetAsync(&ctrl->diag, 0, sizeof(Diag), 0));
     ActiveView av{E.list, &ctrl->active_count, E.nblocks};
-    k_mc_field_count<<<persistent_grid(k_mc_field_count, BLK_THREADS, E.nblocks), BLK_THREADS>>>(
-        E.gv, sv, 0.f, av, nullptr, nullptr, nullptr, &ctrl->tickets[0], &ctrl->diag);
+    // the engine's block-field stage (own samples, then the halos no active block owns) with counters on
+    k_field_own<true><<<persistent_grid(k_field_own<true>, BLK_THREADS, E.nblocks), BLK_THREADS>>>(
+        E.gv, sv, 0.f, av, E.fields, E.b2a, &ctrl->tickets[0], &ctrl->diag);
+    k_field_halo<true><<<persistent_grid(k_field_halo<true>, BLK_THREADS, E.nblocks), BLK_THREADS>>>(
+        E.gv, sv, 0.f, av, E.fields, E.b2a, E.flags, nullptr, nullptr, &ctrl->tickets[3], &ctrl->diag);
     check_launch();
     Ctrl h;
     if (cudaMemcpy(&h, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost) != cudaSuccess) return SDF_ERR_CUDA;
@@ -603,6 +609,10 @@ sdf_status sdf_engine_count_work(sdf_engine* e, unsigned long long out[4]) {
     out[1] = h.diag.leaf_evals;
     out[2] = h.diag.points;
     out[3] = (unsigned long long)h.active_count;
+    out[4] = h.diag.warp_pops;
+    out[5] = h.diag.warp_tests;
+    out[6] = h.diag.warp_leaves;
+    out[7] = 0;
     return SDF_OK;
 }
 

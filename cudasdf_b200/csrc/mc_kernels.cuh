@@ -69,6 +69,28 @@ __device__ __forceinline__ int claim(unsigned* ticket, int n, int* s_item) {
     return *s_item;
 }
 
+// The block's 729 samples in Morton order of (x, y, z): the first 512 form sixteen 4 x 4 x 2 bricks of
+// 32, the +1 faces come as 8 x 4 slabs. Each warp takes 32 consecutive entries, so its points are
+// close together and share more of their BVH walks than a run of 32 in row order (9 x 4 x 1).
+struct FieldOrder {
+    unsigned short idx[FIELD_N];
+};
+constexpr FieldOrder make_field_order() {
+    FieldOrder o{};
+    int n = 0;
+    for (unsigned m = 0; m < 4096u; ++m) {
+        unsigned x = 0, y = 0, z = 0;
+        for (int b = 0; b < 4; ++b) {
+            x |= ((m >> (3 * b)) & 1u) << b;
+            y |= ((m >> (3 * b + 1)) & 1u) << b;
+            z |= ((m >> (3 * b + 2)) & 1u) << b;
+        }
+        if (x < 9 && y < 9 && z < 9) o.idx[n++] = (unsigned short)((z * 9 + y) * 9 + x);
+    }
+    return o;
+}
+__device__ const FieldOrder g_field_order = make_field_order();
+
 // 9^3 samples of block `lin` into s_field (index (z*9 + y)*9 + x); samples outside the grid are 0 and
 // never read by an in-bounds cell
 template <bool COUNT = false>
@@ -78,7 +100,8 @@ __device__ __forceinline__ void eval_block_field(const GridView& g, const SceneV
     block_coord(g, lin, bx, by, bz);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     for (int chunk = warp; chunk < FIELD_CHUNKS; chunk += nwarps) {
-        const int s = chunk * 32 + lane;
+        const int r = chunk * 32 + lane;
+        const int s = r < FIELD_N ? (int)g_field_order.idx[r] : r;
         const int sx = s % 9, sy = (s / 9) % 9, sz = s / 81;
         const int gx = bx * 8 + sx, gy = by * 8 + sy, gz = bz * 8 + sz;
         const bool valid = s < FIELD_N && gx < g.w && gy < g.h && gz < g.d;
@@ -186,6 +209,50 @@ __global__ void __launch_bounds__(BLK_THREADS) k_scout_t(GridView g, SceneView s
 // ------------------------------------------------------------------------------------------------
 // block field + per-cell counts
 // ------------------------------------------------------------------------------------------------
+// per-cell vertex counts of the block whose 9^3 field is in s_field (countActiveBlockTriangles,
+// MarchingCubesKernels.cu:914-970): optionally the whole field to fields_out, the per-cell counts in the
+// drop-in layout and the block total
+__device__ __forceinline__ void block_counts(const GridView& g, int a, int lin, float* s_field, unsigned* s_red,
+                                             float* __restrict__ fields_out, unsigned* __restrict__ block_totals,
+                                             unsigned* __restrict__ packet_counts) {
+    if (threadIdx.x < FIELD_STRIDE - FIELD_N) s_field[FIELD_N + threadIdx.x] = 0.f;
+    __syncthreads();
+    if (fields_out) {
+        float4* dst = reinterpret_cast<float4*>(fields_out + (size_t)a * FIELD_STRIDE);
+        const float4* src = reinterpret_cast<const float4*>(s_field);
+        for (int i = threadIdx.x; i < FIELD_STRIDE / 4; i += blockDim.x) dst[i] = src[i];
+    }
+    int bx, by, bz;
+    block_coord(g, lin, bx, by, bz);
+    unsigned cnt[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int tid = 2 * threadIdx.x + h;
+        const CellInfo c = cell_info(g, bx, by, bz, tid);
+        cnt[h] = 0;
+        if (!c.oob) {
+            float cv[8];
+            const int code = cell_case(s_field, c.lx, c.ly, c.lz, cv);
+            const unsigned long long word = c_mcCases[code];
+            cnt[h] = 3u * __popc(cell_valid_mask(g, c.x, c.y, c.z, cv, word));
+        }
+    }
+    if (packet_counts)
+        *reinterpret_cast<uint2*>(packet_counts + (size_t)a * 512 + 2 * threadIdx.x) = make_uint2(cnt[0], cnt[1]);
+    if (block_totals) {
+        unsigned v = cnt[0] + cnt[1];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned s = 0;
+            for (int w = 0; w < BLK_THREADS / 32; ++w) s += s_red[w];
+            block_totals[a] = s;
+        }
+    }
+}
+
 template <bool COUNT>
 __global__ void __launch_bounds__(BLK_THREADS) k_mc_field_t(GridView g, SceneView sc, float time, ActiveView av,
                                                           float* __restrict__ fields_out,
@@ -201,48 +268,148 @@ __global__ void __launch_bounds__(BLK_THREADS) k_mc_field_t(GridView g, SceneVie
         if (a < 0) break;
         const int lin = av.list[a];
         eval_block_field<COUNT>(g, sc, time, lin, s_field, diag);
-        if (threadIdx.x < FIELD_STRIDE - FIELD_N) s_field[FIELD_N + threadIdx.x] = 0.f;
-        __syncthreads();
-        if (fields_out) {
-            float4* dst = reinterpret_cast<float4*>(fields_out + (size_t)a * FIELD_STRIDE);
-            const float4* src = reinterpret_cast<const float4*>(s_field);
-            for (int i = threadIdx.x; i < FIELD_STRIDE / 4; i += blockDim.x) dst[i] = src[i];
-        }
+        block_counts(g, a, lin, s_field, s_red, fields_out, block_totals, packet_counts);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// block field with shared halos (engine path). Sample (x, y, z) of the grid belongs to block
+// (x / 8, y / 8, z / 8); the 9^3 field of a block is its own 8^3 samples plus the 217 samples of its
+// +x / +y / +z faces, edges and corner, which are their neighbours' own samples. k_field_own
+// evaluates every active block's own samples once, into the block's row of the field array;
+// k_field_halo completes each row, copying the halo from active neighbours' rows and evaluating only
+// the halo samples whose block is not active. Every sample is the same map() call at the same grid
+// point as in k_mc_field, so the rows are identical. A row's own entries are only written by
+// k_field_own and its halo entries only by k_field_halo of the same block, so the copies read
+// finished values.
+// ------------------------------------------------------------------------------------------------
+constexpr int OWN_N = 512;
+constexpr int HALO_N = FIELD_N - OWN_N;  // 81 + 72 + 64
+
+// halo sample h (0 <= h < 217) of a block in 9^3-local coordinates: the x = 8 face, then the y = 8
+// face without x = 8, then the z = 8 face without x = 8 and y = 8
+__device__ __forceinline__ void halo_coord(int h, int& x, int& y, int& z) {
+    if (h < 81) {
+        x = 8; y = h % 9; z = h / 9;
+    } else if (h < 153) {
+        h -= 81; y = 8; x = h & 7; z = h >> 3;
+    } else {
+        h -= 153; z = 8; x = h & 7; y = h >> 3;
+    }
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(BLK_THREADS) k_field_own(GridView g, SceneView sc, float time, ActiveView av,
+                                                         float* __restrict__ fields, int* __restrict__ block_to_active,
+                                                         unsigned* ticket, Diag* diag) {
+    __shared__ int s_item;
+    const int n = active_count(av);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (;;) {
+        const int a = claim(ticket, n, &s_item);
+        if (a < 0) break;
+        const int lin = av.list[a];
+        if (threadIdx.x == 0) block_to_active[lin] = a;
         int bx, by, bz;
         block_coord(g, lin, bx, by, bz);
-        unsigned cnt[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int tid = 2 * threadIdx.x + h;
-            const CellInfo c = cell_info(g, bx, by, bz, tid);
-            cnt[h] = 0;
-            if (!c.oob) {
-                float cv[8];
-                const int code = cell_case(s_field, c.lx, c.ly, c.lz, cv);
-                const unsigned long long word = c_mcCases[code];
-                cnt[h] = 3u * __popc(cell_valid_mask(g, c.x, c.y, c.z, cv, word));
-            }
-        }
-        if (packet_counts)
-            *reinterpret_cast<uint2*>(packet_counts + (size_t)a * 512 + 2 * threadIdx.x) = make_uint2(cnt[0], cnt[1]);
-        if (block_totals) {
-            unsigned v = cnt[0] + cnt[1];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                unsigned s = 0;
-                for (int w = 0; w < BLK_THREADS / 32; ++w) s += s_red[w];
-                block_totals[a] = s;
-            }
+        // sixteen 4 x 4 x 2 Morton bricks of 32 samples
+        for (int chunk = warp; chunk < OWN_N / 32; chunk += nwarps) {
+            const int r = chunk * 32 + lane;
+            const int sx = (r & 1) | ((r >> 2) & 2) | ((r >> 4) & 4);
+            const int sy = ((r >> 1) & 1) | ((r >> 3) & 2) | ((r >> 5) & 4);
+            const int sz = ((r >> 2) & 1) | ((r >> 4) & 2) | ((r >> 6) & 4);
+            const int gx = bx * 8 + sx, gy = by * 8 + sy, gz = bz * 8 + sz;
+            const bool valid = gx < g.w && gy < g.h && gz < g.d;
+            MapState<false> st;
+            map_warp<false, COUNT>(sc, grid_loc(g, gx, gy, gz), valid, time, st, diag);
+            fields[(size_t)a * FIELD_STRIDE + (sz * 9 + sy) * 9 + sx] = valid ? st.d : 0.f;
         }
     }
 }
 
-// the block-field kernel, and its work-counting twin (counting runs only)
+template <bool COUNT>
+__global__ void __launch_bounds__(BLK_THREADS) k_field_halo(GridView g, SceneView sc, float time, ActiveView av,
+                                                          float* __restrict__ fields,
+                                                          const int* __restrict__ block_to_active,
+                                                          const unsigned* __restrict__ flags,
+                                                          unsigned* __restrict__ block_totals,
+                                                          unsigned* __restrict__ packet_counts, unsigned* ticket,
+                                                          Diag* diag) {
+    __shared__ __align__(16) float s_field[FIELD_STRIDE];
+    __shared__ unsigned s_red[BLK_THREADS / 32];
+    __shared__ unsigned short s_miss[HALO_N];
+    __shared__ int s_warp_base[BLK_THREADS / 32 + 1];
+    __shared__ int s_item;
+    static_assert(HALO_N <= BLK_THREADS, "one halo sample per thread");
+    const int n = active_count(av);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (;;) {
+        const int a = claim(ticket, n, &s_item);
+        if (a < 0) break;
+        const int lin = av.list[a];
+        int bx, by, bz;
+        block_coord(g, lin, bx, by, bz);
+        float* row = fields + (size_t)a * FIELD_STRIDE;
+        {
+            const float4* src = reinterpret_cast<const float4*>(row);
+            float4* dst = reinterpret_cast<float4*>(s_field);
+            for (int i = threadIdx.x; i < FIELD_STRIDE / 4; i += blockDim.x) dst[i] = src[i];
+        }
+        __syncthreads();  // the row (own entries; stale halo entries) is in place before the halo writes
+        // halo samples: from the owning block's row when it is active, else queued for evaluation
+        bool miss = false;
+        int hx = 0, hy = 0, hz = 0;
+        if (threadIdx.x < HALO_N) {
+            halo_coord(threadIdx.x, hx, hy, hz);
+            const int ox = bx + (hx >> 3), oy = by + (hy >> 3), oz = bz + (hz >> 3);
+            int b = -1;
+            if (ox < g.bx && oy < g.by && oz < g.bz) {
+                const int olin = ox + g.bx * (oy + g.by * oz);
+                if (flags[olin]) b = block_to_active[olin];
+            }
+            if (b >= 0)
+                s_field[(hz * 9 + hy) * 9 + hx] = fields[(size_t)b * FIELD_STRIDE + ((hz & 7) * 9 + (hy & 7)) * 9 + (hx & 7)];
+            else
+                miss = true;
+        }
+        // the missing samples in halo order (ballot prefix within warps, then across warps)
+        const unsigned bal = __ballot_sync(0xffffffffu, miss);
+        if (lane == 0) s_warp_base[warp] = __popc(bal);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int acc = 0;
+            for (int w = 0; w < nwarps; ++w) {
+                const int c = s_warp_base[w];
+                s_warp_base[w] = acc;
+                acc += c;
+            }
+            s_warp_base[nwarps] = acc;
+        }
+        __syncthreads();
+        if (miss) s_miss[s_warp_base[warp] + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)((hz * 9 + hy) * 9 + hx);
+        __syncthreads();
+        const int nmiss = s_warp_base[nwarps];
+        for (int chunk = warp; chunk * 32 < nmiss; chunk += nwarps) {
+            const int r = chunk * 32 + lane;
+            const int s = r < nmiss ? (int)s_miss[r] : 0;
+            const int sx = s % 9, sy = (s / 9) % 9, sz = s / 81;
+            const int gx = bx * 8 + sx, gy = by * 8 + sy, gz = bz * 8 + sz;
+            const bool valid = r < nmiss && gx < g.w && gy < g.h && gz < g.d;
+            MapState<false> st;
+            map_warp<false, COUNT>(sc, grid_loc(g, gx, gy, gz), valid, time, st, diag);
+            if (r < nmiss) s_field[s] = valid ? st.d : 0.f;
+        }
+        __syncthreads();
+        if (threadIdx.x < HALO_N) {
+            const int h = (hz * 9 + hy) * 9 + hx;
+            row[h] = s_field[h];
+        }
+        block_counts(g, a, lin, s_field, s_red, nullptr, block_totals, packet_counts);
+    }
+}
+
+// the single-kernel block field of the drop-in launcher (no block-to-active map is at hand there)
 static constexpr auto k_mc_field = k_mc_field_t<false>;
-static constexpr auto k_mc_field_count = k_mc_field_t<true>;
 
 // FP32 FMA throughput probe: 8 independent FMA chains per thread, no memory traffic in the loop
 __global__ void __launch_bounds__(256) k_fma_peak(float* out, int iters, float a, float b) {

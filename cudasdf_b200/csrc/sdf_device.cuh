@@ -345,6 +345,9 @@ struct Diag {
     unsigned long long leaf_evals;  //   per-point primitive evaluations,
     unsigned long long points;      //   evaluated points
     unsigned long long scouted;     // blocks the surrogate-culled scout evaluated exactly
+    unsigned long long warp_pops;   // counting runs: warp-wide stack pops,
+    unsigned long long warp_tests;  //   of which with a box test (some lane alive),
+    unsigned long long warp_leaves; //   and leaf steps (some lane evaluates the primitive)
     int stack_overflow;             // a search needed more than 64 stack entries
     int timeout;                    // a bounded wait gave up
 };
@@ -354,7 +357,7 @@ struct Diag {
 template <bool ATTR, bool COUNT = false>
 __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool valid, float time, MapState<ATTR>& st,
                                          Diag* diag) {
-    unsigned long long cnt_pops = 0, cnt_leaves = 0;
+    unsigned long long cnt_pops = 0, cnt_leaves = 0, cnt_wpops = 0, cnt_wtests = 0, cnt_wleaves = 0;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     st.init();
@@ -382,10 +385,14 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
             // a lane pops this node iff it pushed it and has popped fewer than MAP_CAP nodes
             const bool pops = ((mask >> lane) & 1u) && iter < MAP_CAP;
             if (pops) iter++;
-            if (COUNT) cnt_pops += __popc(__ballot_sync(FULL, pops));
+            if (COUNT) {
+                cnt_pops += __popc(__ballot_sync(FULL, pops));
+                ++cnt_wpops;
+            }
             // a node can only pass the prune test for a lane whose running distance is > 0
             const unsigned alive = __ballot_sync(FULL, pops && st.d > 0.f);
             if (alive == 0) continue;
+            if (COUNT) ++cnt_wtests;
             const float4 na = __ldg(sc.nodes + 2 * node);
             const float4 nb = __ldg(sc.nodes + 2 * node + 1);
             const bool hit = ((alive >> lane) & 1u) && box_closer(p, na, nb, st.d);
@@ -395,7 +402,10 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
             if (right == -1) {
                 const float4* pr = sc.prims + (size_t)left * PRIM_ROWS;
                 const Leaf L = load_leaf(pr);
-                if (COUNT) cnt_leaves += __popc(hm);
+                if (COUNT) {
+                    cnt_leaves += __popc(hm);
+                    ++cnt_wleaves;
+                }
                 if (hit) {
                     float3 pre;
                     const float dp = leaf_distance(L, p, time, pre);
@@ -422,6 +432,9 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
         atomicAdd(&diag->node_pops, cnt_pops);
         atomicAdd(&diag->leaf_evals, cnt_leaves + (unsigned long long)nlive * (sc.nprims - sc.nbvh));
         atomicAdd(&diag->points, (unsigned long long)nlive);
+        atomicAdd(&diag->warp_pops, cnt_wpops);
+        atomicAdd(&diag->warp_tests, cnt_wtests);
+        atomicAdd(&diag->warp_leaves, cnt_wleaves);
     }
     // non-union primitives: a linear pass in scene order (:703-803)
     for (int i = sc.nbvh; i < sc.nprims; ++i) {

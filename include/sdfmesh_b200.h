@@ -263,8 +263,9 @@ sdf_status sdf_engine_eval_normals(sdf_engine* e, const float* d_points, int n, 
 
 /* Work counters of one extraction's block-field stage (a separate, slower counting run):
  * out[0] BVH nodes popped per point (summed), out[1] primitive evaluations, out[2] points,
- * out[3] active blocks. */
-sdf_status sdf_engine_count_work(sdf_engine* e, unsigned long long out[4]);
+ * out[3] active blocks, out[4] warp-wide stack pops, out[5] of those with a box test,
+ * out[6] warp-wide leaf steps, out[7] reserved (0). */
+sdf_status sdf_engine_count_work(sdf_engine* e, unsigned long long out[8]);
 /* FP32 FMA throughput of the current device in TFLOP/s, measured by a short FMA-loop kernel. */
 sdf_status sdf_measure_fp32_peak(double* tflops);
 
