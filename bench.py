@@ -1,17 +1,22 @@
 """Benchmark: Gvoxels/s of SDF -> mesh extraction on one B200 (or N, one process per GPU).
 
-Workload (default): marching cubes over a 1024^3 grid on [-1, 1]^3 of a seeded composite scene of
+Workload (default, c4): marching cubes over a 1024^3 grid on [-1, 1]^3 of a seeded composite scene of
 16384 smooth-blended primitives (sphere/box/capsule/torus, sizes log-uniform in [0.02, 0.2]); VBO
-(float4 positions) + EBO (uint32 indices). A step is one full extraction: scout -> compaction ->
-block field -> block scan -> emission, with the scene already on the device.
+(float4 positions) + EBO (uint32 indices). A step is one full extraction with the scene already on
+the device: (surrogate coarse-block inference ->) scout -> compaction -> block field (own samples,
+then halos) -> block scan -> emission.
 
-  value  = grid samples (1024^3) per second of device time, summed over ranks
-  e2e    = the same through the public engine API with host buffers: scene upload from pinned host
-           memory + host BVH build + extraction + read-back of counts and the whole vertex buffer
+  value  = grid samples (1024^3) per second of device time of the surrogate-culled extraction, summed
+           over ranks; the network is trained, certified and audited once before the timed region
+           (its cost is reported under "surrogate"), and the culled mesh is checked byte-identical
+           to the plain one
+  plain  = the same for the plain exact extraction (no surrogate)
+  e2e    = the surrogate-culled extraction through the public engine API with host buffers: scene
+           upload from pinned host memory + extraction + read-back of counts and the whole vertex buffer
   --impl reference: the reference's own CUDA path (built from its sources into oracle/_ref) on the
            same GPU, driven in CudaSDFMesh::Update's stage order.
 
-Run: python bench.py [--gpus N --steps K --warmup W --config c4 --impl ours|reference]
+Run: python bench.py [--gpus N --steps K --warmup W --config c4 --impl ours|reference --plain]
 """
 from __future__ import annotations
 
@@ -31,7 +36,7 @@ CONFIGS = {
     "c1": {"config": 1, "technique": 0, "workload": "mc_sphere_128"},
     "c2": {"config": 2, "technique": 0, "workload": "mc_256prims_256"},
     "c3": {"config": 3, "technique": 1, "workload": "dc_4096prims_512"},
-    "c4": {"config": 4, "technique": 0, "workload": "mc_16384prims_1024"},
+    "c4": {"config": 4, "technique": 0, "workload": "mc_16384prims_1024", "surrogate": True},
 }
 
 
@@ -44,6 +49,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--plain", action="store_true", help="time the plain exact path only (no surrogate)")
     return ap.parse_args()
 
 
@@ -144,6 +150,33 @@ def fp32_peak_tflops():
     return v.value if rc == 0 else None
 
 
+STAGES = ("ms_scout", "ms_field", "ms_scan", "ms_emit")
+
+
+def timed_extractions(eng, buf, steps, flush, world):
+    """K extractions, each timed with CUDA events on the launching stream, L2 flushed before each; the
+    engine's own per-stage events (recorded on the same stream) give the stage split of the same steps."""
+    import torch
+    stream = torch.cuda.current_stream()
+    eng.set_timing(True)
+    barrier(world)
+    times, stages = [], {k: [] for k in STAGES}
+    st = None
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = eng.extract(buf)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        for k in STAGES:
+            stages[k].append(st[k])
+    barrier(world)
+    eng.set_timing(False)
+    return times, st, {k: sum(v) / len(v) for k, v in stages.items()}
+
+
 def run_ours(args, rank, world):
     import numpy as np
     import torch
@@ -158,6 +191,7 @@ def run_ours(args, rank, world):
     cell = S.cell_size_for(res)
     prims = S.config_scene(cfg_id)
     mask = L.OUT_INDICES
+    surrogate = spec.get("surrogate", False) and not args.plain
     eng = Engine()
     eng.configure(make_config(cell, technique=tech, out_mask=mask))
     eng.set_scene(prims)
@@ -168,34 +202,46 @@ def run_ours(args, rank, world):
     del probe_buf
     buf = MeshBuffers(V + 1024, mask)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
-    stream = torch.cuda.current_stream()
-    for _ in range(args.warmup):
-        eng.extract(buf)
-    # per-stage split (event timing inside the engine), one untimed extraction
-    eng.set_timing(True)
-    stages = eng.extract(buf)
-    eng.set_timing(False)
-    barrier(world)
+    voxels = float(res) ** 3
+    out = {"V": V, "res": res, "nprims": len(prims)}
+
     clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
-    times = []
-    for _ in range(args.steps):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        st = eng.extract(buf)
-        e1.record(stream)
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
-    barrier(world)
+    # ---- plain exact extraction
+    for _ in range(args.warmup):
+        eng.extract(buf)
+    times, st, out["plain_stages"] = timed_extractions(eng, buf, args.steps, flush, world)
+    plain_ms = max_over_ranks(sum(times) / len(times), world)
+    out["plain"] = {"ms": plain_ms, "value": world * voxels / (plain_ms * 1e-3) / 1e9, "stats": st}
+    launches_per_step = 6  # scout, compaction, own field, halo field, block scan, emission
+    if surrogate:
+        plain_verts = buf.vertices[:V].clone()
+        t0 = time.perf_counter()
+        sst = eng.surrogate_train()
+        torch.cuda.synchronize()
+        train_wall = (time.perf_counter() - t0) * 1e3
+        audit = eng.surrogate_audit(0.0)
+        out["surrogate"] = {"train": sst, "train_wall_ms": train_wall, "audit": audit}
+        if audit["violations"] == 0:
+            eng.surrogate_enable(True)
+            launches_per_step = 7  # + the surrogate's coarse-block inference
+        else:  # the exact audit is the judge: a violated certificate falls back to the plain path
+            out["surrogate"]["fallback"] = "audit found active blocks in culled coarse blocks"
+        for _ in range(args.warmup):
+            eng.extract(buf)
+        buf.vertices.zero_()
+        times, st, out["stages"] = timed_extractions(eng, buf, args.steps, flush, world)
+        out["surrogate"]["identical_mesh"] = bool(int(st["total_vertices"]) == V and
+                                                  torch.equal(buf.vertices[:V], plain_verts))
+        del plain_verts
+    else:
+        out["stages"] = out["plain_stages"]
     clk = clocks.stop()
-    ms = sum(times) / len(times)
-    ms_max = max_over_ranks(ms, world)
-    voxels = float(res) ** 3
-    value = world * voxels / (ms_max * 1e-3) / 1e9
-    out = {"ms": ms_max, "value": value, "stats": st, "stages": stages, "clocks": clk, "V": V, "res": res,
-           "times": times, "nprims": len(prims)}
-    # end to end through the public API with host buffers
+    ms = max_over_ranks(sum(times) / len(times), world)
+    out.update({"ms": ms, "value": world * voxels / (ms * 1e-3) / 1e9, "stats": st, "clocks": clk, "times": times,
+                "launches_per_step": launches_per_step})
+    # end to end through the public API with host buffers: scene upload from pinned host memory (an
+    # unchanged scene keeps its host BVH and surrogate), extraction, read-back of the whole vertex buffer
     if not args.no_e2e:
         host_verts = torch.empty((V, 4), dtype=torch.float32, pin_memory=True)
         pinned_prims = torch.from_numpy(prims.view(np.uint8).copy()).pin_memory()
@@ -306,24 +352,28 @@ def run_reference(args, rank, world):
             "stats": st, "clocks": clk, "res": res}
 
 
+METRIC = "Gvoxels/s SDF\u2192mesh at 1024\u00b3, surrogate-culled vs plain, identical topology"
+
+
 def main():
     args = parse()
     rank, world, local = dist_setup(args.gpus)
     spec = CONFIGS[args.config]
-    base = {"metric": "Gvoxels/s SDF->mesh extraction (1024^3 plain exact marching cubes; surrogate-culled "
-                      "variant reported separately)" if args.config == "c4" else "Gvoxels/s SDF->mesh extraction",
+    headline = spec.get("surrogate", False)
+    base = {"metric": METRIC if headline else f"Gvoxels/s SDF\u2192mesh extraction ({spec['workload']})",
             "unit": "Gvoxels/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded scene, shapes/sizes of the benchmark configuration)"}
+            "data": "synthetic (seeded scene with the benchmark configuration's primitive law, sizes and counts)"}
+    nprims = len(__import__("cudasdf_b200.scenes", fromlist=["x"]).config_scene(spec["config"]))
     if args.impl == "reference":
         if rank != 0:
             return
         r = run_reference(args, rank, world)
         line = dict(base)
         line.update({"impl": "reference", "value": r["value"], "ms_per_step": r["ms"],
-                     "config": {"workload": spec["workload"], "grid": r["res"], "primitives": len(
-                         __import__("cudasdf_b200.scenes", fromlist=["x"]).config_scene(spec["config"])),
+                     "config": {"workload": spec["workload"], "grid": r["res"], "primitives": nprims,
                                 "outputs": "VBO float4 + EBO uint32", "parallelism": "single GPU",
+                                "path": "the reference's plain exact path (it has no surrogate)",
                                 "l2": "per-stage host syncs of the reference (CudaSDFMesh.cpp:83-88)"},
                      "reference_kernel_ms": r["ms_kernels"], "reference_stats": r["stats"], "clocks": r["clocks"],
                      "cpu_baseline": {"value": r["value"], "unit": "Gvoxels/s", "cores": 1, "kind": "reference",
@@ -339,13 +389,25 @@ def main():
     st = r["stats"]
     line = dict(base)
     line.update({"value": r["value"], "ms_per_step": r["ms"],
-                 "config": {"workload": spec["workload"], "grid": r["res"], "primitives": r["nprims"],
-                            "outputs": "VBO float4 + EBO uint32", "active_blocks": st["active_blocks"],
-                            "vertices": st["total_vertices"], "parallelism": f"replicas x{world}",
+                 "config": {"workload": spec["workload"] + ("_surrogate_culled" if "surrogate" in r else ""),
+                            "grid": r["res"], "primitives": r["nprims"], "outputs": "VBO float4 + EBO uint32",
+                            "active_blocks": st["active_blocks"], "vertices": st["total_vertices"],
+                            "scouted_blocks": st["scouted_blocks"], "parallelism": f"replicas x{world}",
                             "l2": "flushed between timed steps (256 MiB write)"},
-                 "stage_ms": {k: r["stages"][k] for k in ("ms_scout", "ms_field", "ms_scan", "ms_emit")},
+                 "stage_ms": r["stages"],
+                 "plain": {"value": r["plain"]["value"], "ms_per_step": r["plain"]["ms"],
+                           "stage_ms": r["plain_stages"]},
                  "bvh_cap_hits": st["bvh_cap_hits"], "clocks": r["clocks"],
-                 "gpu_launches": 5 * args.steps})
+                 "gpu_launches": r["launches_per_step"] * args.steps})
+    if "surrogate" in r:
+        sg = r["surrogate"]
+        line["surrogate"] = {"ratio_vs_plain": r["value"] / r["plain"]["value"],
+                             "identical_mesh": sg.get("identical_mesh"), "audit": sg["audit"],
+                             "eps_max": sg["train"]["eps_max"], "eps_cert": sg["train"]["eps_cert"],
+                             "margin": sg["train"]["margin"], "final_loss": sg["train"]["final_loss"],
+                             "train_ms": {"samples": sg["train"]["ms_samples"], "train": sg["train"]["ms_train"],
+                                          "certify": sg["train"]["ms_certify"], "wall": sg["train_wall_ms"]},
+                             "fallback": sg.get("fallback")}
     if "e2e" in r:
         line["e2e"] = r["e2e"]
     line["roofline"] = roofline(r)
@@ -374,7 +436,8 @@ def roofline(r):
         return None
     flops = c["field_node_visits"] * FLOP_PER_NODE + c["field_leaf_evals"] * FLOP_PER_LEAF
     achieved = flops / (ms_field * 1e-3) / 1e12
-    return {"kernel": "k_mc_field (block field: warp-coherent BVH map())", "bound": "fp32", "achieved": achieved,
+    return {"kernel": "k_field_own + k_field_halo (block field: warp-coherent BVH map())", "bound": "fp32",
+            "achieved": achieved,
             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": "measured by the library's FMA loop on this GPU (no FP32 figure in MEASURED_PEAKS.json)",
             "traffic": None, "work": c}

@@ -16,7 +16,7 @@ struct Ctrl {
     unsigned tickets[12];
     unsigned total_vertices;
     unsigned dc_vertices;
-    unsigned pad;
+    unsigned halo_misses;  // listed halo samples of the block field (k_field_plan)
     Diag diag;
 };
 
@@ -100,6 +100,8 @@ struct EngineImpl {
     int debug = 0;
     cudaEvent_t ev[8] = {};
     size_t packet_cap = 0;
+    unsigned* miss = nullptr;          // listed halo samples, capacity nblocks * HALO_N
+    size_t miss_cap = 0;
     Diag* eval_diag = nullptr;
     std::vector<sdf_primitive> scene;  // the primitives as given (the surrogate's surface run uses them)
     SurrogateState* sur = nullptr;
@@ -108,7 +110,7 @@ struct EngineImpl {
 
     void release() {
         void* ptrs[] = {d_prims, d_nodes, flags, list, fields, block_totals, block_offsets, packet_counts,
-                        packet_offsets, b2a, masks, dc_voff, dc_verts, dc_norms, ctrl_region, eval_diag};
+                        packet_offsets, b2a, masks, dc_voff, dc_verts, dc_norms, ctrl_region, eval_diag, miss};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         d_prims = nullptr; d_nodes = nullptr; flags = nullptr; list = nullptr; fields = nullptr;
@@ -116,7 +118,8 @@ struct EngineImpl {
         b2a = nullptr; masks = nullptr; dc_voff = nullptr; dc_verts = nullptr; dc_norms = nullptr;
         ctrl_region = nullptr;
         eval_diag = nullptr;
-        prims_cap = nodes_cap = dc_cap = packet_cap = 0;
+        miss = nullptr;
+        prims_cap = nodes_cap = dc_cap = packet_cap = miss_cap = 0;
         if (h_ctrl) cudaFreeHost(h_ctrl);
         h_ctrl = nullptr;
         for (auto& e : ev)
@@ -166,6 +169,33 @@ static float surrogate_reach(const EngineImpl& E, float slack_cells) {
 }
 
 static float surrogate_margin(const EngineImpl& E) { return E.sur->eps + surrogate_reach(E, E.sur->slack_cells); }
+
+// the block field with shared halos (plan -> evaluation -> gather, see mc_kernels.cuh) and the block totals
+template <bool COUNT>
+static sdf_status run_block_field(EngineImpl& E, const sdfb::SceneView& sv, float time, const sdfb::ActiveView& av,
+                                  sdfb::Ctrl* ctrl, unsigned* packet_counts, cudaStream_t st) {
+    using namespace sdfb;
+    const size_t need = (size_t)E.nblocks * HALO_N;
+    if (E.miss_cap < need) {
+        if (dev_alloc(E.miss, need) != SDF_OK) {
+            E.miss_cap = 0;
+            return SDF_ERR_NOMEM;
+        }
+        E.miss_cap = need;
+    }
+    k_field_plan<<<num_sms() * 8, 256, 0, st>>>(E.gv, av, E.flags, E.fields, E.b2a, E.miss, &ctrl->halo_misses);
+    check_launch();
+    k_field_own<COUNT><<<persistent_grid(k_field_own<COUNT>, BLK_THREADS, E.nblocks), BLK_THREADS, 0, st>>>(
+        E.gv, sv, time, av, E.fields, &ctrl->tickets[0], &ctrl->diag);
+    check_launch();
+    k_field_miss<COUNT><<<persistent_grid(k_field_miss<COUNT>, BLK_THREADS, 1 << 30), BLK_THREADS, 0, st>>>(
+        E.gv, sv, time, av, E.fields, E.miss, &ctrl->halo_misses, &ctrl->tickets[4], &ctrl->diag);
+    check_launch();
+    k_field_gather<<<persistent_grid(k_field_gather, BLK_THREADS, E.nblocks), BLK_THREADS, 0, st>>>(
+        E.gv, av, E.fields, E.b2a, E.flags, COUNT ? nullptr : E.block_totals, packet_counts, &ctrl->tickets[3]);
+    check_launch();
+    return SDF_OK;
+}
 
 static void coarse_dims(const EngineImpl& E, int& cx, int& cy, int& cz) {
     using namespace sdfb;
@@ -401,13 +431,8 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
     if (!out->normals) mask &= ~OUT_NORMALS;
 
     if (!dc) {
-        k_field_own<false><<<persistent_grid(k_field_own<false>, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(
-            gv, sv, time, av, E.fields, E.b2a, &ctrl->tickets[0], diag);
-        check_launch();
-        k_field_halo<false><<<persistent_grid(k_field_halo<false>, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(
-            gv, sv, time, av, E.fields, E.b2a, E.flags, E.block_totals, (E.debug & 1) ? E.packet_counts : nullptr,
-            &ctrl->tickets[3], diag);
-        check_launch();
+        if (run_block_field<false>(E, sv, time, av, ctrl, (E.debug & 1) ? E.packet_counts : nullptr, st) != SDF_OK)
+            return SDF_ERR_NOMEM;
         if (E.timing) cudaEventRecord(E.ev[2], st);
         k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)nb)), SCAN_THREADS, 0, st>>>(
             E.block_totals, E.block_offsets, 0, &ctrl->active_count, 1, scan_state(scanB), &ctrl->total_vertices, diag);
@@ -598,11 +623,7 @@ sdf_status sdf_engine_count_work(sdf_engine* e, unsigned long long out[8]) {
     record(cudaMemsetAsync(&ctrl->diag, 0, sizeof(Diag), 0));
     ActiveView av{E.list, &ctrl->active_count, E.nblocks};
     // the engine's block-field stage (own samples, then the halos no active block owns) with counters on
-    k_field_own<true><<<persistent_grid(k_field_own<true>, BLK_THREADS, E.nblocks), BLK_THREADS>>>(
-        E.gv, sv, 0.f, av, E.fields, E.b2a, &ctrl->tickets[0], &ctrl->diag);
-    k_field_halo<true><<<persistent_grid(k_field_halo<true>, BLK_THREADS, E.nblocks), BLK_THREADS>>>(
-        E.gv, sv, 0.f, av, E.fields, E.b2a, E.flags, nullptr, nullptr, &ctrl->tickets[3], &ctrl->diag);
-    check_launch();
+    if (run_block_field<true>(E, sv, 0.f, av, ctrl, nullptr, 0) != SDF_OK) return SDF_ERR_NOMEM;
     Ctrl h;
     if (cudaMemcpy(&h, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost) != cudaSuccess) return SDF_ERR_CUDA;
     out[0] = h.diag.node_pops;

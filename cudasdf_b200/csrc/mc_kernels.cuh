@@ -275,16 +275,21 @@ __global__ void __launch_bounds__(BLK_THREADS) k_mc_field_t(GridView g, SceneVie
 // ------------------------------------------------------------------------------------------------
 // block field with shared halos (engine path). Sample (x, y, z) of the grid belongs to block
 // (x / 8, y / 8, z / 8); the 9^3 field of a block is its own 8^3 samples plus the 217 samples of its
-// +x / +y / +z faces, edges and corner, which are their neighbours' own samples. k_field_own
-// evaluates every active block's own samples once, into the block's row of the field array;
-// k_field_halo completes each row, copying the halo from active neighbours' rows and evaluating only
-// the halo samples whose block is not active. Every sample is the same map() call at the same grid
-// point as in k_mc_field, so the rows are identical. A row's own entries are only written by
-// k_field_own and its halo entries only by k_field_halo of the same block, so the copies read
-// finished values.
+// +x / +y / +z faces, edges and corner, which are their neighbours' own samples. Every sample is the
+// same map() call at the same grid point as in k_mc_field, so the rows are identical; each sample
+// is evaluated once per extraction when its block is active, and only halo samples whose block is
+// not active are evaluated for the block that needs them.
+//   k_field_plan    block-to-active map; the halo samples whose block is not active, as a list
+//   k_field_own     every active block's own samples
+//   k_field_miss    the listed halo samples, 32 per warp task
+//   k_field_gather  completes each row with the halo copied from the active neighbours' rows, then
+//                   the per-cell counts and the block total
+// A row's own entries are written only by k_field_own, its listed halo entries only by k_field_miss
+// and its other halo entries only by k_field_gather of the same block.
 // ------------------------------------------------------------------------------------------------
 constexpr int OWN_N = 512;
 constexpr int HALO_N = FIELD_N - OWN_N;  // 81 + 72 + 64
+constexpr int OWN_TASKS = OWN_N / 32;    // warp tasks per block
 
 // halo sample h (0 <= h < 217) of a block in 9^3-local coordinates: the x = 8 face, then the y = 8
 // face without x = 8, then the z = 8 face without x = 8 and y = 8
@@ -298,22 +303,60 @@ __device__ __forceinline__ void halo_coord(int h, int& x, int& y, int& z) {
     }
 }
 
+// linear index of the block owning halo sample (hx, hy, hz) of block (bx, by, bz), -1 outside the grid
+__device__ __forceinline__ int halo_owner(const GridView& g, int bx, int by, int bz, int hx, int hy, int hz) {
+    const int ox = bx + (hx >> 3), oy = by + (hy >> 3), oz = bz + (hz >> 3);
+    if (ox >= g.bx || oy >= g.by || oz >= g.bz) return -1;
+    return ox + g.bx * (oy + g.by * oz);
+}
+
+// one thread per (active block, halo sample); missing samples are listed as (a << 8) | h
+__global__ void __launch_bounds__(256) k_field_plan(GridView g, ActiveView av, const unsigned* __restrict__ flags,
+                                                    float* __restrict__ fields, int* __restrict__ block_to_active,
+                                                    unsigned* __restrict__ miss, unsigned* __restrict__ miss_count) {
+    const int n = active_count(av);
+    const long long total = (long long)n * HALO_N;
+    const int lane = threadIdx.x & 31;
+    for (long long i0 = (long long)blockIdx.x * blockDim.x; i0 < total; i0 += (long long)gridDim.x * blockDim.x) {
+        const long long i = i0 + threadIdx.x;
+        bool m = false;
+        int a = 0, h = 0;
+        if (i < total) {
+            a = (int)(i / HALO_N);
+            h = (int)(i - (long long)a * HALO_N);
+            const int lin = av.list[a];
+            if (h == 0) block_to_active[lin] = a;
+            int bx, by, bz, hx, hy, hz;
+            block_coord(g, lin, bx, by, bz);
+            halo_coord(h, hx, hy, hz);
+            const int olin = halo_owner(g, bx, by, bz, hx, hy, hz);
+            if (olin < 0)
+                fields[(size_t)a * FIELD_STRIDE + (hz * 9 + hy) * 9 + hx] = 0.f;  // outside the grid
+            else
+                m = flags[olin] == 0u;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, m);
+        unsigned base = 0;
+        if (lane == 0 && bal) base = atomicAdd(miss_count, (unsigned)__popc(bal));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (m) miss[base + __popc(bal & ((1u << lane) - 1u))] = ((unsigned)a << 8) | (unsigned)h;
+    }
+}
+
+// own samples: one CTA per active block, its eight warps on the sixteen 4 x 4 x 2 Morton bricks (all
+// warps of the SM walk the BVH near the same block, which keeps the nodes they read in L1)
 template <bool COUNT>
 __global__ void __launch_bounds__(BLK_THREADS) k_field_own(GridView g, SceneView sc, float time, ActiveView av,
-                                                         float* __restrict__ fields, int* __restrict__ block_to_active,
-                                                         unsigned* ticket, Diag* diag) {
+                                                         float* __restrict__ fields, unsigned* ticket, Diag* diag) {
     __shared__ int s_item;
     const int n = active_count(av);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     for (;;) {
         const int a = claim(ticket, n, &s_item);
         if (a < 0) break;
-        const int lin = av.list[a];
-        if (threadIdx.x == 0) block_to_active[lin] = a;
         int bx, by, bz;
-        block_coord(g, lin, bx, by, bz);
-        // sixteen 4 x 4 x 2 Morton bricks of 32 samples
-        for (int chunk = warp; chunk < OWN_N / 32; chunk += nwarps) {
+        block_coord(g, av.list[a], bx, by, bz);
+        for (int chunk = warp; chunk < OWN_TASKS; chunk += nwarps) {
             const int r = chunk * 32 + lane;
             const int sx = (r & 1) | ((r >> 2) & 2) | ((r >> 4) & 4);
             const int sy = ((r >> 1) & 1) | ((r >> 3) & 2) | ((r >> 5) & 4);
@@ -327,22 +370,46 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_own(GridView g, SceneView
     }
 }
 
+// listed halo samples, 32 per warp task, tasks claimed one at a time by each warp
 template <bool COUNT>
-__global__ void __launch_bounds__(BLK_THREADS) k_field_halo(GridView g, SceneView sc, float time, ActiveView av,
+__global__ void __launch_bounds__(BLK_THREADS) k_field_miss(GridView g, SceneView sc, float time, ActiveView av,
                                                           float* __restrict__ fields,
-                                                          const int* __restrict__ block_to_active,
-                                                          const unsigned* __restrict__ flags,
-                                                          unsigned* __restrict__ block_totals,
-                                                          unsigned* __restrict__ packet_counts, unsigned* ticket,
+                                                          const unsigned* __restrict__ miss,
+                                                          const unsigned* __restrict__ miss_count, unsigned* ticket,
                                                           Diag* diag) {
+    const int nmiss = (int)*miss_count;
+    const int tasks = (nmiss + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = (int)atomicAdd(ticket, 1u);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= tasks) break;
+        const int e = t * 32 + lane;
+        const bool live = e < nmiss;
+        const unsigned m = live ? miss[e] : miss[t * 32];
+        const int a = (int)(m >> 8);
+        int sx, sy, sz, bx, by, bz;
+        halo_coord((int)(m & 255u), sx, sy, sz);
+        block_coord(g, av.list[a], bx, by, bz);
+        const int gx = bx * 8 + sx, gy = by * 8 + sy, gz = bz * 8 + sz;
+        const bool valid = live && gx < g.w && gy < g.h && gz < g.d;
+        MapState<false> st;
+        map_warp<false, COUNT>(sc, grid_loc(g, gx, gy, gz), valid, time, st, diag);
+        if (live) fields[(size_t)a * FIELD_STRIDE + (sz * 9 + sy) * 9 + sx] = valid ? st.d : 0.f;
+    }
+}
+
+__global__ void __launch_bounds__(BLK_THREADS) k_field_gather(GridView g, ActiveView av, float* __restrict__ fields,
+                                                            const int* __restrict__ block_to_active,
+                                                            const unsigned* __restrict__ flags,
+                                                            unsigned* __restrict__ block_totals,
+                                                            unsigned* __restrict__ packet_counts, unsigned* ticket) {
     __shared__ __align__(16) float s_field[FIELD_STRIDE];
     __shared__ unsigned s_red[BLK_THREADS / 32];
-    __shared__ unsigned short s_miss[HALO_N];
-    __shared__ int s_warp_base[BLK_THREADS / 32 + 1];
     __shared__ int s_item;
     static_assert(HALO_N <= BLK_THREADS, "one halo sample per thread");
     const int n = active_count(av);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     for (;;) {
         const int a = claim(ticket, n, &s_item);
         if (a < 0) break;
@@ -355,54 +422,18 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_halo(GridView g, SceneVie
             float4* dst = reinterpret_cast<float4*>(s_field);
             for (int i = threadIdx.x; i < FIELD_STRIDE / 4; i += blockDim.x) dst[i] = src[i];
         }
-        __syncthreads();  // the row (own entries; stale halo entries) is in place before the halo writes
-        // halo samples: from the owning block's row when it is active, else queued for evaluation
-        bool miss = false;
-        int hx = 0, hy = 0, hz = 0;
+        __syncthreads();  // the row is in place before the copied halo entries overwrite their slots
         if (threadIdx.x < HALO_N) {
+            int hx, hy, hz;
             halo_coord(threadIdx.x, hx, hy, hz);
-            const int ox = bx + (hx >> 3), oy = by + (hy >> 3), oz = bz + (hz >> 3);
-            int b = -1;
-            if (ox < g.bx && oy < g.by && oz < g.bz) {
-                const int olin = ox + g.bx * (oy + g.by * oz);
-                if (flags[olin]) b = block_to_active[olin];
+            const int olin = halo_owner(g, bx, by, bz, hx, hy, hz);
+            if (olin >= 0 && flags[olin]) {
+                const int b = block_to_active[olin];
+                const int h = (hz * 9 + hy) * 9 + hx;
+                const float v = fields[(size_t)b * FIELD_STRIDE + ((hz & 7) * 9 + (hy & 7)) * 9 + (hx & 7)];
+                s_field[h] = v;
+                row[h] = v;
             }
-            if (b >= 0)
-                s_field[(hz * 9 + hy) * 9 + hx] = fields[(size_t)b * FIELD_STRIDE + ((hz & 7) * 9 + (hy & 7)) * 9 + (hx & 7)];
-            else
-                miss = true;
-        }
-        // the missing samples in halo order (ballot prefix within warps, then across warps)
-        const unsigned bal = __ballot_sync(0xffffffffu, miss);
-        if (lane == 0) s_warp_base[warp] = __popc(bal);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int acc = 0;
-            for (int w = 0; w < nwarps; ++w) {
-                const int c = s_warp_base[w];
-                s_warp_base[w] = acc;
-                acc += c;
-            }
-            s_warp_base[nwarps] = acc;
-        }
-        __syncthreads();
-        if (miss) s_miss[s_warp_base[warp] + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)((hz * 9 + hy) * 9 + hx);
-        __syncthreads();
-        const int nmiss = s_warp_base[nwarps];
-        for (int chunk = warp; chunk * 32 < nmiss; chunk += nwarps) {
-            const int r = chunk * 32 + lane;
-            const int s = r < nmiss ? (int)s_miss[r] : 0;
-            const int sx = s % 9, sy = (s / 9) % 9, sz = s / 81;
-            const int gx = bx * 8 + sx, gy = by * 8 + sy, gz = bz * 8 + sz;
-            const bool valid = r < nmiss && gx < g.w && gy < g.h && gz < g.d;
-            MapState<false> st;
-            map_warp<false, COUNT>(sc, grid_loc(g, gx, gy, gz), valid, time, st, diag);
-            if (r < nmiss) s_field[s] = valid ? st.d : 0.f;
-        }
-        __syncthreads();
-        if (threadIdx.x < HALO_N) {
-            const int h = (hz * 9 + hy) * 9 + hx;
-            row[h] = s_field[h];
         }
         block_counts(g, a, lin, s_field, s_red, nullptr, block_totals, packet_counts);
     }
