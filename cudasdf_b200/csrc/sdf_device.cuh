@@ -337,6 +337,39 @@ __device__ __forceinline__ bool box_closer(float3 p, float4 a, float4 b, float d
     return SQRT(dd) < dmin;
 }
 
+// The decision of box_closer for one running distance dmin, with the parts that depend on dmin alone
+// computed once per change of dmin: lo / hi are the two fast-path thresholds (lo = hi = -1 when
+// dmin > 0 fails, so every box is rejected; lo = -1, hi = +inf when dmin^2 could under- or overflow,
+// so the square root decides).
+struct PruneBound {
+    float lo, hi, dmin;
+    __device__ __forceinline__ void set(float d) {
+        dmin = d;
+        if (!(d > 0.f)) {
+            lo = -1.f;
+            hi = -1.f;
+        } else if (d >= 1e-18f && d <= 1e18f) {
+            const float d2 = MUL(d, d);
+            lo = MUL(d2, 0x1.ffffep-1f);
+            hi = MUL(d2, 0x1.00001p+0f);
+        } else {
+            lo = -1.f;
+            hi = __int_as_float(0x7f800000);
+        }
+    }
+    __device__ __forceinline__ bool alive() const { return hi >= 0.f; }
+    // box_closer(p, a, b, dmin) for the dmin of the last set()
+    __device__ __forceinline__ bool closer(float3 p, float4 a, float4 b) const {
+        const float dx = fmaxf(fmaxf(SUB(a.x, p.x), SUB(p.x, a.w)), 0.f);
+        const float dy = fmaxf(fmaxf(SUB(a.y, p.y), SUB(p.y, b.x)), 0.f);
+        const float dz = fmaxf(fmaxf(SUB(a.z, p.z), SUB(p.z, b.y)), 0.f);
+        const float dd = FMA(dz, dz, FMA(dx, dx, MUL(dy, dy)));
+        if (dd < lo) return true;
+        if (dd > hi) return false;
+        return SQRT(dd) < dmin;
+    }
+};
+
 // Per-launch diagnostics shared by all kernels of an extraction.
 struct Diag {
     unsigned long long cap_hits;    // points whose search was cut by the 256-pop cap
@@ -364,6 +397,8 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
     const unsigned live = __ballot_sync(FULL, valid);
     int iter = 0;
     if (sc.nnodes > 0 && live) {
+        PruneBound pb;
+        pb.set(st.d);
         // warp stack: entry j lives in lane (j & 31) of register pair A (j < 32) or B (j >= 32)
         int nodeA = 0, nodeB = 0;
         unsigned maskA = 0, maskB = 0;
@@ -390,12 +425,12 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
                 ++cnt_wpops;
             }
             // a node can only pass the prune test for a lane whose running distance is > 0
-            const unsigned alive = __ballot_sync(FULL, pops && st.d > 0.f);
-            if (alive == 0) continue;
+            const bool lane_alive = pops && pb.alive();
+            if (!__any_sync(FULL, lane_alive)) continue;
             if (COUNT) ++cnt_wtests;
             const float4 na = __ldg(sc.nodes + 2 * node);
             const float4 nb = __ldg(sc.nodes + 2 * node + 1);
-            const bool hit = ((alive >> lane) & 1u) && box_closer(p, na, nb, st.d);
+            const bool hit = lane_alive && pb.closer(p, na, nb);
             const unsigned hm = __ballot_sync(FULL, hit);
             if (hm == 0) continue;
             const int left = __float_as_int(nb.z), right = __float_as_int(nb.w);
@@ -410,6 +445,7 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
                     float3 pre;
                     const float dp = leaf_distance(L, p, time, pre);
                     combine<ATTR>(st, L.op, L.pos.w, pr, left, dp, pre);
+                    pb.set(st.d);
                 }
             } else {
                 if (sp + 2 > MAP_STACK) { overflow = true; break; }
