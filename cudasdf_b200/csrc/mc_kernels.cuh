@@ -20,6 +20,7 @@
 namespace sdfb {
 
 constexpr int BLK_THREADS = 256;           // 8 warps per CTA
+static_assert(BLK_THREADS <= 32 * MAP_WARPS, "one map_warp stack per warp");
 constexpr int FIELD_N = 729;               // 9^3 samples of one block incl. the +1 halo
 constexpr int FIELD_STRIDE = 736;          // padded to a multiple of 16 floats (64 B rows)
 constexpr int FIELD_CHUNKS = (FIELD_N + 31) / 32;

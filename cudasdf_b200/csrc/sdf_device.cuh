@@ -76,6 +76,7 @@ struct SceneView {
 constexpr int PRIM_ROWS = 10;
 constexpr int MAP_STACK = 64;   // the reference's per-point stack (MarchingCubesKernels.cu:577)
 constexpr int MAP_CAP = 256;    // the reference's popped-node cap (:582)
+constexpr int MAP_WARPS = 8;    // warps per CTA of every kernel that calls map_warp (one stack each)
 
 // row 0 rotation | 1 dispParams | 2 position, blend | 3 scale, rounding | 4 color, annular |
 // 5 params[0..3] | 6 params[4..5], type, operation | 7 displacement, pad, uvScale |
@@ -396,27 +397,22 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
     st.init();
     const unsigned live = __ballot_sync(FULL, valid);
     int iter = 0;
-    if (sc.nnodes > 0 && live) {
+    // the warp's stack of (node, mask of the lanes that pushed it) in shared memory; a CTA with more
+    // warps than stacks is refused (reported as a stack overflow)
+    __shared__ uint2 s_map_stack[MAP_WARPS][MAP_STACK];
+    bool overflow = blockDim.x > 32 * MAP_WARPS;
+    if (sc.nnodes > 0 && live && !overflow) {
         PruneBound pb;
         pb.set(st.d);
-        // warp stack: entry j lives in lane (j & 31) of register pair A (j < 32) or B (j >= 32)
-        int nodeA = 0, nodeB = 0;
-        unsigned maskA = 0, maskB = 0;
-        int sp = 0;
-        if (lane == 0) { nodeA = 0; maskA = live; }
-        sp = 1;
-        bool overflow = false;
+        uint2* stk = s_map_stack[threadIdx.x >> 5];
+        if (lane == 0) stk[0] = make_uint2(0u, live);
+        __syncwarp();
+        int sp = 1;
         while (sp > 0) {
             --sp;
-            int node;
-            unsigned mask;
-            if (sp < 32) {
-                node = __shfl_sync(FULL, nodeA, sp);
-                mask = __shfl_sync(FULL, maskA, sp);
-            } else {
-                node = __shfl_sync(FULL, nodeB, sp - 32);
-                mask = __shfl_sync(FULL, maskB, sp - 32);
-            }
+            const uint2 e = stk[sp];
+            const int node = (int)e.x;
+            const unsigned mask = e.y;
             // a lane pops this node iff it pushed it and has popped fewer than MAP_CAP nodes
             const bool pops = ((mask >> lane) & 1u) && iter < MAP_CAP;
             if (pops) iter++;
@@ -449,20 +445,21 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
                 }
             } else {
                 if (sp + 2 > MAP_STACK) { overflow = true; break; }
-                if (sp < 32) { if (lane == sp) { nodeA = right; maskA = hm; } }
-                else if (lane == sp - 32) { nodeB = right; maskB = hm; }
-                ++sp;
-                if (sp < 32) { if (lane == sp) { nodeA = left; maskA = hm; } }
-                else if (lane == sp - 32) { nodeB = left; maskB = hm; }
-                ++sp;
+                __syncwarp();  // every lane has read stk[sp] (popped above) before it is overwritten
+                if (lane == 0) {
+                    stk[sp] = make_uint2((unsigned)right, hm);
+                    stk[sp + 1] = make_uint2((unsigned)left, hm);
+                }
+                __syncwarp();
+                sp += 2;
             }
         }
         if (diag) {
             const unsigned capped = __ballot_sync(FULL, valid && iter >= MAP_CAP);
             if (lane == 0 && capped) atomicAdd(&diag->cap_hits, (unsigned long long)__popc(capped));
-            if (lane == 0 && overflow) atomicExch(&diag->stack_overflow, 1);
         }
     }
+    if (diag && overflow && lane == 0) atomicExch(&diag->stack_overflow, 1);
     if (COUNT && diag && lane == 0) {
         const unsigned nlive = __popc(live);
         atomicAdd(&diag->node_pops, cnt_pops);
