@@ -35,7 +35,8 @@ sys.path.insert(0, ROOT)
 CONFIGS = {
     "c1": {"config": 1, "technique": 0, "workload": "mc_sphere_128"},
     "c2": {"config": 2, "technique": 0, "workload": "mc_256prims_256"},
-    "c3": {"config": 3, "technique": 1, "workload": "dc_4096prims_512"},
+    "c3": {"config": 3, "technique": 1, "workload": "dc_masspoint_4096prims_512",
+           "dc": {"dc_solver": 1, "projection_iters": 3, "adaptive_diagonal": 1, "cond_threshold": 1e4}},
     "c4": {"config": 4, "technique": 0, "workload": "mc_16384prims_1024", "surrogate": True},
 }
 
@@ -193,7 +194,7 @@ def run_ours(args, rank, world):
     mask = L.OUT_INDICES
     surrogate = spec.get("surrogate", False) and not args.plain
     eng = Engine()
-    eng.configure(make_config(cell, technique=tech, out_mask=mask))
+    eng.configure(make_config(cell, technique=tech, out_mask=mask, **spec.get("dc", {})))
     eng.set_scene(prims)
     # capacity: one extraction to size the buffers
     probe_buf = MeshBuffers(1 << 20, mask)

@@ -505,6 +505,7 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
         stats->dc_cell_vertices = h.dc_vertices;
         stats->bvh_cap_hits = (int64_t)h.diag.cap_hits;
         stats->scouted_blocks = culled ? (int64_t)h.diag.scouted : (int64_t)nb;
+        stats->dc_fp64_cells = (int64_t)h.diag.fp64_cells;
         stats->ms_total = std::chrono::duration<float, std::milli>(t1 - t0).count();
         if (E.timing) {
             cudaEventElapsedTime(&stats->ms_scout, E.ev[0], E.ev[1]);

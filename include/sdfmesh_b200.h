@@ -197,7 +197,8 @@ typedef struct sdf_config {
     int32_t dc_solver;          /* SDF_DC_SOLVER_* */
     int32_t projection_iters;   /* mass-point solver: vertex projection iterations (0 = off) */
     int32_t adaptive_diagonal;  /* mass-point solver: split quads along the shorter diagonal */
-    float cond_threshold;       /* mass-point solver: FP64 eigensolve above this condition number */
+    float cond_threshold;       /* mass-point solver: pseudo-inverse truncation at lmax / cond_threshold;
+                                   cells with condition number above cond_threshold / 16 are solved in FP64 */
     uint32_t out_mask;          /* SDF_OUT_* streams to write (positions are always written) */
 } sdf_config;
 
@@ -220,6 +221,7 @@ typedef struct sdf_stats {
     int64_t bvh_cap_hits;       /* points whose traversal stopped at the 256-visit cap */
     float ms_scout, ms_field, ms_scan, ms_emit, ms_total; /* filled when timing is enabled */
     int64_t scouted_blocks;     /* blocks whose centre the exact scout evaluated (all, unless culled) */
+    int64_t dc_fp64_cells;      /* mass-point DC: cells whose QEF was solved in FP64 (condition number) */
 } sdf_stats;
 
 typedef struct sdf_engine sdf_engine;
