@@ -426,6 +426,8 @@ def main():
 # 3 products, 3 cross terms, 3 x (2 FMA + 1 mul), 3 divisions), the primitive's distance (about 12)
 # and the smooth-union blend (about 12).
 FLOP_PER_NODE = 12
+# DRAM bytes per active block of the block-field stage, from an ncu capture (see roofline())
+TRAFFIC_PER_ACTIVE_BLOCK = (14.304768e6 + 14.137600e6) / 12524
 FLOP_PER_LEAF = 44 + 12 + 12 + 1
 
 
@@ -437,11 +439,16 @@ def roofline(r):
         return None
     flops = c["field_node_visits"] * FLOP_PER_NODE + c["field_leaf_evals"] * FLOP_PER_LEAF
     achieved = flops / (ms_field * 1e-3) / 1e12
-    return {"kernel": "k_field_own + k_field_halo (block field: warp-coherent BVH map())", "bound": "fp32",
+    active = r["stats"]["active_blocks"]
+    return {"kernel": "block field stage (k_field_own + k_field_miss: warp-coherent BVH map())", "bound": "fp32",
             "achieved": achieved,
             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": "measured by the library's FMA loop on this GPU (no FP32 figure in MEASURED_PEAKS.json)",
-            "traffic": None, "work": c}
+            "traffic": TRAFFIC_PER_ACTIVE_BLOCK * active,
+            "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one k_field_own capture on the "
+                              "256^3 workload (profiles/k_field_own_mc_256prims_256.md), 2.27 KB per active block, "
+                              "scaled by this run's active blocks",
+            "work": c}
 
 
 if __name__ == "__main__":
