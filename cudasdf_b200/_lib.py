@@ -61,6 +61,21 @@ class SurrogateStats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class BatchScene(ctypes.Structure):
+    _fields_ = [("prims", ctypes.c_void_p), ("count", ctypes.c_int32), ("config", SdfConfig)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("scenes", ctypes.c_int64), ("total_blocks", ctypes.c_int64), ("active_blocks", ctypes.c_int64),
+                ("mc_vertices", ctypes.c_int64), ("dc_vertices", ctypes.c_int64), ("ms_total", ctypes.c_float),
+                ("graph", ctypes.c_int32), ("tuned_ctas", ctypes.c_int32 * 4)]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_}
+        d["tuned_ctas"] = list(self.tuned_ctas)
+        return d
+
+
 class SdfGrid(ctypes.Structure):
     """The reference's SDFGrid (Commons.cuh:115-186), 232 bytes."""
     _fields_ = [("d_activeBlocks", ctypes.c_void_p), ("d_activeBlockCount", ctypes.c_void_p),
@@ -90,6 +105,8 @@ DROPIN_SYMBOLS = ["launchScoutActiveBlocks", "launchCountActiveBlockTriangles", 
 SURROGATE_SYMBOLS = ["sdf_surrogate_default_config", "sdf_surrogate_train", "sdf_surrogate_enable",
                      "sdf_surrogate_audit", "sdf_surrogate_num_params", "sdf_surrogate_set_params",
                      "sdf_surrogate_get_params", "sdf_surrogate_forward", "sdf_surrogate_gradient"]
+BATCH_SYMBOLS = ["sdf_batch_create", "sdf_batch_destroy", "sdf_batch_set_scenes", "sdf_batch_extract",
+                 "sdf_batch_capture"]
 STATIC_SCOUT_SYMBOLS = ["sdf_scout_active_blocks_static", "sdf_scout_static_max_blocks"]
 ENGINE_SYMBOLS = ["sdf_engine_create", "sdf_engine_destroy", "sdf_engine_configure", "sdf_engine_set_scene",
                   "sdf_engine_extract", "sdf_engine_set_timing", "sdf_engine_set_debug", "sdf_engine_get_bvh",
@@ -172,6 +189,17 @@ def lib():
     L.sdf_surrogate_forward.restype = i
     L.sdf_surrogate_gradient.argtypes = [vp, vp, vp, i, vp, vp]
     L.sdf_surrogate_gradient.restype = i
+    L.sdf_batch_create.argtypes = [ctypes.POINTER(vp), i]
+    L.sdf_batch_create.restype = i
+    L.sdf_batch_destroy.argtypes = [vp]
+    L.sdf_batch_destroy.restype = None
+    L.sdf_batch_set_scenes.argtypes = [vp, ctypes.POINTER(BatchScene), i, u]
+    L.sdf_batch_set_scenes.restype = i
+    L.sdf_batch_extract.argtypes = [vp, f, ctypes.POINTER(SdfOutputs), ctypes.POINTER(SdfOutputs), vp, vp, vp,
+                                    ctypes.POINTER(BatchStats)]
+    L.sdf_batch_extract.restype = i
+    L.sdf_batch_capture.argtypes = [vp, f, ctypes.POINTER(SdfOutputs), ctypes.POINTER(SdfOutputs), vp, i]
+    L.sdf_batch_capture.restype = i
     L.sdf_scout_active_blocks_static.argtypes = [G, f]
     L.sdf_scout_active_blocks_static.restype = i
     L.sdf_scout_static_max_blocks.restype = u

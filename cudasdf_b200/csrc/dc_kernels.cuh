@@ -48,7 +48,7 @@ __global__ void k_dc_block_map(const int* __restrict__ list, const int* __restri
 
 // dcMarkCells (:1312-1346): corner masks + has-vertex counts. With fields_out the block field is
 // also stored for the solve pass.
-__global__ void __launch_bounds__(BLK_THREADS) k_dc_mark(GridView g, SceneView sc, float time, ActiveView av,
+__global__ void __launch_bounds__(BLK_THREADS) k_dc_mark(GridView g0, SceneView sc0, float time, ActiveView av,
                                                          float* __restrict__ fields_out, DcBuffers B, unsigned* ticket,
                                                          Diag* diag) {
     __shared__ __align__(16) float s_field[FIELD_STRIDE];
@@ -57,7 +57,11 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_mark(GridView g, SceneView s
     for (;;) {
         const int a = claim(ticket, n, &s_item);
         if (a < 0) break;
-        const int lin = av.list[a];
+        GridView g = g0;
+        SceneView sc = sc0;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[a], g, sc, lin, bbase);
         eval_block_field(g, sc, time, lin, s_field, diag);
         if (threadIdx.x < FIELD_STRIDE - FIELD_N) s_field[FIELD_N + threadIdx.x] = 0.f;
         __syncthreads();
@@ -300,7 +304,7 @@ __device__ __forceinline__ float3 value_gradient_warp(const SceneView& sc, float
     return f3(0.f, 0.f, 0.f);
 }
 
-__global__ void __launch_bounds__(BLK_THREADS) k_dc_solve(GridView g, SceneView sc, float time, ActiveView av,
+__global__ void __launch_bounds__(BLK_THREADS) k_dc_solve(GridView g0, SceneView sc0, float time, ActiveView av,
                                                           const float* __restrict__ fields_in, DcBuffers B,
                                                           DcSolveParams P, unsigned* ticket, Diag* diag) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -310,7 +314,11 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_solve(GridView g, SceneView 
     for (;;) {
         const int a = claim(ticket, n, &S.item);
         if (a < 0) break;
-        const int lin = av.list[a];
+        GridView g = g0;
+        SceneView sc = sc0;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[a], g, sc, lin, bbase);
         if (fields_in) {
             const float4* src = reinterpret_cast<const float4*>(fields_in + (size_t)a * FIELD_STRIDE);
             float4* dst = reinterpret_cast<float4*>(S.field);
@@ -576,39 +584,47 @@ __device__ __forceinline__ bool quad_cells(const GridView& g, const int* b2a, in
 __device__ __forceinline__ int edge_corner(int axis) { return axis == 0 ? 1 : (axis == 1 ? 3 : 4); }
 
 // dcCountQuads (:1714-1784); block_totals (optional) gets the per-block sum
-__global__ void k_dc_count_quads(GridView g, ActiveView av, DcBuffers B, unsigned* __restrict__ counts,
+__global__ void k_dc_count_quads(GridView g0, ActiveView av, DcBuffers B, unsigned* __restrict__ counts,
                                  unsigned* __restrict__ block_totals) {
     __shared__ unsigned s_red[16];
-    const int a = blockIdx.x;
-    if (a >= active_count(av)) return;
+    const int n = active_count(av);
     const int tid = threadIdx.x;
-    int bx, by, bz;
-    block_coord(g, av.list[a], bx, by, bz);
-    const size_t pk = (size_t)a * 512 + tid;
-    const CellInfo c = cell_info(g, bx, by, bz, tid);
-    unsigned cnt = 0;
-    if (!c.oob) {
-        const unsigned char mask = B.masks[pk];
-        const unsigned s0 = mask & 1u;
-        for (int axis = 0; axis < 3; ++axis) {
-            if (((mask >> edge_corner(axis)) & 1u) == s0) continue;
-            int q[4];
-            if (quad_cells(g, B.block_to_active, axis, c.x, c.y, c.z, q) && surface_mask(B.masks[q[0]]) &&
-                surface_mask(B.masks[q[1]]) && surface_mask(B.masks[q[2]]) && surface_mask(B.masks[q[3]]))
-                cnt += 6;
+    for (int a = blockIdx.x; a < n; a += gridDim.x) {
+        GridView g = g0;
+        SceneView unused;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[a], g, unused, lin, bbase);
+        const int* b2a = B.block_to_active + bbase;  // this scene's block-to-active map
+        int bx, by, bz;
+        block_coord(g, lin, bx, by, bz);
+        const size_t pk = (size_t)a * 512 + tid;
+        const CellInfo c = cell_info(g, bx, by, bz, tid);
+        unsigned cnt = 0;
+        if (!c.oob) {
+            const unsigned char mask = B.masks[pk];
+            const unsigned s0 = mask & 1u;
+            for (int axis = 0; axis < 3; ++axis) {
+                if (((mask >> edge_corner(axis)) & 1u) == s0) continue;
+                int q[4];
+                if (quad_cells(g, b2a, axis, c.x, c.y, c.z, q) && surface_mask(B.masks[q[0]]) &&
+                    surface_mask(B.masks[q[1]]) && surface_mask(B.masks[q[2]]) && surface_mask(B.masks[q[3]]))
+                    cnt += 6;
+            }
         }
-    }
-    counts[pk] = cnt;
-    if (block_totals) {
-        unsigned v = cnt;
+        counts[pk] = cnt;
+        if (block_totals) {
+            unsigned v = cnt;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((tid & 31) == 0) s_red[tid >> 5] = v;
-        __syncthreads();
-        if (tid == 0) {
-            unsigned s = 0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += s_red[w];
-            block_totals[a] = s;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if ((tid & 31) == 0) s_red[tid >> 5] = v;
+            __syncthreads();
+            if (tid == 0) {
+                unsigned s = 0;
+                for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += s_red[w];
+                block_totals[a] = s;
+            }
+            __syncthreads();  // s_red is free for the next block
         }
     }
 }
@@ -632,24 +648,25 @@ struct QuadVerts {
     float3 qc;
 };
 
-__device__ __forceinline__ float3 cell_min_of_packet(const GridView& g, const int* list, int packet) {
+__device__ __forceinline__ float3 cell_min_of_packet(const GridView& g, const int* list, unsigned base, int packet) {
     const int ab = packet >> 9, t = packet & 511;
     int bx, by, bz;
-    block_coord(g, list[ab], bx, by, bz);
+    block_coord(g, list[ab] - (int)base, bx, by, bz);
     const CellInfo c = cell_info(g, bx, by, bz, t);
     return grid_loc(g, c.x, c.y, c.z);
 }
 
 // decodes the quad's four vertices (:1851-1875); false when a vertex index is out of range (the
 // reference then skips the quad without advancing its write cursor)
-__device__ __forceinline__ bool quad_vertices(const GridView& g, const int* list, const DcBuffers& B, const int q[4],
-                                              unsigned maxV, QuadVerts& Q) {
+__device__ __forceinline__ bool quad_vertices(const GridView& g, const int* list, unsigned base, const DcBuffers& B,
+                                              const int q[4], unsigned maxV, QuadVerts& Q) {
     unsigned vi[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) vi[j] = B.vert_offsets[q[j]];
     if (vi[0] >= maxV || vi[1] >= maxV || vi[2] >= maxV || vi[3] >= maxV) return false;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) Q.v[j] = decode_vertex(B.cell_verts[vi[j]], cell_min_of_packet(g, list, q[j]), g.cell);
+    for (int j = 0; j < 4; ++j)
+        Q.v[j] = decode_vertex(B.cell_verts[vi[j]], cell_min_of_packet(g, list, base, q[j]), g.cell);
     Q.qc = f3(MUL(0.25f, ADD(ADD(ADD(Q.v[0].x, Q.v[1].x), Q.v[2].x), Q.v[3].x)),
               MUL(0.25f, ADD(ADD(ADD(Q.v[0].y, Q.v[1].y), Q.v[2].y), Q.v[3].y)),
               MUL(0.25f, ADD(ADD(ADD(Q.v[0].z, Q.v[1].z), Q.v[2].z), Q.v[3].z)));
@@ -664,7 +681,7 @@ __device__ __forceinline__ bool quad_indices_ok(const DcBuffers& B, const int q[
            B.vert_offsets[q[3]] < maxV;
 }
 
-__global__ void __launch_bounds__(BLK_THREADS) k_dc_quads(GridView g, SceneView sc, float time, ActiveView av,
+__global__ void __launch_bounds__(BLK_THREADS) k_dc_quads(GridView g0, SceneView sc0, float time, ActiveView av,
                                                           DcBuffers B, const unsigned* __restrict__ offsets,
                                                           const unsigned* __restrict__ counts,
                                                           const unsigned* __restrict__ block_offsets, MeshOut out,
@@ -678,8 +695,14 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quads(GridView g, SceneView 
     for (;;) {
         const int a = claim(ticket, n, &S.item);
         if (a < 0) break;
+        GridView g = g0;
+        SceneView sc = sc0;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[a], g, sc, lin, bbase);
+        const int* b2a = B.block_to_active + bbase;  // this scene's block-to-active map
         int bx, by, bz;
-        block_coord(g, av.list[a], bx, by, bz);
+        block_coord(g, lin, bx, by, bz);
         // cell offsets: per-cell (drop-in layout) or block offset + in-block scan of the counts
         unsigned cnt[2], off[2];
 #pragma unroll
@@ -711,7 +734,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quads(GridView g, SceneView 
                 for (int axis = 0; axis < 3; ++axis) {
                     if (((m >> edge_corner(axis)) & 1u) == s0) continue;
                     int q[4];
-                    if (!quad_cells(g, B.block_to_active, axis, c.x, c.y, c.z, q)) continue;
+                    if (!quad_cells(g, b2a, axis, c.x, c.y, c.z, q)) continue;
                     if (!surface_mask(B.masks[q[0]]) || !surface_mask(B.masks[q[1]]) || !surface_mask(B.masks[q[2]]) ||
                         !surface_mask(B.masks[q[3]]))
                         continue;
@@ -740,8 +763,8 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quads(GridView g, SceneView 
                     const int tid = S.q_cell[i] >> 2, axis = S.q_cell[i] & 3;
                     const CellInfo c = cell_info(g, bx, by, bz, tid);
                     int q[4];
-                    quad_cells(g, B.block_to_active, axis, c.x, c.y, c.z, q);
-                    valid = quad_vertices(g, av.list, B, q, out.maxV, Q);
+                    quad_cells(g, b2a, axis, c.x, c.y, c.z, q);
+                    valid = quad_vertices(g, av.list, bbase, B, q, out.maxV, Q);
                     w = S.q_out[i];
                 }
                 const float3 nref = normal_warp(sc, Q.qc, valid, time, g.cell, diag);
@@ -819,9 +842,9 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quads(GridView g, SceneView 
                         const int tid = S.q_cell[qi] >> 2, axis = S.q_cell[qi] & 3;
                         const CellInfo c = cell_info(g, bx, by, bz, tid);
                         int q[4];
-                        quad_cells(g, B.block_to_active, axis, c.x, c.y, c.z, q);
+                        quad_cells(g, b2a, axis, c.x, c.y, c.z, q);
                         QuadVerts Q;
-                        valid = quad_vertices(g, av.list, B, q, out.maxV, Q);
+                        valid = quad_vertices(g, av.list, bbase, B, q, out.maxV, Q);
                         if (valid) {
                             const unsigned char fl = S.q_flags[qi];
                             if (fl & 1) { const float3 t = Q.v[1]; Q.v[1] = Q.v[3]; Q.v[3] = t; }

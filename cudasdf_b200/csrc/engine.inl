@@ -475,7 +475,7 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
             gv, sv, time, av, E.fields, B, sp, &ctrl->tickets[1], diag);
         check_launch();
         if (E.timing) cudaEventRecord(E.ev[3], st);
-        k_dc_count_quads<<<nb, 512, 0, st>>>(gv, av, B, E.packet_counts, E.block_totals);
+        k_dc_count_quads<<<std::min(nb, num_sms() * 4), 512, 0, st>>>(gv, av, B, E.packet_counts, E.block_totals);
         check_launch();
         k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)nb)), SCAN_THREADS, 0, st>>>(
             E.block_totals, E.block_offsets, 0, &ctrl->active_count, 1, scan_state(scanB), &ctrl->total_vertices, diag);

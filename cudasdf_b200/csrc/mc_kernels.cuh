@@ -29,11 +29,48 @@ constexpr int MAX_BLOCK_TRIS = 512 * 5;    // upper bound of triangles in one bl
 // marching-cubes case table (re-encoded reference table, see gen_mc_cases.py)
 __constant__ unsigned long long c_mcCases[256] = {SDF_MC_CASE_WORDS};
 
+// One scene of a batched extraction: its grid, its primitives and BVH, and where its blocks start in
+// the batch's global block numbering (scene s owns global blocks [block_base, block_base + blocks)).
+struct SceneDesc {
+    GridView g;
+    SceneView sc;
+    unsigned block_base;
+    unsigned brick_base;   // first global scout brick (4 x 4 x 2 blocks) of the scene
+};
+
 struct ActiveView {
     const int* list;       // active block linear indices, ascending
     const int* count_dev;  // device-side active count
     int cap;               // host-side bound (numActiveBlocks of the drop-in launchers)
+    const SceneDesc* scenes = nullptr;  // batched extraction: list entries are global block indices
+    int nscenes = 0;
 };
+
+// the scene owning global block e (the last scene whose block_base is <= e)
+__device__ __forceinline__ int scene_of_block(const SceneDesc* s, int n, unsigned e) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s[mid].block_base <= e) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Active-list entry -> the grid and scene it belongs to, its block index inside that scene and the
+// scene's first global block (0 and the kernel's own grid / scene outside a batch).
+__device__ __forceinline__ void resolve(const ActiveView& av, int entry, GridView& g, SceneView& sc, int& lin,
+                                        unsigned& base) {
+    if (!av.scenes) {
+        lin = entry;
+        base = 0u;
+        return;
+    }
+    const SceneDesc& d = av.scenes[scene_of_block(av.scenes, av.nscenes, (unsigned)entry)];
+    g = d.g;
+    sc = d.sc;
+    base = d.block_base;
+    lin = entry - (int)base;
+}
 
 struct MeshOut {
     float4* verts;
@@ -176,6 +213,25 @@ __device__ __forceinline__ CellInfo cell_info(const GridView& g, int bx, int by,
 // centres of a warp are spatially close and their BVH walks coincide; the result is a 0/1 flag per
 // linear block index, compacted in index order afterwards.
 // ------------------------------------------------------------------------------------------------
+// scoutActiveBlocks (MarchingCubesKernels.cu:850-889) for one brick of 4 x 4 x 2 blocks: one warp,
+// one lane per block centre
+__device__ __forceinline__ void scout_brick(const GridView& g, const SceneView& sc, float time, int wx, int wy, int wz,
+                                            unsigned* flags, Diag* diag) {
+    const int lane = threadIdx.x & 31;
+    const int bx = wx * 4 + (lane & 3), by = wy * 4 + ((lane >> 2) & 3), bz = wz * 2 + (lane >> 4);
+    const bool valid = bx < g.bx && by < g.by && bz < g.bz;
+    const float3 c = f3(FMA(ADD((float)(bx * 8), 4.f), g.cell, g.ox), FMA(ADD((float)(by * 8), 4.f), g.cell, g.oy),
+                        FMA(ADD((float)(bz * 8), 4.f), g.cell, g.oz));
+    MapState<false> st;
+    map_warp<false>(sc, c, valid, time, st, diag);
+    const float r = MUL(8 * 0.5f * 1.73205f + 2.0f, g.cell);
+    if (valid) flags[bx + g.bx * (by + g.by * bz)] = fabsf(st.d) <= r ? 1u : 0u;
+}
+
+__device__ __forceinline__ int scout_bricks(const GridView& g) {
+    return ((g.bx + 3) >> 2) * ((g.by + 3) >> 2) * ((g.bz + 1) >> 1);
+}
+
 // CULL: the brick lies in coarse block (wx, wy, wz / 2) of 4 x 4 x 4 blocks (32^3 cells); when the
 // surrogate's value at that coarse block's centre exceeds `margin` in magnitude, the brick's blocks
 // are marked inactive without evaluating the scene.
@@ -188,9 +244,9 @@ __global__ void __launch_bounds__(BLK_THREADS) k_scout_t(GridView g, SceneView s
     const int nbx = (g.bx + 3) >> 2, nby = (g.by + 3) >> 2, nbz = (g.bz + 1) >> 1;
     if (warp_global >= nbx * nby * nbz) return;
     const int wx = warp_global % nbx, t = warp_global / nbx, wy = t % nby, wz = t / nby;
-    const int bx = wx * 4 + (lane & 3), by = wy * 4 + ((lane >> 2) & 3), bz = wz * 2 + (lane >> 4);
-    const bool valid = bx < g.bx && by < g.by && bz < g.bz;
     if (CULL) {
+        const int bx = wx * 4 + (lane & 3), by = wy * 4 + ((lane >> 2) & 3), bz = wz * 2 + (lane >> 4);
+        const bool valid = bx < g.bx && by < g.by && bz < g.bz;
         const float fc = coarse_f[wx + nbx * (wy + nby * (wz >> 1))];
         if (fabsf(fc) > margin) {
             if (valid) flags[bx + g.bx * (by + g.by * bz)] = 0u;
@@ -199,12 +255,48 @@ __global__ void __launch_bounds__(BLK_THREADS) k_scout_t(GridView g, SceneView s
         const unsigned v = __ballot_sync(0xffffffffu, valid);
         if (lane == 0) atomicAdd(&diag->scouted, (unsigned long long)__popc(v));
     }
-    const float3 c = f3(FMA(ADD((float)(bx * 8), 4.f), g.cell, g.ox), FMA(ADD((float)(by * 8), 4.f), g.cell, g.oy),
-                        FMA(ADD((float)(bz * 8), 4.f), g.cell, g.oz));
-    MapState<false> st;
-    map_warp<false>(sc, c, valid, time, st, diag);
-    const float r = MUL(8 * 0.5f * 1.73205f + 2.0f, g.cell);
-    if (valid) flags[bx + g.bx * (by + g.by * bz)] = fabsf(st.d) <= r ? 1u : 0u;
+    scout_brick(g, sc, time, wx, wy, wz, flags, diag);
+}
+
+// the scout of every scene of a batch in one launch: global brick -> scene -> brick of that scene;
+// flags are in the batch's global block numbering
+__global__ void __launch_bounds__(BLK_THREADS) k_scout_batch(const SceneDesc* __restrict__ scenes, int nscenes,
+                                                             unsigned total_bricks, float time, unsigned* flags,
+                                                             Diag* diag) {
+    const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (w >= total_bricks) return;
+    int lo = 0, hi = nscenes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (scenes[mid].brick_base <= w) lo = mid; else hi = mid - 1;
+    }
+    const SceneDesc& d = scenes[lo];
+    const GridView g = d.g;
+    const int local = (int)(w - d.brick_base);
+    const int nbx = (g.bx + 3) >> 2, nby = (g.by + 3) >> 2;
+    const int wx = local % nbx, t = local / nbx, wy = t % nby, wz = t / nby;
+    scout_brick(g, d.sc, time, wx, wy, wz, flags + d.block_base, diag);
+}
+
+// first output vertex of every scene of a batch: the offset of its first active block (the active
+// list is ascending in global block numbering, so each scene's blocks are one run of it)
+__global__ void k_batch_scene_first(const SceneDesc* __restrict__ scenes, int nscenes, ActiveView av,
+                                    const unsigned* __restrict__ block_offsets, const unsigned* __restrict__ total,
+                                    unsigned* __restrict__ first) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s > nscenes) return;
+    const int n = active_count(av);
+    if (s == nscenes) {
+        first[s] = *total;
+        return;
+    }
+    const unsigned b = scenes[s].block_base;
+    int lo = 0, hi = n;  // first active entry with a global block index >= b
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if ((unsigned)av.list[mid] < b) lo = mid + 1; else hi = mid;
+    }
+    first[s] = lo < n ? block_offsets[lo] : *total;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -312,7 +404,7 @@ __device__ __forceinline__ int halo_owner(const GridView& g, int bx, int by, int
 }
 
 // one thread per (active block, halo sample); missing samples are listed as (a << 8) | h
-__global__ void __launch_bounds__(256) k_field_plan(GridView g, ActiveView av, const unsigned* __restrict__ flags,
+__global__ void __launch_bounds__(256) k_field_plan(GridView g0, ActiveView av, const unsigned* __restrict__ flags,
                                                     float* __restrict__ fields, int* __restrict__ block_to_active,
                                                     unsigned* __restrict__ miss, unsigned* __restrict__ miss_count) {
     const int n = active_count(av);
@@ -325,8 +417,12 @@ __global__ void __launch_bounds__(256) k_field_plan(GridView g, ActiveView av, c
         if (i < total) {
             a = (int)(i / HALO_N);
             h = (int)(i - (long long)a * HALO_N);
-            const int lin = av.list[a];
-            if (h == 0) block_to_active[lin] = a;
+            GridView g = g0;
+            SceneView unused;
+            int lin;
+            unsigned bbase;
+            resolve(av, av.list[a], g, unused, lin, bbase);
+            if (h == 0) block_to_active[bbase + lin] = a;
             int bx, by, bz, hx, hy, hz;
             block_coord(g, lin, bx, by, bz);
             halo_coord(h, hx, hy, hz);
@@ -334,7 +430,7 @@ __global__ void __launch_bounds__(256) k_field_plan(GridView g, ActiveView av, c
             if (olin < 0)
                 fields[(size_t)a * FIELD_STRIDE + (hz * 9 + hy) * 9 + hx] = 0.f;  // outside the grid
             else
-                m = flags[olin] == 0u;
+                m = flags[bbase + olin] == 0u;
         }
         const unsigned bal = __ballot_sync(0xffffffffu, m);
         unsigned base = 0;
@@ -347,7 +443,7 @@ __global__ void __launch_bounds__(256) k_field_plan(GridView g, ActiveView av, c
 // own samples: one CTA per active block, its eight warps on the sixteen 4 x 4 x 2 Morton bricks (all
 // warps of the SM walk the BVH near the same block, which keeps the nodes they read in L1)
 template <bool COUNT>
-__global__ void __launch_bounds__(BLK_THREADS) k_field_own(GridView g, SceneView sc, float time, ActiveView av,
+__global__ void __launch_bounds__(BLK_THREADS) k_field_own(GridView g0, SceneView sc0, float time, ActiveView av,
                                                          float* __restrict__ fields, unsigned* ticket, Diag* diag) {
     __shared__ int s_item;
     const int n = active_count(av);
@@ -355,8 +451,13 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_own(GridView g, SceneView
     for (;;) {
         const int a = claim(ticket, n, &s_item);
         if (a < 0) break;
+        GridView g = g0;
+        SceneView sc = sc0;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[a], g, sc, lin, bbase);
         int bx, by, bz;
-        block_coord(g, av.list[a], bx, by, bz);
+        block_coord(g, lin, bx, by, bz);
         for (int chunk = warp; chunk < OWN_TASKS; chunk += nwarps) {
             const int r = chunk * 32 + lane;
             const int sx = (r & 1) | ((r >> 2) & 2) | ((r >> 4) & 4);
@@ -373,7 +474,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_own(GridView g, SceneView
 
 // listed halo samples, 32 per warp task, tasks claimed one at a time by each warp
 template <bool COUNT>
-__global__ void __launch_bounds__(BLK_THREADS) k_field_miss(GridView g, SceneView sc, float time, ActiveView av,
+__global__ void __launch_bounds__(BLK_THREADS) k_field_miss(GridView g0, SceneView sc0, float time, ActiveView av,
                                                           float* __restrict__ fields,
                                                           const unsigned* __restrict__ miss,
                                                           const unsigned* __restrict__ miss_count, unsigned* ticket,
@@ -390,18 +491,33 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_miss(GridView g, SceneVie
         const bool live = e < nmiss;
         const unsigned m = live ? miss[e] : miss[t * 32];
         const int a = (int)(m >> 8);
+        GridView g = g0;
+        SceneView sc = sc0;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[a], g, sc, lin, bbase);
         int sx, sy, sz, bx, by, bz;
         halo_coord((int)(m & 255u), sx, sy, sz);
-        block_coord(g, av.list[a], bx, by, bz);
+        block_coord(g, lin, bx, by, bz);
         const int gx = bx * 8 + sx, gy = by * 8 + sy, gz = bz * 8 + sz;
-        const bool valid = live && gx < g.w && gy < g.h && gz < g.d;
-        MapState<false> st;
-        map_warp<false, COUNT>(sc, grid_loc(g, gx, gy, gz), valid, time, st, diag);
-        if (live) fields[(size_t)a * FIELD_STRIDE + (sz * 9 + sy) * 9 + sx] = valid ? st.d : 0.f;
+        const bool inside = live && gx < g.w && gy < g.h && gz < g.d;
+        const float3 p = grid_loc(g, gx, gy, gz);
+        // the warp walks one scene's BVH at a time (a batch's tasks can straddle two scenes)
+        unsigned pending = __ballot_sync(0xffffffffu, live);
+        while (pending) {
+            const unsigned lead_base = __shfl_sync(0xffffffffu, bbase, __ffs(pending) - 1);
+            const bool mine = live && bbase == lead_base && ((pending >> lane) & 1u);
+            SceneView scw = sc;
+            if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead_base)].sc;
+            MapState<false> st;
+            map_warp<false, COUNT>(scw, p, mine && inside, time, st, diag);
+            if (mine) fields[(size_t)a * FIELD_STRIDE + (sz * 9 + sy) * 9 + sx] = inside ? st.d : 0.f;
+            pending &= ~__ballot_sync(0xffffffffu, mine);
+        }
     }
 }
 
-__global__ void __launch_bounds__(BLK_THREADS) k_field_gather(GridView g, ActiveView av, float* __restrict__ fields,
+__global__ void __launch_bounds__(BLK_THREADS) k_field_gather(GridView g0, ActiveView av, float* __restrict__ fields,
                                                             const int* __restrict__ block_to_active,
                                                             const unsigned* __restrict__ flags,
                                                             unsigned* __restrict__ block_totals,
@@ -414,7 +530,11 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_gather(GridView g, Active
     for (;;) {
         const int a = claim(ticket, n, &s_item);
         if (a < 0) break;
-        const int lin = av.list[a];
+        GridView g = g0;
+        SceneView unused;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[a], g, unused, lin, bbase);
         int bx, by, bz;
         block_coord(g, lin, bx, by, bz);
         float* row = fields + (size_t)a * FIELD_STRIDE;
@@ -428,8 +548,8 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_gather(GridView g, Active
             int hx, hy, hz;
             halo_coord(threadIdx.x, hx, hy, hz);
             const int olin = halo_owner(g, bx, by, bz, hx, hy, hz);
-            if (olin >= 0 && flags[olin]) {
-                const int b = block_to_active[olin];
+            if (olin >= 0 && flags[bbase + olin]) {
+                const int b = block_to_active[bbase + olin];
                 const int h = (hz * 9 + hy) * 9 + hx;
                 const float v = fields[(size_t)b * FIELD_STRIDE + ((hz & 7) * 9 + (hy & 7)) * 9 + (hx & 7)];
                 s_field[h] = v;
@@ -551,7 +671,7 @@ __device__ void emit_attributes(const GridView& g, const SceneView& sc, float ti
 // Modes: FIELD_FROM (fields_in != nullptr: load the stored field; else evaluate it) and OFFSETS_FROM
 // (packet_offsets_in != nullptr: per-cell offsets of the drop-in layout; else block_offsets + an
 // in-block scan).
-__global__ void __launch_bounds__(BLK_THREADS) k_mc_emit(GridView g, SceneView sc, float time, ActiveView av,
+__global__ void __launch_bounds__(BLK_THREADS) k_mc_emit(GridView g0, SceneView sc0, float time, ActiveView av,
                                                          const float* __restrict__ fields_in,
                                                          const unsigned* __restrict__ block_offsets,
                                                          const unsigned* __restrict__ packet_offsets_in,
@@ -563,7 +683,11 @@ __global__ void __launch_bounds__(BLK_THREADS) k_mc_emit(GridView g, SceneView s
     for (;;) {
         const int a = claim(ticket, n, &S.item);
         if (a < 0) break;
-        const int lin = av.list[a];
+        GridView g = g0;
+        SceneView sc = sc0;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[a], g, sc, lin, bbase);
         if (fields_in) {
             const float4* src = reinterpret_cast<const float4*>(fields_in + (size_t)a * FIELD_STRIDE);
             float4* dst = reinterpret_cast<float4*>(S.field);

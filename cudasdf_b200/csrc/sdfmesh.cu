@@ -349,4 +349,5 @@ const char* sdf_version(void) { return "sdfmesh_b200 0.1 (sm_100a)"; }
 
 #include "engine.inl"
 #include "surrogate.inl"
+#include "batch.inl"
 #include "noalloc.inl"

@@ -219,3 +219,58 @@ class Engine:
             L.check(self._lib.sdf_engine_read_buffer(self.h, int(which), out.ctypes.data, out.nbytes),
                     "sdf_engine_read_buffer")
         return out
+
+
+class Batch:
+    """Many scenes meshed together (sdf_batch_* in include/sdfmesh_b200.h).
+
+    scenes: list of (primitives, SdfConfig). Marching-cubes scenes write one concatenated soup into
+    the mc buffers, dual-contouring scenes into the dc buffers."""
+
+    def __init__(self, device: int = -1):
+        self._lib = L.lib()
+        h = ctypes.c_void_p()
+        L.check(self._lib.sdf_batch_create(ctypes.byref(h), int(device)), "sdf_batch_create")
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if self.h:
+            self._lib.sdf_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_scenes(self, scenes, out_mask: int):
+        self._keep = [np.ascontiguousarray(p, dtype=PRIM_DTYPE) for p, _ in scenes]
+        arr = (L.BatchScene * len(scenes))()
+        for k, ((_, cfg), p) in enumerate(zip(scenes, self._keep)):
+            arr[k].prims = p.ctypes.data
+            arr[k].count = len(p)
+            arr[k].config = cfg
+        L.check(self._lib.sdf_batch_set_scenes(self.h, arr, len(scenes), int(out_mask)), "sdf_batch_set_scenes")
+        self.n = len(scenes)
+
+    def _outs(self, mc: MeshBuffers, dc: MeshBuffers):
+        return (ctypes.byref(mc.c_struct()) if mc is not None else None,
+                ctypes.byref(dc.c_struct()) if dc is not None else None)
+
+    def capture(self, mc: MeshBuffers, dc: MeshBuffers, time: float = 0.0, tune: bool = True, stream=None):
+        om, od = self._outs(mc, dc)
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        L.check(self._lib.sdf_batch_capture(self.h, float(time), om, od, sp, 1 if tune else 0), "sdf_batch_capture")
+
+    def extract(self, mc: MeshBuffers, dc: MeshBuffers, time: float = 0.0, stream=None):
+        """Returns (first_vertex, vertex_count, stats)."""
+        om, od = self._outs(mc, dc)
+        first = np.zeros(self.n, np.int64)
+        count = np.zeros(self.n, np.int64)
+        st = L.BatchStats()
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        L.check(self._lib.sdf_batch_extract(self.h, float(time), om, od, sp, first.ctypes.data, count.ctypes.data,
+                                            ctypes.byref(st)), "sdf_batch_extract")
+        return first, count, st.as_dict()

@@ -353,6 +353,53 @@ sdf_status sdf_surrogate_forward(sdf_engine* e, const float* d_points, int n, fl
 sdf_status sdf_surrogate_gradient(sdf_engine* e, const float* d_points, const float* d_targets, int n, float* h_grad,
                                   float* h_loss);
 
+/* ---------------------------------------------------------------------------------------------
+ * Batched extraction (no counterpart in the reference, which meshes one scene per Update call).
+ * Many independent scenes, each with its own grid, primitives and technique, are meshed together:
+ * every stage is one launch over all scenes (the blocks of all marching-cubes scenes form one work
+ * queue, those of all dual-contouring scenes another), with per-scene output bases from one scan.
+ * sdf_batch_capture records the whole device part of an extraction once as a CUDA graph, after an
+ * autotuner has timed the persistent-grid shapes of the heavy kernels on this batch; later
+ * sdf_batch_extract calls replay the graph.
+ * --------------------------------------------------------------------------------------------- */
+typedef struct sdf_batch_scene {
+    const sdf_primitive* prims; /* host array, read during sdf_batch_set_scenes */
+    int32_t count;
+    sdf_config config;          /* grid, technique and DC options of this scene (out_mask: the batch's) */
+} sdf_batch_scene;
+
+typedef struct sdf_batch_stats {
+    int64_t scenes;
+    int64_t total_blocks;
+    int64_t active_blocks;
+    int64_t mc_vertices;        /* triangle-soup vertices of the marching-cubes scenes */
+    int64_t dc_vertices;        /* ... of the dual-contouring scenes */
+    float ms_total;             /* host wall time of the call */
+    int32_t graph;              /* 1 when the call replayed a captured graph */
+    int32_t tuned_ctas[4];      /* CTAs per SM chosen for: block field, emission, DC solve, DC quads */
+} sdf_batch_stats;
+
+typedef struct sdf_batch sdf_batch;
+
+sdf_status sdf_batch_create(sdf_batch** out, int device);
+void sdf_batch_destroy(sdf_batch* b);
+/* Builds every scene's BVH (the engine's order), uploads all scenes and sizes the device buffers.
+ * out_mask applies to all scenes. Drops a captured graph. */
+sdf_status sdf_batch_set_scenes(sdf_batch* b, const sdf_batch_scene* scenes, int n, uint32_t out_mask);
+/* One extraction of all scenes on `stream`. The marching-cubes scenes write one concatenated triangle
+ * soup into mc_out, the dual-contouring scenes into dc_out (either may be NULL when no scene uses
+ * it); scene i occupies vertices [first_vertex[i], first_vertex[i] + vertex_count[i]) of its
+ * technique's buffer (host arrays of n entries, may be NULL), and its identity indices count from
+ * the buffer's start. Synchronous (the counts are read back). */
+sdf_status sdf_batch_extract(sdf_batch* b, float time, const sdf_outputs* mc_out, const sdf_outputs* dc_out,
+                             void* stream, int64_t* first_vertex, int64_t* vertex_count, sdf_batch_stats* stats);
+/* Autotunes the CTAs per SM of the heavy kernels on this batch (timing replays), then captures one
+ * extraction with the chosen shapes as a CUDA graph for the given outputs and time; later
+ * sdf_batch_extract calls with the same outputs replay it (other outputs fall back to direct launches).
+ * tune = 0 skips the autotuner (occupancy-limited grids). */
+sdf_status sdf_batch_capture(sdf_batch* b, float time, const sdf_outputs* mc_out, const sdf_outputs* dc_out,
+                             void* stream, int tune);
+
 /* First CUDA error recorded by a drop-in launcher since the last call (cleared on read). */
 int sdf_last_error(void);
 /* Library version string. */

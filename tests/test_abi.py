@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
     L = _lib.lib()
     missing = [n for n in declared_functions() if not hasattr(L, n)]
     assert not missing, missing
-    assert set(_lib.DROPIN_SYMBOLS + _lib.ENGINE_SYMBOLS + _lib.SURROGATE_SYMBOLS +
+    assert set(_lib.DROPIN_SYMBOLS + _lib.ENGINE_SYMBOLS + _lib.SURROGATE_SYMBOLS + _lib.BATCH_SYMBOLS +
                _lib.STATIC_SCOUT_SYMBOLS) <= set(declared_functions())
     assert L.sdf_version().startswith(b"sdfmesh_b200")
 
@@ -55,7 +55,7 @@ def test_header_compiles_as_c():
     from cudasdf_b200 import _lib
     structs = {"sdf_config": _lib.SdfConfig, "sdf_outputs": _lib.SdfOutputs, "sdf_stats": _lib.SdfStats,
                "sdf_surrogate_config": _lib.SurrogateConfig, "sdf_surrogate_stats": _lib.SurrogateStats,
-               "sdf_grid": _lib.SdfGrid}
+               "sdf_grid": _lib.SdfGrid, "sdf_batch_scene": _lib.BatchScene, "sdf_batch_stats": _lib.BatchStats}
     body = "".join(f'printf("%zu\\n", sizeof({n}));' for n in structs)
     src = ('#include <stdio.h>\n#include "sdfmesh_b200.h"\n'
            'int main(void){ if (sizeof(sdf_primitive) != 160) return 1; ' + body + ' return 0; }\n')
