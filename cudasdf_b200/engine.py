@@ -264,13 +264,16 @@ class Batch:
         sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
         L.check(self._lib.sdf_batch_capture(self.h, float(time), om, od, sp, 1 if tune else 0), "sdf_batch_capture")
 
-    def extract(self, mc: MeshBuffers, dc: MeshBuffers, time: float = 0.0, stream=None):
-        """Returns (first_vertex, vertex_count, stats)."""
+    def extract(self, mc: MeshBuffers, dc: MeshBuffers, time: float = 0.0, stream=None, allow_capacity=False):
+        """Returns (first_vertex, vertex_count, stats); the counts are exact even when a buffer was too
+        small (SDF_ERR_CAPACITY, raised unless allow_capacity)."""
         om, od = self._outs(mc, dc)
         first = np.zeros(self.n, np.int64)
         count = np.zeros(self.n, np.int64)
         st = L.BatchStats()
         sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
-        L.check(self._lib.sdf_batch_extract(self.h, float(time), om, od, sp, first.ctypes.data, count.ctypes.data,
-                                            ctypes.byref(st)), "sdf_batch_extract")
+        rc = self._lib.sdf_batch_extract(self.h, float(time), om, od, sp, first.ctypes.data, count.ctypes.data,
+                                         ctypes.byref(st))
+        if not (allow_capacity and rc == L.SDF_ERR_CAPACITY):
+            L.check(rc, "sdf_batch_extract")
         return first, count, st.as_dict()
