@@ -583,6 +583,7 @@ __global__ void __launch_bounds__(256) k_fma_peak(float* out, int iters, float a
 // ------------------------------------------------------------------------------------------------
 struct EmitSmem {
     float field[FIELD_STRIDE];
+    unsigned long long cases[256];            // the case table, staged from constant memory
     unsigned warp_sums[BLK_THREADS / 32];
     unsigned short tri_cell[MAX_BLOCK_TRIS];  // (cell << 3) | triangle slot
     unsigned tri_out[MAX_BLOCK_TRIS];         // first output vertex of the triangle
@@ -680,6 +681,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_mc_emit(GridView g0, SceneView 
     __shared__ __align__(16) EmitSmem S;
     const int n = active_count(av);
     const bool attrs = (mask & (OUT_COLORS | OUT_PRIMIDS | OUT_UVS | OUT_NORMALS)) != 0;
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) S.cases[i] = c_mcCases[i];
     for (;;) {
         const int a = claim(ticket, n, &S.item);
         if (a < 0) break;
@@ -709,7 +711,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_mc_emit(GridView g0, SceneView 
             word[h] = 0;
             if (!c[h].oob) {
                 const int code = cell_case(S.field, c[h].lx, c[h].ly, c[h].lz, cv[h]);
-                word[h] = c_mcCases[code];
+                word[h] = S.cases[code];
                 vm[h] = cell_valid_mask(g, c[h].x, c[h].y, c[h].z, cv[h], word[h]);
             }
             cnt[h] = 3u * __popc(vm[h]);
@@ -727,34 +729,67 @@ __global__ void __launch_bounds__(BLK_THREADS) k_mc_emit(GridView g0, SceneView 
         }
         if (packet_offsets_out)
             *reinterpret_cast<uint2*>(packet_offsets_out + (size_t)a * 512 + 2 * threadIdx.x) = make_uint2(off[0], off[1]);
-        if (threadIdx.x == 0) S.ntri = 0;
-        __syncthreads();
-        unsigned tslot = local / 3;  // this thread's first slot in the block triangle list
+        // the block's triangle list in output order: slot s writes vertices base + 3 s .. + 2
+        unsigned tslot = local / 3;  // this thread's first slot
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             if (c[h].oob) continue;
-            unsigned w = off[h];
             const int nt = (int)(word[h] & 0xF);
-            for (int k = 0; k < nt; ++k) {
-                if (!((vm[h] >> k) & 1u)) continue;
-                if ((unsigned long long)w + 2 >= out.maxV) break;  // the reference's capacity stop (:1020)
-                float3 v[3];
-                tri_points(g, c[h].x, c[h].y, c[h].z, cv[h], word[h], k, v);
+            for (int k = 0; k < nt; ++k)
+                if ((vm[h] >> k) & 1u) S.tri_cell[tslot++] = (unsigned short)(((2 * threadIdx.x + h) << 3) | k);
+        }
+        const unsigned base = packet_offsets_in ? 0u : block_offsets[a];
+        const unsigned ntri_all = local_total / 3;
+        // the reference stops a block's output at the first triangle that would reach maxV (:1020)
+        unsigned ntri = 0;
+        if (!packet_offsets_in && (unsigned long long)base + 3 <= out.maxV)
+            ntri = min(ntri_all, (unsigned)(((unsigned long long)out.maxV - base - 3) / 3 + 1));
+        if (threadIdx.x == 0) S.ntri = (int)ntri;
+        __syncthreads();
+        if (packet_offsets_in) {
+            // drop-in path: the cells' offsets come from the caller's scan, one run per thread
+            unsigned slot = local / 3;
 #pragma unroll
-                for (int j = 0; j < 3; ++j) out.verts[w + j] = make_float4(v[j].x, v[j].y, v[j].z, 1.f);
-                if ((mask & OUT_INDICES) && out.indices) {
-                    out.indices[w] = w;
-                    out.indices[w + 1] = w + 1;
-                    out.indices[w + 2] = w + 2;
+            for (int h = 0; h < 2; ++h) {
+                if (c[h].oob) continue;
+                unsigned w = off[h];
+                const int nt = (int)(word[h] & 0xF);
+                for (int k = 0; k < nt; ++k) {
+                    if (!((vm[h] >> k) & 1u)) continue;
+                    if ((unsigned long long)w + 2 >= out.maxV) break;
+                    if (attrs) {
+                        S.tri_out[slot] = w;
+                        atomicAdd(&S.ntri, 1);
+                    }
+                    ++slot;
+                    float3 v[3];
+                    tri_points(g, c[h].x, c[h].y, c[h].z, cv[h], word[h], k, v);
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) out.verts[w + j] = make_float4(v[j].x, v[j].y, v[j].z, 1.f);
+                    if ((mask & OUT_INDICES) && out.indices) {
+                        out.indices[w] = w;
+                        out.indices[w + 1] = w + 1;
+                        out.indices[w + 2] = w + 2;
+                    }
+                    w += 3;
                 }
-                if (attrs) {
-                    S.tri_cell[tslot] = (unsigned short)(((2 * threadIdx.x + h) << 3) | k);
-                    S.tri_out[tslot] = w;
-                    atomicAdd(&S.ntri, 1);
-                }
-                ++tslot;
-                w += 3;
             }
+        } else {
+            // one output vertex per thread: consecutive threads write consecutive float4s
+            const unsigned nv = 3 * ntri;
+            for (unsigned v = threadIdx.x; v < nv; v += blockDim.x) {
+                const unsigned slot = v / 3, j = v - 3 * slot;
+                const int cell = S.tri_cell[slot] >> 3, k = S.tri_cell[slot] & 7;
+                const CellInfo ci = cell_info(g, bx, by, bz, cell);
+                float cvv[8];
+                const int code = cell_case(S.field, ci.lx, ci.ly, ci.lz, cvv);
+                const unsigned long long wd = S.cases[code];
+                const float3 p = edge_point(g, ci.x, ci.y, ci.z, cvv, (int)((wd >> (4 + 4 * (3 * k + j))) & 0xF));
+                out.verts[base + v] = make_float4(p.x, p.y, p.z, 1.f);
+                if ((mask & OUT_INDICES) && out.indices) out.indices[base + v] = base + v;
+            }
+            if (attrs)
+                for (unsigned t = threadIdx.x; t < ntri; t += blockDim.x) S.tri_out[t] = base + 3 * t;
         }
         if (attrs) {
             __syncthreads();
