@@ -405,14 +405,22 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
         PruneBound pb;
         pb.set(st.d);
         uint2* stk = s_map_stack[threadIdx.x >> 5];
-        if (lane == 0) stk[0] = make_uint2(0u, live);
-        __syncwarp();
-        int sp = 1;
-        while (sp > 0) {
-            --sp;
-            const uint2 e = stk[sp];
-            const int node = (int)e.x;
-            const unsigned mask = e.y;
+        // The reference pushes right then left and pops the left child next; here the left child is
+        // kept as the next node (same mask) and only the right one goes on the stack: the same pop
+        // sequence with one stack entry less per internal node.
+        int sp = 0;
+        int node = 0;
+        unsigned mask = live;
+        bool have = true;
+        for (;;) {
+            if (!have) {
+                if (sp == 0) break;
+                --sp;
+                const uint2 e = stk[sp];
+                node = (int)e.x;
+                mask = e.y;
+            }
+            have = false;
             // a lane pops this node iff it pushed it and has popped fewer than MAP_CAP nodes
             const bool pops = ((mask >> lane) & 1u) && iter < MAP_CAP;
             if (pops) iter++;
@@ -444,14 +452,14 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
                     pb.set(st.d);
                 }
             } else {
-                if (sp + 2 > MAP_STACK) { overflow = true; break; }
+                if (sp + 2 > MAP_STACK) { overflow = true; break; }  // the reference's stack holds both
                 __syncwarp();  // every lane has read stk[sp] (popped above) before it is overwritten
-                if (lane == 0) {
-                    stk[sp] = make_uint2((unsigned)right, hm);
-                    stk[sp + 1] = make_uint2((unsigned)left, hm);
-                }
+                if (lane == 0) stk[sp] = make_uint2((unsigned)right, hm);
                 __syncwarp();
-                sp += 2;
+                ++sp;
+                node = left;
+                mask = hm;
+                have = true;
             }
         }
         if (diag) {
