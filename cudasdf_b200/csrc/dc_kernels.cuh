@@ -157,6 +157,7 @@ namespace sdfb {
 // ------------------------------------------------------------------------------------------------
 constexpr int DC_HERMITE_CAP = 1536;  // Hermite samples staged per pass
 constexpr int DC_CELL_CAP = 512;
+constexpr int DC_EDGE_KEYS = 729 * 6;   // start corner in the 9^3 lattice x axis x direction
 
 struct SolveSmem {
     float field[FIELD_STRIDE];
@@ -170,6 +171,11 @@ struct SolveSmem {
     // Hermite samples of the current pass
     unsigned short h_cell[DC_HERMITE_CAP];  // (cell tid << 4) | edge
     float3 h_n[DC_HERMITE_CAP];
+    // one normal per (edge, direction) of the pass: the sample that claimed the key evaluates it
+    unsigned short edge_rep[DC_EDGE_KEYS];  // key -> representative sample, 0xFFFF if unclaimed
+    unsigned short h_rep[DC_HERMITE_CAP];   // sample -> its representative
+    unsigned short rep_list[DC_HERMITE_CAP];
+    int nrep;
     int next_cursor;
     int item;
 };
@@ -385,10 +391,36 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_solve(GridView g0, SceneView
             __syncthreads();
             const int next = S.next_cursor;
             const unsigned nh = ncells ? (unsigned)S.cell_h0[ncells - 1] + S.cell_m[ncells - 1] : 0u;
-            // Hermite normals: computeNormal at each edge point (:1383-1411)
-            for (int base = warp * 32; base < (int)nh; base += nwarps * 32) {
-                const int i = base + lane;
-                const bool valid = i < (int)nh;
+            // Hermite normals: computeNormal at each edge point (:1383-1411). The cells around an
+            // edge that name it with the same direction compute the same float edge point from the
+            // same two samples, hence the same normal: it is evaluated once per (edge, direction).
+            for (int k = threadIdx.x; k < DC_EDGE_KEYS; k += blockDim.x) S.edge_rep[k] = 0xFFFF;
+            if (threadIdx.x == 0) S.nrep = 0;
+            __syncthreads();
+            for (int i = threadIdx.x; i < (int)nh; i += blockDim.x) {
+                const int tid = S.h_cell[i] >> 4, e = S.h_cell[i] & 15;
+                const int c0 = edge_c0(e), c1 = edge_c1(e);
+                const int d0 = corner_dx(c0) + 2 * corner_dy(c0) + 4 * corner_dz(c0);
+                const int d1 = corner_dx(c1) + 2 * corner_dy(c1) + 4 * corner_dz(c1);
+                const int lo = d0 < d1 ? c0 : c1;  // the edge's lower corner
+                const int axis = (d0 ^ d1) == 1 ? 0 : ((d0 ^ d1) == 2 ? 1 : 2);
+                const int sx = (tid & 7) + corner_dx(lo), sy = ((tid >> 3) & 7) + corner_dy(lo),
+                          sz = (tid >> 6) + corner_dz(lo);
+                const int key = ((sz * 9 + sy) * 9 + sx) * 6 + axis * 2 + (d0 < d1 ? 0 : 1);
+                const unsigned short prev = atomicCAS(&S.edge_rep[key], (unsigned short)0xFFFF, (unsigned short)i);
+                if (prev == 0xFFFF) {
+                    S.h_rep[i] = (unsigned short)i;
+                    S.rep_list[atomicAdd(&S.nrep, 1)] = (unsigned short)i;
+                } else {
+                    S.h_rep[i] = prev;
+                }
+            }
+            __syncthreads();
+            const int nrep = S.nrep;
+            for (int base = warp * 32; base < nrep; base += nwarps * 32) {
+                const int r = base + lane;
+                const bool valid = r < nrep;
+                const int i = valid ? S.rep_list[r] : 0;
                 float3 p = f3(0.f, 0.f, 0.f);
                 if (valid) {
                     const CellInfo c = cell_info(g, bx, by, bz, S.h_cell[i] >> 4);
@@ -399,6 +431,9 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_solve(GridView g0, SceneView
                 const float3 nrm = normal_warp(sc, p, valid, time, g.cell, diag);
                 if (valid) S.h_n[i] = nrm;
             }
+            __syncthreads();
+            for (int i = threadIdx.x; i < (int)nh; i += blockDim.x)
+                if (S.h_rep[i] != i) S.h_n[i] = S.h_n[S.h_rep[i]];
             __syncthreads();
             // per-cell solve
             for (int i = threadIdx.x; i < (int)ncells; i += blockDim.x) {
