@@ -36,7 +36,6 @@ struct BatchGroup {
     unsigned char* masks = nullptr;
     unsigned* dc_voff = nullptr;
     ushort4* dc_verts = nullptr;
-    short4* dc_norms = nullptr;
     size_t dc_cap = 0;
     DcSolveParams sp{};
     DcQuadParams qp{};
@@ -46,7 +45,7 @@ struct BatchGroup {
 
     void release() {
         void* ptrs[] = {desc, prims, nodes, flags, list, fields, block_totals, block_offsets, b2a, miss, first,
-                        ctrl_region, packet_counts, packet_offsets, masks, dc_voff, dc_verts, dc_norms};
+                        ctrl_region, packet_counts, packet_offsets, masks, dc_voff, dc_verts};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         if (h_ctrl) cudaFreeHost(h_ctrl);
@@ -146,7 +145,7 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
         D.masks = B.masks;
         D.vert_offsets = B.dc_voff;
         D.cell_verts = B.dc_verts;
-        D.cell_normals = B.dc_norms;
+        D.cell_normals = nullptr;  // the per-cell normals feed no output
         D.cell_normals_tmp = nullptr;
         D.counts = B.packet_counts;
         D.offsets = B.packet_offsets;
@@ -289,7 +288,6 @@ static sdf_status build_group(BatchGroup& B, const sdf_batch_scene* scenes) {
         if (s == SDF_OK) s = dev_alloc(B.dc_voff, cells);
         B.dc_cap = std::min<size_t>(cells, (size_t)1 << 28);
         if (s == SDF_OK) s = dev_alloc(B.dc_verts, B.dc_cap);
-        if (s == SDF_OK) s = dev_alloc(B.dc_norms, B.dc_cap);
     }
     if (s != SDF_OK) return s;
     const size_t tA = scan_tiles((unsigned)nb) + 1, tC = scan_tiles((unsigned)(nb * 512)) + 1;

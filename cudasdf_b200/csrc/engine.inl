@@ -449,7 +449,7 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
         B.masks = E.masks;
         B.vert_offsets = E.dc_voff;
         B.cell_verts = E.dc_verts;
-        B.cell_normals = E.dc_norms;
+        B.cell_normals = (E.debug & 1) ? E.dc_norms : nullptr;  // no output reads them; debug keeps them
         B.cell_normals_tmp = nullptr;
         B.counts = E.packet_counts;
         B.offsets = E.packet_offsets;

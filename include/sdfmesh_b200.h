@@ -240,7 +240,9 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
 /* Enables per-stage CUDA-event timing inside sdf_engine_extract. */
 void sdf_engine_set_timing(sdf_engine* e, int enabled);
 /* Debug outputs: bit 0 also writes the per-cell vertex counts/offsets of the drop-in layout in
- * marching-cubes mode (readable through sdf_engine_buffer 1 and 2). */
+ * marching-cubes mode (readable through sdf_engine_buffer 1 and 2) and, in dual-contouring mode,
+ * the per-cell vertex normals of the reference's dcSolveCellVertices (sdf_engine_buffer 6), which
+ * no output of the engine needs. */
 void sdf_engine_set_debug(sdf_engine* e, int flags);
 /* The scene as uploaded: sorted primitives (count = numPrimitives) and BVH nodes. */
 int sdf_engine_get_bvh(sdf_engine* e, sdf_bvh_node* nodes_out, int capacity, int* num_bvh_primitives);
