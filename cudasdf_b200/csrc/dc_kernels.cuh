@@ -802,9 +802,20 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quads(GridView g0, SceneView
                     valid = quad_vertices(g, av.list, bbase, B, q, out.maxV, Q);
                     w = S.q_out[i];
                 }
-                const float3 nref = normal_warp(sc, Q.qc, valid, time, g.cell, diag);
+                // map() at the centre: with attributes only when an output needs them; its distance
+                // is the centre sample of the winding normal
                 MapState<true> st;
-                map_warp<true>(sc, Q.qc, valid, time, st, diag);
+                float d0;
+                if (mask & (OUT_COLORS | OUT_PRIMIDS | OUT_UVS)) {
+                    map_warp<true>(sc, Q.qc, valid, time, st, diag);
+                    d0 = st.d;
+                } else {
+                    MapState<false> s0;
+                    map_warp<false>(sc, Q.qc, valid, time, s0, diag);
+                    d0 = s0.d;
+                    st.init();
+                }
+                const float3 nref = normal_warp_at(sc, Q.qc, d0, valid, time, g.cell, diag);
                 if (!valid) continue;
                 const float3 nt = cross_ff(sub3(Q.v[1], Q.v[0]), sub3(Q.v[2], Q.v[0]));
                 const bool flip = dot3(nt, nref) < 0.f;

@@ -489,6 +489,21 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
     }
 }
 
+// computeNormal (MarchingCubesKernels.cu:814-844) for the 32 points of a warp, with the distance at
+// p itself already known (map() at p, with or without attributes: the distance is the same).
+__device__ __forceinline__ float3 normal_warp_at(const SceneView& sc, float3 p, float d0, bool valid, float time,
+                                                 float cell, Diag* diag) {
+    const float h = MUL(cell, 0.001f);
+    MapState<false> sx, sy, sz;
+    map_warp<false>(sc, f3(ADD(p.x, h), p.y, p.z), valid, time, sx, diag);
+    map_warp<false>(sc, f3(p.x, ADD(p.y, h), p.z), valid, time, sy, diag);
+    map_warp<false>(sc, f3(p.x, p.y, ADD(p.z, h)), valid, time, sz, diag);
+    const float3 g = f3(SUB(sx.d, d0), SUB(sy.d, d0), SUB(sz.d, d0));
+    const float len = SQRT(dot3(g, g));
+    if (len > 1e-6f) return f3(DIV(g.x, len), DIV(g.y, len), DIV(g.z, len));
+    return f3(0.f, 1.f, 0.f);
+}
+
 // computeNormal (MarchingCubesKernels.cu:814-844) for the 32 points of a warp.
 __device__ __forceinline__ float3 normal_warp(const SceneView& sc, float3 p, bool valid, float time, float cell,
                                               Diag* diag) {
