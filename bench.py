@@ -129,17 +129,26 @@ def barrier(world):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
 
 
 def max_over_ranks(x, world):
+    """The maximum of x over all ranks (every rank's device time; the job takes the slowest)."""
     import torch
     if world == 1:
         return x
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_throughput(world, units_per_rank, ms_max):
+    """Whole-job throughput of N replicas: every rank processes its own units; the job lasts as long
+    as the slowest rank."""
+    return world * units_per_rank / (ms_max * 1e-3) / 1e9
 
 
 def fp32_peak_tflops():
@@ -214,7 +223,7 @@ def run_ours(args, rank, world):
         eng.extract(buf)
     times, st, out["plain_stages"] = timed_extractions(eng, buf, args.steps, flush, world)
     plain_ms = max_over_ranks(sum(times) / len(times), world)
-    out["plain"] = {"ms": plain_ms, "value": world * voxels / (plain_ms * 1e-3) / 1e9, "stats": st}
+    out["plain"] = {"ms": plain_ms, "value": job_throughput(world, voxels, plain_ms), "stats": st}
     launches_per_step = 6  # scout, compaction, own field, halo field, block scan, emission
     if surrogate:
         plain_verts = buf.vertices[:V].clone()
@@ -240,7 +249,7 @@ def run_ours(args, rank, world):
         out["stages"] = out["plain_stages"]
     clk = clocks.stop()
     ms = max_over_ranks(sum(times) / len(times), world)
-    out.update({"ms": ms, "value": world * voxels / (ms * 1e-3) / 1e9, "stats": st, "clocks": clk, "times": times,
+    out.update({"ms": ms, "value": job_throughput(world, voxels, ms), "stats": st, "clocks": clk, "times": times,
                 "launches_per_step": launches_per_step})
     # end to end through the public API with host buffers: scene upload from pinned host memory (an
     # unchanged scene keeps its host BVH and surrogate), extraction, read-back of the whole vertex buffer

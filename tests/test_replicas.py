@@ -1,0 +1,53 @@
+"""bench.py's multi-process path on CPU: two gloo ranks (one process per rank, as torchrun starts
+them) meet at the barrier, agree on the slowest rank's time and report the whole-job throughput of
+two independent replicas. The extraction itself does not shard (replicas only), so no data moves
+between ranks."""
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+from conftest import ROOT
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, out):
+    import sys
+    sys.path.insert(0, ROOT)
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    import bench
+    bench.barrier(world)
+    ms = 10.0 + 5.0 * rank  # rank 1 is the slow one
+    ms_max = bench.max_over_ranks(ms, world)
+    value = bench.job_throughput(world, 1024.0 ** 3, ms_max)
+    out[rank] = (ms_max, value)
+    bench.barrier(world)
+    dist.destroy_process_group()
+
+
+@pytest.mark.timeout(120)
+def test_two_replicas_report_the_slowest_rank():
+    ctx = mp.get_context("spawn")
+    manager = ctx.Manager()
+    out = manager.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(90)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    assert out[0] == out[1]
+    ms_max, value = out[0]
+    assert ms_max == 15.0
+    assert abs(value - 2 * 1024.0 ** 3 / 15e-3 / 1e9) < 1e-9
