@@ -382,7 +382,6 @@ __global__ void __launch_bounds__(BLK_THREADS) k_mc_field_t(GridView g, SceneVie
 // ------------------------------------------------------------------------------------------------
 constexpr int OWN_N = 512;
 constexpr int HALO_N = FIELD_N - OWN_N;  // 81 + 72 + 64
-constexpr int OWN_TASKS = OWN_N / 32;    // warp tasks per block
 
 // halo sample h (0 <= h < 217) of a block in 9^3-local coordinates: the x = 8 face, then the y = 8
 // face without x = 8, then the z = 8 face without x = 8 and y = 8
@@ -440,8 +439,8 @@ __global__ void __launch_bounds__(256) k_field_plan(GridView g0, ActiveView av, 
     }
 }
 
-// own samples: one CTA per active block, its eight warps on the sixteen 4 x 4 x 2 Morton bricks (all
-// warps of the SM walk the BVH near the same block, which keeps the nodes they read in L1)
+// own samples: one CTA per active block, its eight warps on the eight 4 x 4 x 4 bricks (all warps of
+// the SM walk the BVH near the same block, which keeps the nodes they read in L1)
 template <bool COUNT>
 __global__ void __launch_bounds__(BLK_THREADS) k_field_own(GridView g0, SceneView sc0, float time, ActiveView av,
                                                          float* __restrict__ fields, unsigned* ticket, Diag* diag) {
@@ -458,16 +457,17 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_own(GridView g0, SceneVie
         resolve(av, av.list[a], g, sc, lin, bbase);
         int bx, by, bz;
         block_coord(g, lin, bx, by, bz);
-        for (int chunk = warp; chunk < OWN_TASKS; chunk += nwarps) {
-            const int r = chunk * 32 + lane;
-            const int sx = (r & 1) | ((r >> 2) & 2) | ((r >> 4) & 4);
-            const int sy = ((r >> 1) & 1) | ((r >> 3) & 2) | ((r >> 5) & 4);
-            const int sz = ((r >> 2) & 1) | ((r >> 4) & 2) | ((r >> 6) & 4);
-            const int gx = bx * 8 + sx, gy = by * 8 + sy, gz = bz * 8 + sz;
-            const bool valid = gx < g.w && gy < g.h && gz < g.d;
-            MapState<false> st;
-            map_warp<false, COUNT>(sc, grid_loc(g, gx, gy, gz), valid, time, st, diag);
-            fields[(size_t)a * FIELD_STRIDE + (sz * 9 + sy) * 9 + sx] = valid ? st.d : 0.f;
+        // eight 4 x 4 x 4 bricks of 64 samples, one per warp, two z-neighbours per lane
+        for (int brick = warp; brick < OWN_N / 64; brick += nwarps) {
+            const int sx = (brick & 1) * 4 + (lane & 3), sy = ((brick >> 1) & 1) * 4 + ((lane >> 2) & 3);
+            const int sz0 = (brick >> 2) * 4 + 2 * (lane >> 4), sz1 = sz0 + 1;
+            const int gx = bx * 8 + sx, gy = by * 8 + sy, gz0 = bz * 8 + sz0, gz1 = gz0 + 1;
+            const bool v0 = gx < g.w && gy < g.h && gz0 < g.d, v1 = gx < g.w && gy < g.h && gz1 < g.d;
+            float d0, d1;
+            map_warp2<COUNT>(sc, grid_loc(g, gx, gy, gz0), grid_loc(g, gx, gy, gz1), v0, v1, time, d0, d1, diag);
+            float* row = fields + (size_t)a * FIELD_STRIDE;
+            row[(sz0 * 9 + sy) * 9 + sx] = v0 ? d0 : 0.f;
+            row[(sz1 * 9 + sy) * 9 + sx] = v1 ? d1 : 0.f;
         }
     }
 }

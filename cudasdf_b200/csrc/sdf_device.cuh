@@ -489,6 +489,136 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
     }
 }
 
+// map() distance for 64 points per warp, two per lane (points 0 and 1 of a lane are usually
+// neighbours). One stack entry carries the two lane masks of its pushers, so the pop, the node loads,
+// the ballots and the push are shared by the two walks while every point still makes its own prune
+// decision at every node it pops: each point's sequence of pops is its own depth-first walk with the
+// 64-entry stack and the 256-pop cap, exactly as in map_warp. Must be called by all 32 lanes.
+template <bool COUNT = false>
+__device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float3 p1, bool v0, bool v1, float time,
+                                          float& d0, float& d1, Diag* diag) {
+    unsigned long long cnt_pops = 0, cnt_leaves = 0, cnt_wpops = 0, cnt_wtests = 0, cnt_wleaves = 0;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    MapState<false> s0, s1;
+    s0.init();
+    s1.init();
+    const unsigned live0 = __ballot_sync(FULL, v0), live1 = __ballot_sync(FULL, v1);
+    int it0 = 0, it1 = 0;
+    __shared__ uint4 s_map_stack2[MAP_WARPS][MAP_STACK];
+    bool overflow = blockDim.x > 32 * MAP_WARPS;
+    if (sc.nnodes > 0 && (live0 | live1) && !overflow) {
+        PruneBound b0, b1;
+        b0.set(s0.d);
+        b1.set(s1.d);
+        uint4* stk = s_map_stack2[threadIdx.x >> 5];
+        int sp = 0;
+        int node = 0;
+        unsigned m0 = live0, m1 = live1;
+        bool have = true;
+        for (;;) {
+            if (!have) {
+                if (sp == 0) break;
+                --sp;
+                const uint4 e = stk[sp];
+                node = (int)e.x;
+                m0 = e.y;
+                m1 = e.z;
+            }
+            have = false;
+            const bool pops0 = ((m0 >> lane) & 1u) && it0 < MAP_CAP;
+            const bool pops1 = ((m1 >> lane) & 1u) && it1 < MAP_CAP;
+            if (pops0) it0++;
+            if (pops1) it1++;
+            if (COUNT) {
+                cnt_pops += __popc(__ballot_sync(FULL, pops0)) + __popc(__ballot_sync(FULL, pops1));
+                cnt_wpops += 2;
+            }
+            const bool a0 = pops0 && b0.alive(), a1 = pops1 && b1.alive();
+            if (!__any_sync(FULL, a0 || a1)) continue;
+            if (COUNT) cnt_wtests += 2;
+            const float4 na = __ldg(sc.nodes + 2 * node);
+            const float4 nb = __ldg(sc.nodes + 2 * node + 1);
+            const bool h0 = a0 && b0.closer(p0, na, nb);
+            const bool h1 = a1 && b1.closer(p1, na, nb);
+            const unsigned hm0 = __ballot_sync(FULL, h0), hm1 = __ballot_sync(FULL, h1);
+            if ((hm0 | hm1) == 0) continue;
+            const int left = __float_as_int(nb.z), right = __float_as_int(nb.w);
+            if (right == -1) {
+                const float4* pr = sc.prims + (size_t)left * PRIM_ROWS;
+                const Leaf L = load_leaf(pr);
+                if (COUNT) {
+                    cnt_leaves += __popc(hm0) + __popc(hm1);
+                    cnt_wleaves += (__any_sync(FULL, h0 || h1) ? 1 : 0) + (__any_sync(FULL, h0 && h1) ? 1 : 0);
+                }
+                // first pass: each lane's first hit point; second pass: point 1 of lanes that hit both
+                if (h0 || h1) {
+                    const bool use0 = h0;
+                    MapState<false> t;
+                    t.d = use0 ? s0.d : s1.d;
+                    float3 pre;
+                    const float dp = leaf_distance(L, use0 ? p0 : p1, time, pre);
+                    combine<false>(t, L.op, L.pos.w, pr, left, dp, pre);
+                    if (use0) {
+                        s0.d = t.d;
+                        b0.set(t.d);
+                    } else {
+                        s1.d = t.d;
+                        b1.set(t.d);
+                    }
+                }
+                if (h0 && h1) {
+                    float3 pre;
+                    const float dp = leaf_distance(L, p1, time, pre);
+                    combine<false>(s1, L.op, L.pos.w, pr, left, dp, pre);
+                    b1.set(s1.d);
+                }
+            } else {
+                if (sp + 2 > MAP_STACK) { overflow = true; break; }  // the reference's stack holds both
+                __syncwarp();  // every lane has read stk[sp] (popped above) before it is overwritten
+                if (lane == 0) stk[sp] = make_uint4((unsigned)right, hm0, hm1, 0u);
+                __syncwarp();
+                ++sp;
+                node = left;
+                m0 = hm0;
+                m1 = hm1;
+                have = true;
+            }
+        }
+        if (diag) {
+            const unsigned c0 = __ballot_sync(FULL, v0 && it0 >= MAP_CAP), c1 = __ballot_sync(FULL, v1 && it1 >= MAP_CAP);
+            if (lane == 0 && (c0 | c1)) atomicAdd(&diag->cap_hits, (unsigned long long)(__popc(c0) + __popc(c1)));
+        }
+    }
+    if (diag && overflow && lane == 0) atomicExch(&diag->stack_overflow, 1);
+    if (COUNT && diag && lane == 0) {
+        const unsigned nlive = __popc(live0) + __popc(live1);
+        atomicAdd(&diag->node_pops, cnt_pops);
+        atomicAdd(&diag->leaf_evals, cnt_leaves + (unsigned long long)nlive * (sc.nprims - sc.nbvh));
+        atomicAdd(&diag->points, (unsigned long long)nlive);
+        atomicAdd(&diag->warp_pops, cnt_wpops);
+        atomicAdd(&diag->warp_tests, cnt_wtests);
+        atomicAdd(&diag->warp_leaves, cnt_wleaves);
+    }
+    // non-union primitives: a linear pass in scene order (:703-803)
+    for (int i = sc.nbvh; i < sc.nprims; ++i) {
+        const float4* pr = sc.prims + (size_t)i * PRIM_ROWS;
+        const Leaf L = load_leaf(pr);
+        if (v0) {
+            float3 pre;
+            const float dp = leaf_distance(L, p0, time, pre);
+            combine<false>(s0, L.op, L.pos.w, pr, i, dp, pre);
+        }
+        if (v1) {
+            float3 pre;
+            const float dp = leaf_distance(L, p1, time, pre);
+            combine<false>(s1, L.op, L.pos.w, pr, i, dp, pre);
+        }
+    }
+    d0 = s0.d;
+    d1 = s1.d;
+}
+
 // computeNormal (MarchingCubesKernels.cu:814-844) for the 32 points of a warp, with the distance at
 // p itself already known (map() at p, with or without attributes: the distance is the same).
 __device__ __forceinline__ float3 normal_warp_at(const SceneView& sc, float3 p, float d0, bool valid, float time,
