@@ -250,6 +250,17 @@ class CudaSDFMesh:
         self.total_indices = 0
         self.num_active = num_active
 
+    def DCNormalPasses(self, time, cosAngleThreshold):
+        """The two dual-contouring normal passes that CudaSDFMesh::Update never calls
+        (Wrappers.cu:87-105): normals recomputed at the cell vertices, then the angle-gated smoothing
+        into the tmp buffer. Run after Update with the dual-contouring technique."""
+        lib = L.lib()
+        G = ctypes.byref(self.grid)
+        lib.launchDCRecomputeNormalsAtVertices(G, self.num_active, float(time))
+        self._err("dcRecomputeNormalsAtVertices")
+        lib.launchDCSmoothCellNormals(G, self.num_active, float(cosAngleThreshold))
+        self._err("dcSmoothCellNormals")
+
     # inspection helpers for the tests
     def active_blocks(self):
         return self._bufs["activeBlocks"][: self.num_active].cpu().numpy()

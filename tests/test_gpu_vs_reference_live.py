@@ -143,3 +143,41 @@ def _run_case(prims, seed, res, technique, exact):
     # (1.2e-7) moves a component by about 1.2e-7 / h, i.e. 2.4e-3 at cell 0.05; most are unaffected
     dn = np.abs(mine["normals"][:, :3] - ref["normals"][:, :3]).max(1)
     assert np.mean(dn < 1e-4) > 0.8 and np.mean(dn < 1e-2) > 0.99, (np.mean(dn < 1e-4), np.mean(dn < 1e-2))
+
+
+@pytest.mark.parametrize("seed,n,res", [(51, 24, 45), (52, 40, 64)])
+def test_dc_normal_passes_match_reference(seed, n, res):
+    """launchDCRecomputeNormalsAtVertices and launchDCSmoothCellNormals after a DC update, on the
+    reference and on the library: the cell normals and the smoothed copies agree."""
+    import torch
+
+    from cudasdf_b200 import _lib as L
+    from cudasdf_b200.dropin import CudaSDFMesh
+    prims = mixed_scene(seed, n, "union", displaced=False, cones=False)
+    bmin, bmax = (-1.1, -1.05, -1.0), (1.1, 1.0, 1.05)
+    cell = float(np.float32(2.2) / np.float32(res))
+    cos_t = float(np.cos(np.radians(30.0)))
+    m = R.RefMesh(cell, bmin, bmax, max_vertices=4_000_000)
+    m.set_primitives(prims)
+    st = m.run(0.0, 1, 1.0, R.OUT_INDICES, sort_active=True)
+    m.dc_normal_passes(0.0, cos_t)
+    nA = st["activeUsed"]
+    mask = m.copy(R.RB_DCMASK, np.uint8, nA * 512)
+    voff = m.copy(R.RB_DCVOFF, np.uint32, nA * 512)
+    nd = int(voff[-1]) + int(mask[-1] not in (0, 255))
+    ref_n = m.copy(R.RB_DCNORM, np.int16, nd * 4).reshape(nd, 4)
+    ref_t = m.copy(R.RB_DCNORMTMP, np.int16, nd * 4).reshape(nd, 4)
+    m.close()
+    mesh = CudaSDFMesh(max_active_blocks=1 << 30, max_vertices=4_000_000)
+    mesh.Initialize(cell, bmin, bmax)
+    for p in prims:
+        mesh.AddPrimitive(p)
+    verts = torch.empty((4_000_000, 4), dtype=torch.float32, device="cuda")
+    idx = torch.empty(4_000_000, dtype=torch.int32, device="cuda")
+    mesh.Update(0.0, verts, None, idx, technique=L.TECH_DC)
+    mesh.DCNormalPasses(0.0, cos_t)
+    assert mesh.num_active == nA
+    got_n = mesh.dc_buffer("dcNormals", nd)[:, :3]
+    got_t = mesh.dc_buffer("dcNormalsTmp", nd)[:, :3]
+    assert (got_n == ref_n[:, :3]).all(), int((got_n != ref_n[:, :3]).any(1).sum())
+    assert (got_t == ref_t[:, :3]).all(), int((got_t != ref_t[:, :3]).any(1).sum())
