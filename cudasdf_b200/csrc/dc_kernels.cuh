@@ -581,7 +581,8 @@ __global__ void k_dc_smooth_normals(GridView g, ActiveView av, DcBuffers B, unsi
         const float d = dot3(nb, self);
         if (d >= cosT) {
             const float w = DIV(SUB(d, cosT), fmaxf(1e-6f, SUB(1.f, cosT)));
-            sum = add3(sum, scl3(nb, w));
+            // nSum + w * nNbr (:1697), the product fused into the sum
+            sum = f3(FMA(w, nb.x, sum.x), FMA(w, nb.y, sum.y), FMA(w, nb.z, sum.z));
         }
     }
     const float len = SQRT(dot3(sum, sum));
