@@ -13,8 +13,10 @@ then halos) -> block scan -> emission.
   plain  = the same for the plain exact extraction (no surrogate)
   e2e    = the surrogate-culled extraction through the public engine API with host buffers: scene
            upload from pinned host memory + extraction + read-back of counts and the whole vertex buffer
-  --impl reference: the reference's own CUDA path (built from its sources into oracle/_ref) on the
-           same GPU, driven in CudaSDFMesh::Update's stage order.
+  --impl reference: the reference's algorithm on the host cores (its own path exists only as CUDA,
+           so the C restatement in oracle/ with OpenMP stands in), a bounded sample per step
+  --impl reference-cuda: the reference's own CUDA sources (built into oracle/_ref) on the same GPU,
+           driven in CudaSDFMesh::Update's stage order
 
 Run: python bench.py [--gpus N --steps K --warmup W --config c4 --impl ours|reference --plain]
 """
@@ -48,7 +50,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default="c4", choices=sorted(CONFIGS))
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"],
+                    help="reference: the reference's algorithm on the host cores (its path exists only as CUDA, "
+                         "so the CPU restatement in oracle/ stands in); reference-cuda: the reference's own "
+                         "CUDA sources (oracle/_ref) on this GPU")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--plain", action="store_true", help="time the plain exact path only (no surrogate)")
@@ -430,6 +435,48 @@ def cpu_baseline(args):
                       f"blocks, scaled to the full {res}^3 extraction ({total:.1f} s estimated)"}
 
 
+def run_reference_cpu(args):
+    """The reference arm on the host cores: the reference's algorithm (restated in oracle/sdf_oracle.c,
+    OpenMP over all host threads) on a bounded sample of the workload per step - a slice of the
+    scout and a sample of the active blocks' marching cubes, each scaled to the whole grid."""
+    import numpy as np
+
+    from cudasdf_b200 import scenes as S
+    from oracle import oracle as O
+    spec = CONFIGS[args.config]
+    cfg_id = spec["config"]
+    res = S.config_resolution(cfg_id)
+    sc = O.Scene(S.config_scene(cfg_id))
+    g = O.make_grid(S.cell_size_for(res))
+    nblocks = g.bx * g.by * g.bz
+    cores = os.cpu_count() or 1
+    gold = os.path.join(ROOT, "tests", "golden", f"full_mc_c{cfg_id}.npz")
+    if os.path.exists(gold):
+        active = np.sort(np.load(gold)["active"]).astype(np.int32)
+    else:
+        flags = O.scout_flags(sc, g, np.arange(nblocks, dtype=np.int32), 0.0, cores)
+        active = np.nonzero(flags)[0].astype(np.int32)
+    scout_n = min(nblocks, 32768)
+    mc_n = min(len(active), 256)
+    rng = np.random.default_rng(0)
+    values = []
+    for step in range(args.warmup + args.steps):
+        b0 = (step * scout_n) % max(nblocks - scout_n + 1, 1)
+        t0 = time.perf_counter()
+        O.scout_range(sc, g, b0, b0 + scout_n, 0.0, cores)
+        t_scout = (time.perf_counter() - t0) / scout_n * nblocks
+        sample = rng.choice(active, size=mc_n, replace=False) if mc_n else active
+        t0 = time.perf_counter()
+        O.mc_blocks(sc, g, np.sort(sample), 0.0, cores)
+        t_mc = (time.perf_counter() - t0) / max(mc_n, 1) * len(active)
+        if step >= args.warmup:
+            values.append(float(res) ** 3 / (t_scout + t_mc) / 1e9)
+    v = sum(values) / len(values)
+    return {"value": v, "ms": float(res) ** 3 / (v * 1e9) * 1e3, "cores": cores, "res": res,
+            "sample": f"per step: scout of {scout_n} of {nblocks} blocks + marching cubes of {mc_n} of {len(active)} "
+                      f"active blocks, each scaled to the full {res}^3 extraction"}
+
+
 def run_reference_batch(args):
     """The batched workload through the reference's path: one fresh mesh object per scene (its size
     caches are process-wide), the scenes one after another; time of the runs alone."""
@@ -485,7 +532,11 @@ METRIC = "Gvoxels/s SDF\u2192mesh at 1024\u00b3, surrogate-culled vs plain, iden
 
 def main():
     args = parse()
-    rank, world, local = dist_setup(args.gpus)
+    if args.impl != "ours":
+        # the reference arms run on rank 0 alone; no process group, no CUDA context of ours
+        rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    else:
+        rank, world, local = dist_setup(args.gpus)
     spec = CONFIGS[args.config]
     headline = spec.get("surrogate", False)
     base = {"metric": METRIC if headline else f"Gvoxels/s SDF\u2192mesh extraction ({spec['workload']})",
@@ -494,7 +545,23 @@ def main():
             "data": "synthetic (seeded scene with the benchmark configuration's primitive law, sizes and counts)"}
     nprims = (len(__import__("cudasdf_b200.scenes", fromlist=["x"]).config_scene(spec["config"]))
               if spec["config"] <= 4 else "256 scenes")
-    if args.impl == "reference":
+    if args.impl == "reference" and spec["technique"] == 0:
+        if rank != 0:
+            return
+        r = run_reference_cpu(args)
+        line = dict(base)
+        line.update({"impl": "reference", "value": r["value"], "ms_per_step": r["ms"],
+                     "config": {"workload": spec["workload"], "grid": r["res"], "primitives": nprims,
+                                "outputs": "VBO float4 + EBO uint32", "parallelism": f"{r['cores']} host threads",
+                                "path": "the reference's algorithm (plain exact marching cubes) restated in C, "
+                                        "OpenMP; the reference's own path is CUDA only (see --impl reference-cuda)"},
+                     "cpu_baseline": {"value": r["value"], "unit": "Gvoxels/s", "cores": r["cores"], "kind": "port",
+                                      "sample": r["sample"]},
+                     "e2e": {"value": r["value"], "unit": "Gvoxels/s", "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": 0}})
+        print(json.dumps(line))
+        return
+    if args.impl in ("reference", "reference-cuda"):
         if rank != 0:
             return
         r = run_reference(args, rank, world)
@@ -505,9 +572,9 @@ def main():
                                 "path": "the reference's plain exact path (it has no surrogate)",
                                 "l2": "per-stage host syncs of the reference (CudaSDFMesh.cpp:83-88)"},
                      "reference_kernel_ms": r["ms_kernels"], "reference_stats": r["stats"], "clocks": r["clocks"],
-                     "cpu_baseline": {"value": r["value"], "unit": "Gvoxels/s", "cores": 1, "kind": "reference",
-                                      "sample": "the reference's own CUDA path (oracle/_ref) on this B200: its "
-                                                "per-stage launches, host syncs and count read-backs"},
+                     "reference_cuda_path": {"value": r["value"], "unit": "Gvoxels/s",
+                                             "sample": "the reference's own CUDA sources (oracle/_ref) on this GPU: "
+                                                       "its per-stage launches, host syncs and count read-backs"},
                      "e2e": {"value": r["value"], "unit": "Gvoxels/s", "h2d_bytes_per_step": 0,
                              "d2h_bytes_per_step": 0}})
         print(json.dumps(line))
