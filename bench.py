@@ -241,7 +241,7 @@ def run_ours(args, rank, world):
         if audit["violations"] == 0:
             eng.surrogate_enable(True)
             launches_per_step = 7  # + the surrogate's coarse-block inference
-        else:  # the exact audit is the judge: a violated certificate falls back to the plain path
+        else:  # the exact audit decides: a violated certificate falls back to the plain path
             out["surrogate"]["fallback"] = "audit found active blocks in culled coarse blocks"
         for _ in range(args.warmup):
             eng.extract(buf)
