@@ -27,6 +27,7 @@ struct BatchGroup {
     unsigned* block_offsets = nullptr;
     int* b2a = nullptr;
     unsigned* miss = nullptr;
+    unsigned* cell_words = nullptr;     // flat emission (no attribute outputs)
     unsigned* first = nullptr;          // n + 1 first vertices
     unsigned char* ctrl_region = nullptr;
     size_t scanA_off = 0, scanB_off = 0, scanC_off = 0, ctrl_bytes = 0;
@@ -44,7 +45,7 @@ struct BatchGroup {
     unsigned* h_first = nullptr;
 
     void release() {
-        void* ptrs[] = {desc, prims, nodes, flags, list, fields, block_totals, block_offsets, b2a, miss, first,
+        void* ptrs[] = {desc, prims, nodes, flags, list, fields, block_totals, block_offsets, b2a, miss, cell_words, first,
                         ctrl_region, packet_counts, packet_offsets, masks, dc_voff, dc_verts};
         for (void* p : ptrs)
             if (p) cudaFree(p);
@@ -70,7 +71,7 @@ static int capped_grid(K kernel, int threads, long long items, size_t smem, int 
 
 // launch shapes of one extraction, fixed before any capture
 struct BatchGrids {
-    int own, miss, gather, emit, mark, solve, quads, count_quads;
+    int own, miss, gather, emit, mark, solve, quads, count_quads, emit_cells;
 };
 
 static BatchGrids batch_grids(long long blocks, const int ctas[4]) {
@@ -83,6 +84,7 @@ static BatchGrids batch_grids(long long blocks, const int ctas[4]) {
     G.solve = capped_grid(k_dc_solve, BLK_THREADS, blocks, sizeof(SolveSmem), ctas[2]);
     G.quads = capped_grid(k_dc_quads, BLK_THREADS, blocks, sizeof(QuadSmem), ctas[3]);
     G.count_quads = (int)std::min<long long>(std::max(1LL, blocks), (long long)num_sms() * 4);
+    G.emit_cells = capped_grid(k_mc_emit_cells, 256, std::max(1LL, blocks * 2), 0, 0);
     return G;
 }
 
@@ -132,13 +134,17 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
         k_field_own<false><<<G.own, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, &ctrl->tickets[0], diag);
         k_field_miss<false><<<G.miss, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, B.miss, &ctrl->halo_misses,
                                                             &ctrl->tickets[4], diag);
+        const bool flat = B.cell_words && !(m & (OUT_COLORS | OUT_UVS | OUT_PRIMIDS | OUT_NORMALS));
         k_field_gather<<<G.gather, BLK_THREADS, 0, st>>>(g0, av, B.fields, B.b2a, B.flags, B.block_totals, nullptr,
-                                                         &ctrl->tickets[3]);
+                                                         &ctrl->tickets[3], flat ? B.cell_words : nullptr);
         k_exclusive_scan<<<std::max(1u, scan_tiles(nb)), SCAN_THREADS, 0, st>>>(
             B.block_totals, B.block_offsets, 0, &ctrl->active_count, 1, scan_state(B.scan(B.scanB_off)),
             &ctrl->total_vertices, diag);
-        k_mc_emit<<<G.emit, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, B.block_offsets, nullptr, nullptr, mo, m,
-                                                  &ctrl->tickets[1], diag);
+        if (flat)
+            k_mc_emit_cells<<<G.emit_cells, 256, 0, st>>>(g0, av, B.fields, B.cell_words, B.block_offsets, mo, m);
+        else
+            k_mc_emit<<<G.emit, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, B.block_offsets, nullptr, nullptr, mo,
+                                                      m, &ctrl->tickets[1], diag);
     } else {
         DcBuffers D;
         D.block_to_active = B.b2a;
@@ -205,7 +211,7 @@ static bool same_outputs(const sdf_outputs* a, const sdf_outputs& b) {
     return memcmp(a ? a : &z, &b, sizeof(sdf_outputs)) == 0;
 }
 
-static sdf_status build_group(BatchGroup& B, const sdf_batch_scene* scenes) {
+static sdf_status build_group(BatchGroup& B, const sdf_batch_scene* scenes, unsigned out_mask) {
     using namespace sdfb;
     std::vector<sdf_primitive> prims;
     std::vector<sdf_bvh_node> nodes;
@@ -280,6 +286,8 @@ static sdf_status build_group(BatchGroup& B, const sdf_batch_scene* scenes) {
     const bool dc = B.technique == SDF_TECH_DUAL_CONTOURING;
     if (!dc) {
         s = dev_alloc(B.miss, nb * HALO_N);
+        if (s == SDF_OK && !(out_mask & (OUT_COLORS | OUT_UVS | OUT_PRIMIDS | OUT_NORMALS)))
+            s = dev_alloc(B.cell_words, nb * 512);
     } else {
         const size_t cells = nb * 512;
         if (s == SDF_OK) s = dev_alloc(B.packet_counts, cells);
@@ -370,7 +378,7 @@ sdf_status sdf_batch_set_scenes(sdf_batch* b, const sdf_batch_scene* scenes, int
     }
     for (int k = 0; k < 2; ++k) {
         if (I.g[k].scenes.empty()) continue;
-        const sdf_status s = build_group(I.g[k], scenes);
+        const sdf_status s = build_group(I.g[k], scenes, out_mask);
         if (s != SDF_OK) {
             I.g[0].release();
             I.g[1].release();

@@ -102,6 +102,8 @@ struct EngineImpl {
     size_t packet_cap = 0;
     unsigned* miss = nullptr;          // listed halo samples, capacity nblocks * HALO_N
     size_t miss_cap = 0;
+    unsigned* cell_words = nullptr;    // flat emission: one word per cell of every active block
+    size_t cell_words_cap = 0;
     Diag* eval_diag = nullptr;
     std::vector<sdf_primitive> scene;  // the primitives as given (the surrogate's surface run uses them)
     SurrogateState* sur = nullptr;
@@ -110,7 +112,8 @@ struct EngineImpl {
 
     void release() {
         void* ptrs[] = {d_prims, d_nodes, flags, list, fields, block_totals, block_offsets, packet_counts,
-                        packet_offsets, b2a, masks, dc_voff, dc_verts, dc_norms, ctrl_region, eval_diag, miss};
+                        packet_offsets, b2a, masks, dc_voff, dc_verts, dc_norms, ctrl_region, eval_diag, miss,
+                        cell_words};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         d_prims = nullptr; d_nodes = nullptr; flags = nullptr; list = nullptr; fields = nullptr;
@@ -119,7 +122,8 @@ struct EngineImpl {
         ctrl_region = nullptr;
         eval_diag = nullptr;
         miss = nullptr;
-        prims_cap = nodes_cap = dc_cap = packet_cap = miss_cap = 0;
+        cell_words = nullptr;
+        prims_cap = nodes_cap = dc_cap = packet_cap = miss_cap = cell_words_cap = 0;
         if (h_ctrl) cudaFreeHost(h_ctrl);
         h_ctrl = nullptr;
         for (auto& e : ev)
@@ -173,7 +177,8 @@ static float surrogate_margin(const EngineImpl& E) { return E.sur->eps + surroga
 // the block field with shared halos (plan -> evaluation -> gather, see mc_kernels.cuh) and the block totals
 template <bool COUNT>
 static sdf_status run_block_field(EngineImpl& E, const sdfb::SceneView& sv, float time, const sdfb::ActiveView& av,
-                                  sdfb::Ctrl* ctrl, unsigned* packet_counts, cudaStream_t st) {
+                                  sdfb::Ctrl* ctrl, unsigned* packet_counts, cudaStream_t st,
+                                  unsigned* cell_words = nullptr) {
     using namespace sdfb;
     const size_t need = (size_t)E.nblocks * HALO_N;
     if (E.miss_cap < need) {
@@ -192,7 +197,8 @@ static sdf_status run_block_field(EngineImpl& E, const sdfb::SceneView& sv, floa
         E.gv, sv, time, av, E.fields, E.miss, &ctrl->halo_misses, &ctrl->tickets[4], &ctrl->diag);
     check_launch();
     k_field_gather<<<persistent_grid(k_field_gather, BLK_THREADS, E.nblocks), BLK_THREADS, 0, st>>>(
-        E.gv, av, E.fields, E.b2a, E.flags, COUNT ? nullptr : E.block_totals, packet_counts, &ctrl->tickets[3]);
+        E.gv, av, E.fields, E.b2a, E.flags, COUNT ? nullptr : E.block_totals, packet_counts, &ctrl->tickets[3],
+        cell_words);
     check_launch();
     return SDF_OK;
 }
@@ -431,16 +437,31 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
     if (!out->normals) mask &= ~OUT_NORMALS;
 
     if (!dc) {
-        if (run_block_field<false>(E, sv, time, av, ctrl, (E.debug & 1) ? E.packet_counts : nullptr, st) != SDF_OK)
+        // positions and indices only (no per-cell debug layout): the flat per-cell emission
+        const bool flat = !(mask & (OUT_COLORS | OUT_UVS | OUT_PRIMIDS | OUT_NORMALS)) && !(E.debug & 1);
+        if (flat && E.cell_words_cap < (size_t)nb * 512) {
+            if (dev_alloc(E.cell_words, (size_t)nb * 512) != SDF_OK) {
+                E.cell_words_cap = 0;
+                return SDF_ERR_NOMEM;
+            }
+            E.cell_words_cap = (size_t)nb * 512;
+        }
+        if (run_block_field<false>(E, sv, time, av, ctrl, (E.debug & 1) ? E.packet_counts : nullptr, st,
+                                   flat ? E.cell_words : nullptr) != SDF_OK)
             return SDF_ERR_NOMEM;
         if (E.timing) cudaEventRecord(E.ev[2], st);
         k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)nb)), SCAN_THREADS, 0, st>>>(
             E.block_totals, E.block_offsets, 0, &ctrl->active_count, 1, scan_state(scanB), &ctrl->total_vertices, diag);
         check_launch();
         if (E.timing) cudaEventRecord(E.ev[3], st);
-        k_mc_emit<<<persistent_grid(k_mc_emit, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(
-            gv, sv, time, av, E.fields, E.block_offsets, nullptr, (E.debug & 1) ? E.packet_offsets : nullptr, mo, mask,
-            &ctrl->tickets[1], diag);
+        if (flat) {
+            k_mc_emit_cells<<<persistent_grid(k_mc_emit_cells, 256, nb * 2), 256, 0, st>>>(
+                gv, av, E.fields, E.cell_words, E.block_offsets, mo, mask);
+        } else {
+            k_mc_emit<<<persistent_grid(k_mc_emit, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(
+                gv, sv, time, av, E.fields, E.block_offsets, nullptr, (E.debug & 1) ? E.packet_offsets : nullptr, mo,
+                mask, &ctrl->tickets[1], diag);
+        }
         check_launch();
         if (E.timing) cudaEventRecord(E.ev[4], st);
     } else {

@@ -304,10 +304,13 @@ __global__ void k_batch_scene_first(const SceneDesc* __restrict__ scenes, int ns
 // ------------------------------------------------------------------------------------------------
 // per-cell vertex counts of the block whose 9^3 field is in s_field (countActiveBlockTriangles,
 // MarchingCubesKernels.cu:914-970): optionally the whole field to fields_out, the per-cell counts in the
-// drop-in layout and the block total
+// drop-in layout, the block total, and one word per cell for the flat emission (cell_words):
+// case code (bits 0-7), mask of the non-degenerate triangles (bits 8-12), first vertex of the cell
+// inside its block (bits 13-31)
 __device__ __forceinline__ void block_counts(const GridView& g, int a, int lin, float* s_field, unsigned* s_red,
                                              float* __restrict__ fields_out, unsigned* __restrict__ block_totals,
-                                             unsigned* __restrict__ packet_counts) {
+                                             unsigned* __restrict__ packet_counts,
+                                             unsigned* __restrict__ cell_words = nullptr) {
     if (threadIdx.x < FIELD_STRIDE - FIELD_N) s_field[FIELD_N + threadIdx.x] = 0.f;
     __syncthreads();
     if (fields_out) {
@@ -317,22 +320,32 @@ __device__ __forceinline__ void block_counts(const GridView& g, int a, int lin, 
     }
     int bx, by, bz;
     block_coord(g, lin, bx, by, bz);
-    unsigned cnt[2];
+    unsigned cnt[2], code[2], vm[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         const int tid = 2 * threadIdx.x + h;
         const CellInfo c = cell_info(g, bx, by, bz, tid);
         cnt[h] = 0;
+        code[h] = 0;
+        vm[h] = 0;
         if (!c.oob) {
             float cv[8];
-            const int code = cell_case(s_field, c.lx, c.ly, c.lz, cv);
-            const unsigned long long word = c_mcCases[code];
-            cnt[h] = 3u * __popc(cell_valid_mask(g, c.x, c.y, c.z, cv, word));
+            code[h] = (unsigned)cell_case(s_field, c.lx, c.ly, c.lz, cv);
+            const unsigned long long word = c_mcCases[code[h]];
+            vm[h] = cell_valid_mask(g, c.x, c.y, c.z, cv, word);
+            cnt[h] = 3u * __popc(vm[h]);
         }
     }
     if (packet_counts)
         *reinterpret_cast<uint2*>(packet_counts + (size_t)a * 512 + 2 * threadIdx.x) = make_uint2(cnt[0], cnt[1]);
-    if (block_totals) {
+    if (cell_words) {
+        unsigned total;
+        const unsigned pre = block_exclusive<BLK_THREADS>(cnt[0] + cnt[1], s_red, &total);
+        *reinterpret_cast<uint2*>(cell_words + (size_t)a * 512 + 2 * threadIdx.x) =
+            make_uint2(code[0] | (vm[0] << 8) | (pre << 13), code[1] | (vm[1] << 8) | ((pre + cnt[0]) << 13));
+        if (block_totals && threadIdx.x == 0) block_totals[a] = total;
+        __syncthreads();  // s_red is free again
+    } else if (block_totals) {
         unsigned v = cnt[0] + cnt[1];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -521,7 +534,8 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_gather(GridView g0, Activ
                                                             const int* __restrict__ block_to_active,
                                                             const unsigned* __restrict__ flags,
                                                             unsigned* __restrict__ block_totals,
-                                                            unsigned* __restrict__ packet_counts, unsigned* ticket) {
+                                                            unsigned* __restrict__ packet_counts, unsigned* ticket,
+                                                            unsigned* __restrict__ cell_words = nullptr) {
     __shared__ __align__(16) float s_field[FIELD_STRIDE];
     __shared__ unsigned s_red[BLK_THREADS / 32];
     __shared__ int s_item;
@@ -556,7 +570,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_gather(GridView g0, Activ
                 row[h] = v;
             }
         }
-        block_counts(g, a, lin, s_field, s_red, nullptr, block_totals, packet_counts);
+        block_counts(g, a, lin, s_field, s_red, nullptr, block_totals, packet_counts, cell_words);
     }
 }
 
@@ -576,6 +590,58 @@ __global__ void __launch_bounds__(256) k_fma_peak(float* out, int iters, float a
     }
     const float r = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
     if (r == 12345.f) out[threadIdx.x] = r;  // keeps the chains live
+}
+
+// ------------------------------------------------------------------------------------------------
+// flat emission (generateActiveBlockTriangles, MarchingCubesKernels.cu:972-1110, positions and
+// identity indices only): one thread per cell of every active block, no block-wide steps. The cell's
+// case, its non-degenerate triangles and its first vertex inside the block come from the word the
+// gather kernel stored; most cells are empty and return after one load. The vertex order is the
+// block emission's: block offset, then cells in order, then the case's triangles in order.
+// ------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_mc_emit_cells(GridView g0, ActiveView av, const float* __restrict__ fields,
+                                                       const unsigned* __restrict__ cell_words,
+                                                       const unsigned* __restrict__ block_offsets, MeshOut out,
+                                                       unsigned mask) {
+    __shared__ unsigned long long s_cases[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) s_cases[i] = c_mcCases[i];
+    __syncthreads();
+    const long long n = (long long)active_count(av) * 512;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned w = cell_words[i];
+        const unsigned vm = (w >> 8) & 31u;
+        if (!vm) continue;
+        const int a = (int)(i >> 9), tid = (int)(i & 511);
+        GridView g = g0;
+        SceneView unused;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[a], g, unused, lin, bbase);
+        int bx, by, bz;
+        block_coord(g, lin, bx, by, bz);
+        const CellInfo c = cell_info(g, bx, by, bz, tid);
+        const float* f = fields + (size_t)a * FIELD_STRIDE;
+        float cv[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) cv[k] = __ldg(f + fidx(c.lx + corner_dx(k), c.ly + corner_dy(k), c.lz + corner_dz(k)));
+        const unsigned long long word = s_cases[w & 255u];
+        unsigned long long v = (unsigned long long)block_offsets[a] + (w >> 13);
+        const int nt = (int)(word & 0xF);
+        for (int k = 0; k < nt; ++k) {
+            if (!((vm >> k) & 1u)) continue;
+            if (v + 2 >= out.maxV) break;  // the reference's capacity stop (:1020)
+            float3 p[3];
+            tri_points(g, c.x, c.y, c.z, cv, word, k, p);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) out.verts[v + j] = make_float4(p[j].x, p[j].y, p[j].z, 1.f);
+            if ((mask & OUT_INDICES) && out.indices) {
+                out.indices[v] = (unsigned)v;
+                out.indices[v + 1] = (unsigned)v + 1;
+                out.indices[v + 2] = (unsigned)v + 2;
+            }
+            v += 3;
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------------------

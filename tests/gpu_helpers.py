@@ -27,7 +27,7 @@ def exclusive_scan(x):
 
 
 def engine_run(prims, res, technique, out_mask, time=0.0, max_vertices=None, debug=True, cell=None,
-               bmin=(-1.0, -1.0, -1.0), bmax=(1.0, 1.0, 1.0), **cfg_kw):
+               bmin=(-1.0, -1.0, -1.0), bmax=(1.0, 1.0, 1.0), allow_capacity=False, **cfg_kw):
     from cudasdf_b200 import _lib as L
     from cudasdf_b200 import scenes as S
     from cudasdf_b200.engine import Engine, MeshBuffers, make_config
@@ -37,7 +37,7 @@ def engine_run(prims, res, technique, out_mask, time=0.0, max_vertices=None, deb
     eng.set_debug(1 if debug else 0)
     eng.set_scene(prims)
     buf = MeshBuffers(max_vertices or 4_000_000, out_mask)
-    st = eng.extract(buf, time)
+    st = eng.extract(buf, time, allow_capacity=allow_capacity)
     A, V = int(st["active_blocks"]), int(st["total_vertices"])
     r = {"stats": st, "active": eng.buffer(0, np.int32, A)}
     r["verts"] = buf.vertices[:V].cpu().numpy()

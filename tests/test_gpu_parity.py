@@ -139,3 +139,49 @@ def test_repeatable():
     b = H.engine_run(prims, 128, L.TECH_MC, L.OUT_INDICES | L.OUT_COLORS | L.OUT_PRIMIDS)
     for k in ("active", "counts", "verts", "colors", "primids"):
         assert H.sha(a[k]) == H.sha(b[k]), k
+
+
+@pytest.mark.parametrize("name", MC_FIXTURES)
+def test_engine_flat_emission_matches_reference(name):
+    """Positions and indices only, no debug layout: the per-cell flat emission path."""
+    from cudasdf_b200 import _lib as L
+    G = H.load(name)
+    st = H.stats_of(G)
+    kw = {}
+    if "cell" in G.files:
+        kw = {"cell": float(G["cell"]), "bmin": tuple(G["bmin"]), "bmax": tuple(G["bmax"])}
+    r = H.engine_run(G["prims"], int(G["res"]), 0, L.OUT_INDICES, float(G["time"]),
+                     max_vertices=st["totalVertices"] + 1024, debug=False, **kw)
+    assert r["stats"]["total_vertices"] == st["totalVertices"]
+    bad = H.compare(r, G, ["verts", "indices"])
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("name,config", [("full_mc_c1", 1), ("full_mc_c2", 2), ("full_mc_c4", 4)])
+def test_engine_flat_emission_full_size_digest(name, config):
+    from cudasdf_b200 import _lib as L
+    from cudasdf_b200 import scenes as S
+    G = H.load(name)
+    st = H.stats_of(G)
+    r = H.engine_run(S.config_scene(config), S.config_resolution(config), 0, L.OUT_INDICES,
+                     max_vertices=st["totalVertices"] + 1024, debug=False)
+    assert r["stats"]["total_vertices"] == st["totalVertices"]
+    assert H.sha(r["verts"]) == str(G["verts_sha"])
+    if "indices_sha" in G.files:
+        assert H.sha(r["indices"]) == str(G["indices_sha"])
+
+
+def test_flat_emission_capacity_stop():
+    """A vertex buffer smaller than the mesh: both emission paths stop at the same triangle."""
+    from cudasdf_b200 import _lib as L
+    from cudasdf_b200 import scenes as S
+    prims = S.config_scene(2)
+    full = H.engine_run(prims, 64, 0, L.OUT_INDICES, debug=False)
+    V = int(full["stats"]["total_vertices"])
+    cap = V // 2 + 1
+    a = H.engine_run(prims, 64, 0, L.OUT_INDICES, max_vertices=cap, debug=False, allow_capacity=True)
+    b = H.engine_run(prims, 64, 0, L.OUT_INDICES, max_vertices=cap, debug=True, allow_capacity=True)
+    assert a["stats"]["status"] == L.SDF_ERR_CAPACITY and a["stats"]["total_vertices"] == V
+    # a triangle starting at vertex w is written iff w + 2 < cap (triangles start at multiples of 3)
+    W = 3 * ((cap - 3) // 3) + 3
+    assert a["verts"][:W].tobytes() == b["verts"][:W].tobytes() == full["verts"][:W].tobytes()
