@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_own(GridView g0, SceneVie
             const int gx = bx * 8 + sx, gy = by * 8 + sy, gz0 = bz * 8 + sz0, gz1 = gz0 + 1;
             const bool v0 = gx < g.w && gy < g.h && gz0 < g.d, v1 = gx < g.w && gy < g.h && gz1 < g.d;
             float d0, d1;
-            map_warp2<COUNT>(sc, grid_loc(g, gx, gy, gz0), grid_loc(g, gx, gy, gz1), v0, v1, time, d0, d1, diag);
+            map_warp2<COUNT>(sc, grid_loc(g, gx, gy, gz0), grid_loc(g, gx, gy, gz1).z, v0, v1, time, d0, d1, diag);
             float* row = fields + (size_t)a * FIELD_STRIDE;
             row[(sz0 * 9 + sy) * 9 + sx] = v0 ? d0 : 0.f;
             row[(sz1 * 9 + sy) * 9 + sx] = v1 ? d1 : 0.f;

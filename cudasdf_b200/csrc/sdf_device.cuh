@@ -359,15 +359,26 @@ struct PruneBound {
         }
     }
     __device__ __forceinline__ bool alive() const { return hi >= 0.f; }
-    // box_closer(p, a, b, dmin) for the dmin of the last set()
-    __device__ __forceinline__ bool closer(float3 p, float4 a, float4 b) const {
-        const float dx = fmaxf(fmaxf(SUB(a.x, p.x), SUB(p.x, a.w)), 0.f);
-        const float dy = fmaxf(fmaxf(SUB(a.y, p.y), SUB(p.y, b.x)), 0.f);
-        const float dz = fmaxf(fmaxf(SUB(a.z, p.z), SUB(p.z, b.y)), 0.f);
-        const float dd = FMA(dz, dz, FMA(dx, dx, MUL(dy, dy)));
+    // sqrt(dd) < dmin for the dmin of the last set()
+    __device__ __forceinline__ bool closer_dd(float dd) const {
         if (dd < lo) return true;
         if (dd > hi) return false;
         return SQRT(dd) < dmin;
+    }
+    // box_closer(p, a, b, dmin) for the dmin of the last set()
+    __device__ __forceinline__ bool closer(float3 p, float4 a, float4 b) const {
+        return closer_dd(box_dd_z(p.z, a, b, box_dd_xy(p, a, b)));
+    }
+    // the squared box distance of box_closer in its rounding order, dz^2 + (dx^2 + dy^2): the
+    // bracket depends on x and y only, so points that differ only in z share it
+    __device__ __forceinline__ static float box_dd_xy(float3 p, float4 a, float4 b) {
+        const float dx = fmaxf(fmaxf(SUB(a.x, p.x), SUB(p.x, a.w)), 0.f);
+        const float dy = fmaxf(fmaxf(SUB(a.y, p.y), SUB(p.y, b.x)), 0.f);
+        return FMA(dx, dx, MUL(dy, dy));
+    }
+    __device__ __forceinline__ static float box_dd_z(float z, float4 a, float4 b, float xy) {
+        const float dz = fmaxf(fmaxf(SUB(a.z, z), SUB(z, b.y)), 0.f);
+        return FMA(dz, dz, xy);
     }
 };
 
@@ -494,9 +505,12 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
 // the ballots and the push are shared by the two walks while every point still makes its own prune
 // decision at every node it pops: each point's sequence of pops is its own depth-first walk with the
 // 64-entry stack and the 256-pop cap, exactly as in map_warp. Must be called by all 32 lanes.
+// The two points of a lane differ only in z (p1 = (p0.x, p0.y, z1)), so the x and y part of each box
+// distance is computed once for both.
 template <bool COUNT = false>
-__device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float3 p1, bool v0, bool v1, float time,
+__device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float z1, bool v0, bool v1, float time,
                                           float& d0, float& d1, Diag* diag) {
+    const float3 p1 = f3(p0.x, p0.y, z1);
     unsigned long long cnt_pops = 0, cnt_leaves = 0, cnt_wpops = 0, cnt_wtests = 0, cnt_wleaves = 0;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -539,8 +553,9 @@ __device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float3
             if (COUNT) cnt_wtests += 2;
             const float4 na = __ldg(sc.nodes + 2 * node);
             const float4 nb = __ldg(sc.nodes + 2 * node + 1);
-            const bool h0 = a0 && b0.closer(p0, na, nb);
-            const bool h1 = a1 && b1.closer(p1, na, nb);
+            const float xy = PruneBound::box_dd_xy(p0, na, nb);
+            const bool h0 = a0 && b0.closer_dd(PruneBound::box_dd_z(p0.z, na, nb, xy));
+            const bool h1 = a1 && b1.closer_dd(PruneBound::box_dd_z(z1, na, nb, xy));
             const unsigned hm0 = __ballot_sync(FULL, h0), hm1 = __ballot_sync(FULL, h1);
             if ((hm0 | hm1) == 0) continue;
             const int left = __float_as_int(nb.z), right = __float_as_int(nb.w);
