@@ -74,6 +74,12 @@ struct EngineImpl {
     std::vector<sdf_bvh_node> nodes;
     int nbvh = 0;
     int depth = 0;
+    int nprims = 0;                      // primitives on the device (sorted: unions first)
+    int nnodes = 0;                      // BVH nodes on the device
+    bool device_scene = false;           // the scene was built on the GPU (no host copy)
+    unsigned char* bvh_work = nullptr;   // GPU BVH build: work arrays and control block
+    size_t bvh_work_cap = 0;             // primitives the work arrays hold
+    sdfb::bvhd::Ctl* h_bvh_ctl = nullptr;  // pinned read-back of the build's control block
     sdf_primitive* d_prims = nullptr;
     size_t prims_cap = 0;
     sdf_bvh_node* d_nodes = nullptr;
@@ -113,7 +119,7 @@ struct EngineImpl {
     void release() {
         void* ptrs[] = {d_prims, d_nodes, flags, list, fields, block_totals, block_offsets, packet_counts,
                         packet_offsets, b2a, masks, dc_voff, dc_verts, dc_norms, ctrl_region, eval_diag, miss,
-                        cell_words};
+                        cell_words, bvh_work};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         d_prims = nullptr; d_nodes = nullptr; flags = nullptr; list = nullptr; fields = nullptr;
@@ -123,7 +129,10 @@ struct EngineImpl {
         eval_diag = nullptr;
         miss = nullptr;
         cell_words = nullptr;
-        prims_cap = nodes_cap = dc_cap = packet_cap = miss_cap = cell_words_cap = 0;
+        bvh_work = nullptr;
+        prims_cap = nodes_cap = dc_cap = packet_cap = miss_cap = cell_words_cap = bvh_work_cap = 0;
+        if (h_bvh_ctl) cudaFreeHost(h_bvh_ctl);
+        h_bvh_ctl = nullptr;
         if (h_ctrl) cudaFreeHost(h_ctrl);
         h_ctrl = nullptr;
         for (auto& e : ev)
@@ -362,6 +371,85 @@ sdf_status sdf_engine_set_scene(sdf_engine* e, const sdf_primitive* prims, int c
         cudaMemcpy(E.d_nodes, E.nodes.data(), E.nodes.size() * sizeof(sdf_bvh_node), cudaMemcpyHostToDevice) !=
             cudaSuccess)
         return SDF_ERR_CUDA;
+    E.nprims = (int)E.sorted.size();
+    E.nnodes = (int)E.nodes.size();
+    E.device_scene = false;
+    return SDF_OK;
+}
+
+sdf_status sdf_engine_set_scene_device(sdf_engine* e, const sdf_primitive* prims, int count, void* stream_ptr) {
+    using namespace sdfb;
+    if (!e || count < 0 || (count > 0 && !prims)) return SDF_ERR_INVALID;
+    if (reinterpret_cast<uintptr_t>(prims) & 15) return SDF_ERR_INVALID;  // rows are read as float4
+    EngineImpl& E = e->impl;
+    cudaSetDevice(E.device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream_ptr);
+    // the scene changes: the host copy, the host-built nodes and the surrogate no longer apply
+    E.scene.clear();
+    E.sorted.clear();
+    E.nodes.clear();
+    if (E.sur) E.sur->certified = E.sur->enabled = false;
+    E.nprims = E.nbvh = E.nnodes = E.depth = 0;
+    E.device_scene = true;
+    if (count == 0) return SDF_OK;
+    const size_t n = (size_t)count;
+    if (E.prims_cap < n) {
+        if (dev_alloc(E.d_prims, n) != SDF_OK) return SDF_ERR_NOMEM;
+        E.prims_cap = n;
+    }
+    if (E.nodes_cap < 2 * n) {
+        if (dev_alloc(E.d_nodes, 2 * n) != SDF_OK) return SDF_ERR_NOMEM;
+        E.nodes_cap = 2 * n;
+    }
+    // work arrays: 9 floats, 3 ints and 2 segments per primitive, then the control block
+    const size_t seg_bytes = 2 * n * sizeof(bvhd::Seg);
+    const size_t work_bytes = n * (9 * sizeof(float) + 3 * sizeof(int)) + seg_bytes + sizeof(bvhd::Ctl) + 256;
+    if (E.bvh_work_cap < n) {
+        if (dev_alloc(E.bvh_work, work_bytes) != SDF_OK) return SDF_ERR_NOMEM;
+        E.bvh_work_cap = n;
+    }
+    if (!E.h_bvh_ctl && cudaMallocHost(&E.h_bvh_ctl, sizeof(bvhd::Ctl)) != cudaSuccess) {
+        E.h_bvh_ctl = nullptr;
+        return SDF_ERR_NOMEM;
+    }
+    bvhd::Work w;
+    const size_t cap = E.bvh_work_cap;
+    unsigned char* q = E.bvh_work;
+    w.cap = (int)cap;
+    w.box = reinterpret_cast<float*>(q);                 q += 6 * cap * sizeof(float);
+    w.cent = reinterpret_cast<float*>(q);                q += 3 * cap * sizeof(float);
+    w.idx[0] = reinterpret_cast<int*>(q);                q += cap * sizeof(int);
+    w.idx[1] = reinterpret_cast<int*>(q);                q += cap * sizeof(int);
+    w.hist = reinterpret_cast<int*>(q);                  q += cap * sizeof(int);
+    w.seg[0] = reinterpret_cast<bvhd::Seg*>(q);          q += cap * sizeof(bvhd::Seg);
+    w.seg[1] = reinterpret_cast<bvhd::Seg*>(q);          q += cap * sizeof(bvhd::Seg);
+    q = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(q) + 255) & ~uintptr_t(255));
+    w.ctl = reinterpret_cast<bvhd::Ctl*>(q);
+    cudaGetLastError();
+    bvhd::k_bvh_prep<<<1, bvhd::PREP_THREADS, 0, st>>>(prims, count, E.d_prims, E.d_nodes, w);
+    // levels in batches; after each batch the next level's segment count says whether to go on
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E.device);
+    const int grid = (int)std::max<size_t>(1, std::min<size_t>((size_t)sms * 8, n / 2));
+    constexpr int BATCH = 8;
+    for (int level = 0; level < bvhd::MAX_LEVELS; level += BATCH) {
+        const int last = std::min(level + BATCH, bvhd::MAX_LEVELS);
+        for (int l = level; l < last; ++l) bvhd::k_bvh_level<<<grid, bvhd::LEVEL_THREADS, 0, st>>>(w, E.d_nodes, l);
+        if (cudaMemcpyAsync(E.h_bvh_ctl, w.ctl, sizeof(bvhd::Ctl), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return SDF_ERR_CUDA;
+        if (last >= bvhd::MAX_LEVELS || E.h_bvh_ctl->nseg[last] == 0) break;
+    }
+    if (cudaGetLastError() != cudaSuccess) return SDF_ERR_CUDA;
+    const bvhd::Ctl& c = *E.h_bvh_ctl;
+    E.nprims = count;
+    E.nbvh = c.nu;
+    E.nnodes = c.nu > 0 ? 2 * c.nu - 1 : 0;
+    E.depth = c.depth;
+    if (c.overflow || E.depth + 1 > MAP_STACK) {
+        E.nbvh = E.nnodes = 0;
+        return SDF_ERR_STACK;
+    }
     return SDF_OK;
 }
 
@@ -369,9 +457,15 @@ int sdf_engine_get_bvh(sdf_engine* e, sdf_bvh_node* nodes_out, int capacity, int
     if (!e) return -1;
     EngineImpl& E = e->impl;
     if (num_bvh_primitives) *num_bvh_primitives = E.nbvh;
-    if (nodes_out)
+    if (nodes_out && E.device_scene) {
+        const int k = std::min(E.nnodes, capacity);
+        if (k > 0 && cudaMemcpy(nodes_out, E.d_nodes, (size_t)k * sizeof(sdf_bvh_node), cudaMemcpyDeviceToHost) !=
+                         cudaSuccess)
+            return -1;
+    } else if (nodes_out) {
         for (int i = 0; i < (int)E.nodes.size() && i < capacity; ++i) nodes_out[i] = E.nodes[i];
-    return (int)E.nodes.size();
+    }
+    return E.nnodes;
 }
 
 sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out, void* stream_ptr, sdf_stats* stats) {
@@ -408,9 +502,9 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
     SceneView sv;
     sv.prims = reinterpret_cast<const float4*>(E.d_prims);
     sv.nodes = reinterpret_cast<const float4*>(E.d_nodes);
-    sv.nprims = (int)E.sorted.size();
+    sv.nprims = E.nprims;
     sv.nbvh = E.nbvh;
-    sv.nnodes = (int)E.nodes.size();
+    sv.nnodes = E.nnodes;
     const GridView gv = E.gv;
     Diag* diag = &ctrl->diag;
     const int nb = E.nblocks;
@@ -557,6 +651,8 @@ const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes) {
         case 6: p = E.dc_norms; b = E.dc_cap * 8; break;
         case 7: p = E.block_totals; b = (size_t)E.nblocks * 4; break;
         case 8: p = E.fields; b = (size_t)E.nblocks * sdfb::FIELD_STRIDE * 4; break;
+        case 9: p = E.d_prims; b = (size_t)E.nprims * sizeof(sdf_primitive); break;
+        case 10: p = E.d_nodes; b = (size_t)E.nnodes * sizeof(sdf_bvh_node); break;
         default: break;
     }
     if (bytes) *bytes = b;
@@ -567,9 +663,9 @@ static sdfb::SceneView engine_scene_view(EngineImpl& E) {
     sdfb::SceneView sv;
     sv.prims = reinterpret_cast<const float4*>(E.d_prims);
     sv.nodes = reinterpret_cast<const float4*>(E.d_nodes);
-    sv.nprims = (int)E.sorted.size();
+    sv.nprims = E.nprims;
     sv.nbvh = E.nbvh;
-    sv.nnodes = (int)E.nodes.size();
+    sv.nnodes = E.nnodes;
     return sv;
 }
 
@@ -616,9 +712,9 @@ sdf_status sdf_engine_eval(sdf_engine* e, const float* d_points, int n, float ti
     SceneView sv;
     sv.prims = reinterpret_cast<const float4*>(E.d_prims);
     sv.nodes = reinterpret_cast<const float4*>(E.d_nodes);
-    sv.nprims = (int)E.sorted.size();
+    sv.nprims = E.nprims;
     sv.nbvh = E.nbvh;
-    sv.nnodes = (int)E.nodes.size();
+    sv.nnodes = E.nnodes;
     const int warps = (n + 31) / 32;
     const int blocks = std::min((warps + 7) / 8, num_sms() * 8);
     k_eval_points<<<blocks, BLK_THREADS, 0, st>>>(sv, d_points, n, time, d_out, E.eval_diag);
@@ -638,9 +734,9 @@ sdf_status sdf_engine_count_work(sdf_engine* e, unsigned long long out[8]) {
     SceneView sv;
     sv.prims = reinterpret_cast<const float4*>(E.d_prims);
     sv.nodes = reinterpret_cast<const float4*>(E.d_nodes);
-    sv.nprims = (int)E.sorted.size();
+    sv.nprims = E.nprims;
     sv.nbvh = E.nbvh;
-    sv.nnodes = (int)E.nodes.size();
+    sv.nnodes = E.nnodes;
     run_scout_compact(E.gv, sv, 0.f, E.flags, scanA, E.list, &ctrl->active_count, &ctrl->diag, 0);
     record(cudaMemsetAsync(&ctrl->diag, 0, sizeof(Diag), 0));
     ActiveView av{E.list, &ctrl->active_count, E.nblocks};

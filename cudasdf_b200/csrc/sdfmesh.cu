@@ -17,6 +17,7 @@
 #include "bvh_host.h"
 #include "mc_kernels.cuh"
 #include "dc_kernels.cuh"
+#include "bvh_device.cuh"
 #include "surrogate.cuh"
 
 namespace sdfb {

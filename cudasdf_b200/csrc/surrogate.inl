@@ -289,7 +289,17 @@ sdf_status sdf_surrogate_train(sdf_engine* e, const sdf_surrogate_config* cfg_in
             o.max_vertices = vcap;
             sdf_stats st;
             s = sdf_engine_configure(tmp, &cc);
-            if (s == SDF_OK) s = sdf_engine_set_scene(tmp, E.scene.data(), (int)E.scene.size());
+            // a scene built on the GPU has no host copy: its sorted primitives give the same BVH
+            std::vector<sdf_primitive> host_scene;
+            const std::vector<sdf_primitive>* scene = &E.scene;
+            if (E.device_scene) {
+                host_scene.resize((size_t)E.nprims);
+                if (E.nprims > 0 && cudaMemcpy(host_scene.data(), E.d_prims, host_scene.size() * sizeof(sdf_primitive),
+                                               cudaMemcpyDeviceToHost) != cudaSuccess)
+                    s = SDF_ERR_CUDA;
+                scene = &host_scene;
+            }
+            if (s == SDF_OK) s = sdf_engine_set_scene(tmp, scene->data(), (int)scene->size());
             if (s == SDF_OK) {
                 s = sdf_engine_extract(tmp, C.time, &o, nullptr, &st);
                 if (s == SDF_ERR_CAPACITY) s = SDF_OK;  // a subset of the surface is enough

@@ -90,6 +90,20 @@ class Engine:
         p = np.ascontiguousarray(prims, dtype=PRIM_DTYPE)
         L.check(self._lib.sdf_engine_set_scene(self.h, p.ctypes.data, len(p)), "sdf_engine_set_scene")
 
+    def set_scene_device(self, prims, stream=None):
+        """The scene from primitives in device memory (a CUDA tensor of 160-byte records, or a host
+        array, which is uploaded first); the BVH is built on the GPU (sdf_engine_set_scene_device)."""
+        import torch
+        if isinstance(prims, np.ndarray):
+            p = np.ascontiguousarray(prims, dtype=PRIM_DTYPE)
+            prims = torch.from_numpy(p.view(np.uint8).reshape(-1)).cuda()
+        if not (prims.is_cuda and prims.is_contiguous()):
+            raise ValueError("set_scene_device wants a contiguous CUDA tensor")
+        n = prims.numel() * prims.element_size() // PRIM_DTYPE.itemsize
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        self._scene_keep = prims
+        L.check(self._lib.sdf_engine_set_scene_device(self.h, prims.data_ptr(), n, sp), "sdf_engine_set_scene_device")
+
     def set_timing(self, on: bool):
         self._lib.sdf_engine_set_timing(self.h, 1 if on else 0)
 

@@ -234,6 +234,13 @@ sdf_status sdf_engine_configure(sdf_engine* e, const sdf_config* cfg);
 /* Scene as CudaSDFMesh::UpdateBVH (CudaSDFMesh.cpp:216-249): unions first, BVH over the unions, built
  * on the host with the reference's node order, then uploaded in the engine's compact device layout. */
 sdf_status sdf_engine_set_scene(sdf_engine* e, const sdf_primitive* prims, int count);
+/* The scene of sdf_engine_set_scene with the primitives already in device memory (`prims`: a device
+ * pointer, 16-byte aligned) and the BVH built on the GPU, on `stream`: the same sorted primitives,
+ * nodes and hence meshes as the host build of CudaSDFMesh::UpdateBVH (CudaSDFMesh.cpp:216-249,
+ * CudaSDFUtil.h:507-603), which the reference repeats on the host at every Update (:293). Returns
+ * after a synchronisation of `stream` (the sizes of the tree are read back). SDF_ERR_STACK when the
+ * tree is deeper than the traversal's stack. Drops a trained surrogate. */
+sdf_status sdf_engine_set_scene_device(sdf_engine* e, const sdf_primitive* prims, int count, void* stream);
 /* One extraction on `stream` (a cudaStream_t, NULL = legacy default stream). The only host
  * synchronisation is the final count read-back into *stats. */
 sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out, void* stream, sdf_stats* stats);
@@ -248,7 +255,8 @@ void sdf_engine_set_debug(sdf_engine* e, int flags);
 int sdf_engine_get_bvh(sdf_engine* e, sdf_bvh_node* nodes_out, int capacity, int* num_bvh_primitives);
 /* Device pointer to the last extraction's internal arrays, for inspection: 0 active block list,
  * 1 per-cell vertex counts (compat layout), 2 per-cell offsets, 3 DC corner masks, 4 DC cell vertex
- * offsets, 5 DC cell vertices, 6 DC cell normals, 7 per-block vertex totals. */
+ * offsets, 5 DC cell vertices, 6 DC cell normals, 7 per-block vertex totals, 8 block field rows; and
+ * the scene: 9 sorted primitives, 10 BVH nodes. */
 const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes);
 /* Copies the first `bytes` bytes of an internal array (ids as for sdf_engine_buffer) to host memory. */
 sdf_status sdf_engine_read_buffer(sdf_engine* e, int which, void* host_dst, size_t bytes);
