@@ -403,7 +403,8 @@ sdf_status sdf_engine_set_scene_device(sdf_engine* e, const sdf_primitive* prims
     }
     // work arrays: 9 floats, 3 ints and 2 segments per primitive, then the control block
     const size_t seg_bytes = 2 * n * sizeof(bvhd::Seg);
-    const size_t work_bytes = n * (9 * sizeof(float) + 3 * sizeof(int)) + seg_bytes + sizeof(bvhd::Ctl) + 256;
+    const size_t work_bytes = n * (9 * sizeof(float) + 3 * sizeof(int)) + seg_bytes +
+                              bvhd::PREP_CTAS * sizeof(int) + sizeof(bvhd::Ctl) + 256;
     if (E.bvh_work_cap < n) {
         if (dev_alloc(E.bvh_work, work_bytes) != SDF_OK) return SDF_ERR_NOMEM;
         E.bvh_work_cap = n;
@@ -423,18 +424,30 @@ sdf_status sdf_engine_set_scene_device(sdf_engine* e, const sdf_primitive* prims
     w.hist = reinterpret_cast<int*>(q);                  q += cap * sizeof(int);
     w.seg[0] = reinterpret_cast<bvhd::Seg*>(q);          q += cap * sizeof(bvhd::Seg);
     w.seg[1] = reinterpret_cast<bvhd::Seg*>(q);          q += cap * sizeof(bvhd::Seg);
+    w.cta_count = reinterpret_cast<int*>(q);             q += bvhd::PREP_CTAS * sizeof(int);
     q = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(q) + 255) & ~uintptr_t(255));
     w.ctl = reinterpret_cast<bvhd::Ctl*>(q);
     cudaGetLastError();
-    bvhd::k_bvh_prep<<<1, bvhd::PREP_THREADS, 0, st>>>(prims, count, E.d_prims, E.d_nodes, w);
+    const int ctas = (int)std::min<size_t>(bvhd::PREP_CTAS, (n + bvhd::PREP_THREADS - 1) / bvhd::PREP_THREADS);
+    const int per = (int)((n + ctas - 1) / ctas);
+    bvhd::k_bvh_count<<<ctas, bvhd::PREP_THREADS, 0, st>>>(prims, count, per, w);
+    bvhd::k_bvh_scatter<<<ctas, bvhd::PREP_THREADS, 0, st>>>(prims, count, per, E.d_prims, E.d_nodes, w);
     // levels in batches; after each batch the next level's segment count says whether to go on
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E.device);
-    const int grid = (int)std::max<size_t>(1, std::min<size_t>((size_t)sms * 8, n / 2));
+    const int smem_cap = (int)std::min<size_t>(n, bvhd::SMEM_HIST);
+    const size_t smem = (size_t)smem_cap * sizeof(int);
+    if (cudaFuncSetAttribute(bvhd::k_bvh_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return SDF_ERR_CUDA;
+    const int grid_big = (int)std::max<size_t>(1, std::min<size_t>((size_t)sms, n / 33));
+    const int grid_small = (int)std::max<size_t>(1, std::min<size_t>((size_t)sms * 8, n / 64));
     constexpr int BATCH = 8;
     for (int level = 0; level < bvhd::MAX_LEVELS; level += BATCH) {
         const int last = std::min(level + BATCH, bvhd::MAX_LEVELS);
-        for (int l = level; l < last; ++l) bvhd::k_bvh_level<<<grid, bvhd::LEVEL_THREADS, 0, st>>>(w, E.d_nodes, l);
+        for (int l = level; l < last; ++l) {
+            bvhd::k_bvh_big<<<grid_big, bvhd::BIG_THREADS, smem, st>>>(w, E.d_nodes, l, smem_cap);
+            bvhd::k_bvh_small<<<grid_small, bvhd::SMALL_THREADS, 0, st>>>(w, E.d_nodes, l);
+        }
         if (cudaMemcpyAsync(E.h_bvh_ctl, w.ctl, sizeof(bvhd::Ctl), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess)
             return SDF_ERR_CUDA;
