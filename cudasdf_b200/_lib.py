@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libsdfmesh_b200.so")
 SDF_OK, SDF_ERR_INVALID, SDF_ERR_CUDA, SDF_ERR_CAPACITY, SDF_ERR_STACK, SDF_ERR_NOMEM, SDF_ERR_TIMEOUT = range(7)
 STATUS_NAMES = {0: "SDF_OK", 1: "SDF_ERR_INVALID", 2: "SDF_ERR_CUDA", 3: "SDF_ERR_CAPACITY", 4: "SDF_ERR_STACK",
                 5: "SDF_ERR_NOMEM", 6: "SDF_ERR_TIMEOUT"}
-OUT_COLORS, OUT_INDICES, OUT_UVS, OUT_PRIMIDS, OUT_NORMALS = 1, 2, 4, 8, 16
+OUT_COLORS, OUT_INDICES, OUT_UVS, OUT_PRIMIDS, OUT_NORMALS, OUT_WELDED = 1, 2, 4, 8, 16, 32
 TECH_MC, TECH_DC = 0, 1
 DC_SOLVER_REFERENCE, DC_SOLVER_MASSPOINT = 0, 1
 
@@ -38,7 +38,7 @@ class SdfStats(ctypes.Structure):
                 ("dc_cell_vertices", ctypes.c_int64), ("bvh_cap_hits", ctypes.c_int64),
                 ("ms_scout", ctypes.c_float), ("ms_field", ctypes.c_float), ("ms_scan", ctypes.c_float),
                 ("ms_emit", ctypes.c_float), ("ms_total", ctypes.c_float), ("scouted_blocks", ctypes.c_int64),
-                ("dc_fp64_cells", ctypes.c_int64)]
+                ("dc_fp64_cells", ctypes.c_int64), ("welded_vertices", ctypes.c_int64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -17,6 +17,7 @@ struct Ctrl {
     unsigned total_vertices;
     unsigned dc_vertices;
     unsigned halo_misses;  // listed halo samples of the block field (k_field_plan)
+    unsigned welded_vertices;  // indexed marching-cubes output: vertices (one per owned crossed edge)
     Diag diag;
 };
 
@@ -100,7 +101,13 @@ struct EngineImpl {
     size_t dc_cap = 0;
     unsigned char* ctrl_region = nullptr;  // Ctrl, then the three scan regions
     size_t ctrl_bytes = 0;
-    size_t scanA_off = 0, scanB_off = 0, scanC_off = 0;
+    size_t scanA_off = 0, scanB_off = 0, scanD_off = 0, scanC_off = 0;
+    // indexed marching-cubes output: per active block, owned-edge bitmaps, word prefixes, totals, bases
+    unsigned* weld_bits = nullptr;
+    unsigned short* weld_prefix = nullptr;
+    unsigned* weld_totals = nullptr;
+    unsigned* weld_base = nullptr;
+    size_t weld_cap = 0;
     Ctrl* h_ctrl = nullptr;                // pinned read-back
     bool timing = false;
     int debug = 0;
@@ -119,7 +126,7 @@ struct EngineImpl {
     void release() {
         void* ptrs[] = {d_prims, d_nodes, flags, list, fields, block_totals, block_offsets, packet_counts,
                         packet_offsets, b2a, masks, dc_voff, dc_verts, dc_norms, ctrl_region, eval_diag, miss,
-                        cell_words, bvh_work};
+                        cell_words, bvh_work, weld_bits, weld_prefix, weld_totals, weld_base};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         d_prims = nullptr; d_nodes = nullptr; flags = nullptr; list = nullptr; fields = nullptr;
@@ -130,6 +137,8 @@ struct EngineImpl {
         miss = nullptr;
         cell_words = nullptr;
         bvh_work = nullptr;
+        weld_bits = nullptr; weld_prefix = nullptr; weld_totals = nullptr; weld_base = nullptr;
+        weld_cap = 0;
         prims_cap = nodes_cap = dc_cap = packet_cap = miss_cap = cell_words_cap = bvh_work_cap = 0;
         if (h_bvh_ctl) cudaFreeHost(h_bvh_ctl);
         h_bvh_ctl = nullptr;
@@ -332,7 +341,8 @@ sdf_status sdf_engine_configure(sdf_engine* e, const sdf_config* cfg) {
     const size_t tC = sdfb::scan_tiles((unsigned)(nb * 512)) + 1;
     E.scanA_off = (sizeof(sdfb::Ctrl) + 255) & ~size_t(255);
     E.scanB_off = E.scanA_off + tA * 8;
-    E.scanC_off = E.scanB_off + tA * 8;
+    E.scanD_off = E.scanB_off + tA * 8;
+    E.scanC_off = E.scanD_off + tA * 8;
     E.ctrl_bytes = E.scanC_off + tC * 8;
     s = sdfb::dev_alloc(E.ctrl_region, E.ctrl_bytes);
     // per-cell buffers are allocated on first use
@@ -543,9 +553,20 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
     if (!out->primitive_ids) mask &= ~OUT_PRIMIDS;
     if (!out->normals) mask &= ~OUT_NORMALS;
 
+    const bool welded = !dc && (C.out_mask & OUT_WELDED);
+    if (welded && (!out->indices || (mask & (OUT_COLORS | OUT_UVS | OUT_PRIMIDS | OUT_NORMALS))))
+        return SDF_ERR_INVALID;  // an indexed mesh has per-vertex positions only, and needs its indices
     if (!dc) {
         // positions and indices only (no per-cell debug layout): the flat per-cell emission
-        const bool flat = !(mask & (OUT_COLORS | OUT_UVS | OUT_PRIMIDS | OUT_NORMALS)) && !(E.debug & 1);
+        const bool flat = !(mask & (OUT_COLORS | OUT_UVS | OUT_PRIMIDS | OUT_NORMALS)) && (!(E.debug & 1) || welded);
+        if (welded && E.weld_cap < (size_t)nb) {
+            E.weld_cap = 0;
+            if (dev_alloc(E.weld_bits, (size_t)nb * WELD_STRIDE) != SDF_OK ||
+                dev_alloc(E.weld_prefix, (size_t)nb * WELD_STRIDE) != SDF_OK ||
+                dev_alloc(E.weld_totals, (size_t)nb) != SDF_OK || dev_alloc(E.weld_base, (size_t)nb) != SDF_OK)
+                return SDF_ERR_NOMEM;
+            E.weld_cap = (size_t)nb;
+        }
         if (flat && E.cell_words_cap < (size_t)nb * 512) {
             if (dev_alloc(E.cell_words, (size_t)nb * 512) != SDF_OK) {
                 E.cell_words_cap = 0;
@@ -561,7 +582,26 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
             E.block_totals, E.block_offsets, 0, &ctrl->active_count, 1, scan_state(scanB), &ctrl->total_vertices, diag);
         check_launch();
         if (E.timing) cudaEventRecord(E.ev[3], st);
-        if (flat) {
+        if (welded) {
+            WeldBuffers wb;
+            wb.bits = E.weld_bits;
+            wb.prefix = E.weld_prefix;
+            wb.totals = E.weld_totals;
+            wb.base = E.weld_base;
+            wb.flags = E.flags;
+            wb.block_to_active = E.b2a;
+            const int wgrid = std::min(nb, num_sms() * 8);
+            k_weld_mark<<<wgrid, 256, 0, st>>>(gv, av, E.fields, wb);
+            check_launch();
+            unsigned long long* scanD = reinterpret_cast<unsigned long long*>(E.ctrl_region + E.scanD_off);
+            k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)nb)), SCAN_THREADS, 0, st>>>(
+                E.weld_totals, E.weld_base, 0, &ctrl->active_count, 1, scan_state(scanD), &ctrl->welded_vertices, diag);
+            check_launch();
+            k_weld_vertices<<<wgrid, 256, 0, st>>>(gv, av, E.fields, wb, mo.verts, mo.maxV);
+            check_launch();
+            k_weld_indices<<<persistent_grid(k_weld_indices, 256, nb * 2), 256, 0, st>>>(
+                gv, av, E.fields, E.cell_words, E.block_offsets, wb, mo.indices, mo.maxV);
+        } else if (flat) {
             k_mc_emit_cells<<<persistent_grid(k_mc_emit_cells, 256, nb * 2), 256, 0, st>>>(
                 gv, av, E.fields, E.cell_words, E.block_offsets, mo, mask);
         } else {
@@ -634,6 +674,7 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
         stats->bvh_cap_hits = (int64_t)h.diag.cap_hits;
         stats->scouted_blocks = culled ? (int64_t)h.diag.scouted : (int64_t)nb;
         stats->dc_fp64_cells = (int64_t)h.diag.fp64_cells;
+        stats->welded_vertices = welded ? (int64_t)h.welded_vertices : 0;
         stats->ms_total = std::chrono::duration<float, std::milli>(t1 - t0).count();
         if (E.timing) {
             cudaEventElapsedTime(&stats->ms_scout, E.ev[0], E.ev[1]);
@@ -644,7 +685,9 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
     }
     if (h.diag.timeout) return SDF_ERR_TIMEOUT;
     if (h.diag.stack_overflow) return SDF_ERR_STACK;
-    if (h.total_vertices > out->max_vertices || (dc && h.dc_vertices > E.dc_cap)) return SDF_ERR_CAPACITY;
+    if (h.total_vertices > out->max_vertices || (dc && h.dc_vertices > E.dc_cap) ||
+        (welded && h.welded_vertices > out->max_vertices))
+        return SDF_ERR_CAPACITY;
     return SDF_OK;
 }
 

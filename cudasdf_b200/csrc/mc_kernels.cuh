@@ -82,7 +82,7 @@ struct MeshOut {
     unsigned maxV;
 };
 
-enum { OUT_COLORS = 1, OUT_INDICES = 2, OUT_UVS = 4, OUT_PRIMIDS = 8, OUT_NORMALS = 16 };
+enum { OUT_COLORS = 1, OUT_INDICES = 2, OUT_UVS = 4, OUT_PRIMIDS = 8, OUT_NORMALS = 16, OUT_WELDED = 32 };
 
 __device__ __forceinline__ int active_count(const ActiveView& av) {
     int n = av.count_dev ? *av.count_dev : av.cap;

@@ -18,6 +18,7 @@
 #include "mc_kernels.cuh"
 #include "dc_kernels.cuh"
 #include "bvh_device.cuh"
+#include "weld.cuh"
 #include "surrogate.cuh"
 
 namespace sdfb {

@@ -183,7 +183,12 @@ typedef enum sdf_status {
 } sdf_status;
 
 /* output stream mask */
-enum { SDF_OUT_COLORS = 1, SDF_OUT_INDICES = 2, SDF_OUT_UVS = 4, SDF_OUT_PRIMIDS = 8, SDF_OUT_NORMALS = 16 };
+enum { SDF_OUT_COLORS = 1, SDF_OUT_INDICES = 2, SDF_OUT_UVS = 4, SDF_OUT_PRIMIDS = 8, SDF_OUT_NORMALS = 16,
+       /* indexed marching-cubes mesh (no counterpart in the reference, whose index buffer is the
+        * identity): `vertices` receives one vertex per crossed grid edge (stats.welded_vertices of
+        * them), `indices` (required) three per triangle, the soup's triangles in the soup's order;
+        * no colours, UVs, primitive ids or normals; max_vertices bounds both arrays */
+       SDF_OUT_WELDED = 32 };
 enum { SDF_TECH_MARCHING_CUBES = 0, SDF_TECH_DUAL_CONTOURING = 1 };
 /* DC vertex solver: the reference's feature-clustering + regularised QEF, or the mass-point QEF */
 enum { SDF_DC_SOLVER_REFERENCE = 0, SDF_DC_SOLVER_MASSPOINT = 1 };
@@ -222,6 +227,7 @@ typedef struct sdf_stats {
     float ms_scout, ms_field, ms_scan, ms_emit, ms_total; /* filled when timing is enabled */
     int64_t scouted_blocks;     /* blocks whose centre the exact scout evaluated (all, unless culled) */
     int64_t dc_fp64_cells;      /* mass-point DC: cells whose QEF was solved in FP64 (condition number) */
+    int64_t welded_vertices;    /* SDF_OUT_WELDED: vertices of the indexed mesh (total_vertices = indices) */
 } sdf_stats;
 
 typedef struct sdf_engine sdf_engine;
