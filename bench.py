@@ -278,6 +278,10 @@ def run_ours(args, rank, world):
         out["e2e"] = {"value": world * voxels / (e2e_ms * 1e-3) / 1e9, "unit": "Gvoxels/s",
                       "h2d_bytes_per_step": int(len(prims) * 160 + len(nodes) * 32),
                       "d2h_bytes_per_step": int(V * 16 + 8), "ms_per_step": e2e_ms}
+    if tech == L.TECH_MC:
+        out["welded"] = welded_output(args, world, eng, buf, V, flush, voxels,
+                                      make_config(cell, technique=tech, out_mask=mask | L.OUT_WELDED))
+        eng.configure(make_config(cell, technique=tech, out_mask=mask))  # same grid: buffers and surrogate stay
     out["fp32_peak"] = fp32_peak_tflops()
     out["counters"] = count_work(eng, buf, res) if rank == 0 else None
     eng.close()
@@ -285,6 +289,50 @@ def run_ours(args, rank, world):
         del buf
         out["dynamic_scene"] = dynamic_scene(args, world, prims, res, cell, tech, mask, spec, V, flush)
     return out
+
+
+def welded_output(args, world, eng, soup_buf, V, flush, voxels, cfg):
+    """The same extraction (surrogate-culled when the engine has it enabled) with the indexed output:
+    one vertex per crossed grid edge and three indices per triangle. Device time, a check of the mesh
+    against the soup just extracted (every corner's welded vertex within 1e-6 of its soup vertex), and
+    the end-to-end time with the smaller read-back (vertices + indices)."""
+    import torch
+
+    from cudasdf_b200 import _lib as L
+    from cudasdf_b200.engine import MeshBuffers
+    eng.configure(cfg)
+    wbuf = MeshBuffers(V + 1024, L.OUT_INDICES)
+    for _ in range(args.warmup):
+        eng.extract(wbuf)
+    times, st, stages = timed_extractions(eng, wbuf, args.steps, flush, world)
+    ms = max_over_ranks(sum(times) / len(times), world)
+    U = int(st["welded_vertices"])
+    idx = wbuf.indices[:V].long()
+    ok = int(st["total_vertices"]) == V and bool((idx >= 0).all() and (idx < U).all())
+    if ok:
+        err = (wbuf.vertices[idx, :3] - soup_buf.vertices[:V, :3]).abs().max().item()
+        ok = err <= 1e-6
+    res = {"value": job_throughput(world, voxels, ms), "ms_per_step": ms, "stage_ms": stages,
+           "welded_vertices": U, "indices": V, "matches_soup": ok}
+    if not args.no_e2e:
+        host_v = torch.empty((U + 1, 4), dtype=torch.float32, pin_memory=True)
+        host_i = torch.empty(V + 1, dtype=torch.int32, pin_memory=True)
+        e2e = []
+        for i in range(args.warmup + args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st = eng.extract(wbuf)
+            u, n = int(st["welded_vertices"]), int(st["total_vertices"])
+            host_v[:u].copy_(wbuf.vertices[:u], non_blocking=True)
+            host_i[:n].copy_(wbuf.indices[:n], non_blocking=True)
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                e2e.append((time.perf_counter() - t0) * 1e3)
+        e_ms = max_over_ranks(sum(e2e) / len(e2e), world)
+        res["e2e"] = {"value": world * voxels / (e_ms * 1e-3) / 1e9, "unit": "Gvoxels/s", "ms_per_step": e_ms,
+                      "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(U * 16 + V * 4)}
+    return res
 
 
 def dynamic_scene(args, world, prims, grid, cell, tech, mask, spec, V, flush):
@@ -675,7 +723,7 @@ def main():
                  "plain": {"value": r["plain"]["value"], "ms_per_step": r["plain"]["ms"],
                            "stage_ms": r["plain_stages"]},
                  "bvh_cap_hits": st["bvh_cap_hits"], "clocks": r["clocks"],
-                 "dynamic_scene": r.get("dynamic_scene"),
+                 "dynamic_scene": r.get("dynamic_scene"), "welded": r.get("welded"),
                  "gpu_launches": r["launches_per_step"] * args.steps})
     if "surrogate" in r:
         sg = r["surrogate"]

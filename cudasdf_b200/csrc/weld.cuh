@@ -55,10 +55,28 @@ __device__ __forceinline__ int edge_owner(const GridView& g, int X, int Y, int Z
     return best;
 }
 
-// Marks the owned crossed edges of every active block (one CTA per block) and counts them.
+// Whether this block owns the crossed edge at local lower sample (lx, ly, lz) along `axis`. An edge
+// off the block's lower faces (both other coordinates >= 1) has no adjacent cell in a block of smaller
+// linear index, so it is this block's when one of its adjacent cells here lies in the grid; edges on
+// the lower faces ask edge_owner.
+__device__ __forceinline__ bool weld_owns(const GridView& g, int lin, int bx, int by, int bz, int lx, int ly, int lz,
+                                          int axis, const unsigned* flags) {
+    const int l[3] = {lx, ly, lz};
+    const int b[3] = {bx, by, bz};
+    const int dims[3] = {g.w, g.h, g.d};
+    const int ua = axis == 0 ? 1 : 0, ub = axis == 2 ? 1 : 2;
+    if (l[ua] >= 1 && l[ub] >= 1)
+        return 8 * b[ua] + l[ua] - 1 <= dims[ua] - 2 && 8 * b[ub] + l[ub] - 1 <= dims[ub] - 2 &&
+               8 * b[axis] + l[axis] <= dims[axis] - 2;
+    return edge_owner(g, 8 * bx + lx, 8 * by + ly, 8 * bz + lz, axis, flags) == lin;
+}
+
+// Marks the owned crossed edges of every active block (one CTA per block, its row staged in shared
+// memory) and counts them.
 __global__ void __launch_bounds__(256) k_weld_mark(GridView g, ActiveView av, const float* __restrict__ fields,
                                                    WeldBuffers wb) {
-    __shared__ unsigned s_cnt[WELD_STRIDE];
+    __shared__ float s_row[FIELD_N];
+    __shared__ unsigned s_bits[WELD_STRIDE];
     const int n = active_count(av);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int a = blockIdx.x; a < n; a += gridDim.x) {
@@ -66,6 +84,8 @@ __global__ void __launch_bounds__(256) k_weld_mark(GridView g, ActiveView av, co
         int bx, by, bz;
         block_coord(g, lin, bx, by, bz);
         const float* f = fields + (size_t)a * FIELD_STRIDE;
+        for (int i = threadIdx.x; i < FIELD_N; i += blockDim.x) s_row[i] = f[i];
+        __syncthreads();
         for (int s0 = 0; s0 < WELD_STRIDE * 32; s0 += blockDim.x) {
             const int s = s0 + (int)threadIdx.x;
             bool own = false;
@@ -73,27 +93,33 @@ __global__ void __launch_bounds__(256) k_weld_mark(GridView g, ActiveView av, co
                 const int axis = s % 3, cell = s / 3;
                 const int lx = cell % 9, ly = (cell / 9) % 9, lz = cell / 81;
                 const int ux = lx + (axis == 0), uy = ly + (axis == 1), uz = lz + (axis == 2);
-                if (ux <= 8 && uy <= 8 && uz <= 8) {
-                    const bool s_lo = f[fidx(lx, ly, lz)] > 0.f, s_hi = f[fidx(ux, uy, uz)] > 0.f;
-                    if (s_lo != s_hi)
-                        own = edge_owner(g, bx * 8 + lx, by * 8 + ly, bz * 8 + lz, axis, wb.flags) == lin;
-                }
+                if (ux <= 8 && uy <= 8 && uz <= 8 && ((s_row[fidx(lx, ly, lz)] > 0.f) != (s_row[fidx(ux, uy, uz)] > 0.f)))
+                    own = weld_owns(g, lin, bx, by, bz, lx, ly, lz, axis, wb.flags);
             }
             const unsigned word = __ballot_sync(0xffffffffu, own);
-            const int wi = s0 / 32 + warp;
-            if (lane == 0) {
-                wb.bits[(size_t)a * WELD_STRIDE + wi] = word;
-                s_cnt[wi] = (unsigned)__popc(word);
-            }
+            if (lane == 0) s_bits[s0 / 32 + warp] = word;
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned run = 0;
-            for (int w = 0; w < WELD_STRIDE; ++w) {
-                wb.prefix[(size_t)a * WELD_STRIDE + w] = (unsigned short)run;
-                run += s_cnt[w];
+        // word prefixes (72 words: three per lane of warp 0) and the block's count
+        if (warp == 0) {
+            const int k0 = 3 * lane;
+            const unsigned c0 = k0 < WELD_STRIDE ? (unsigned)__popc(s_bits[k0]) : 0u;
+            const unsigned c1 = k0 + 1 < WELD_STRIDE ? (unsigned)__popc(s_bits[k0 + 1]) : 0u;
+            const unsigned c2 = k0 + 2 < WELD_STRIDE ? (unsigned)__popc(s_bits[k0 + 2]) : 0u;
+            const unsigned tsum = c0 + c1 + c2;
+            unsigned x = tsum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
             }
-            wb.totals[a] = run;
+            const unsigned e = x - tsum;
+            unsigned* bits = wb.bits + (size_t)a * WELD_STRIDE;
+            unsigned short* pre = wb.prefix + (size_t)a * WELD_STRIDE;
+            if (k0 < WELD_STRIDE) { bits[k0] = s_bits[k0]; pre[k0] = (unsigned short)e; }
+            if (k0 + 1 < WELD_STRIDE) { bits[k0 + 1] = s_bits[k0 + 1]; pre[k0 + 1] = (unsigned short)(e + c0); }
+            if (k0 + 2 < WELD_STRIDE) { bits[k0 + 2] = s_bits[k0 + 2]; pre[k0 + 2] = (unsigned short)(e + c0 + c1); }
+            if (lane == 31) wb.totals[a] = x;
         }
         __syncthreads();
     }
@@ -162,11 +188,17 @@ __global__ void __launch_bounds__(256) k_weld_indices(GridView g, ActiveView av,
                 const int X = c.x + min(corner_dx(c0), corner_dx(c1)), Y = c.y + min(corner_dy(c0), corner_dy(c1)),
                           Z = c.z + min(corner_dz(c0), corner_dz(c1));
                 const int axis = corner_dx(c0) != corner_dx(c1) ? 0 : (corner_dy(c0) != corner_dy(c1) ? 1 : 2);
-                const int olin = edge_owner(g, X, Y, Z, axis, wb.flags);
-                const int oa = wb.block_to_active[olin];
-                int obx, oby, obz;
-                block_coord(g, olin, obx, oby, obz);
-                const int slot = weld_slot(X - 8 * obx, Y - 8 * oby, Z - 8 * obz, axis);
+                const int lx = X - 8 * bx, ly = Y - 8 * by, lz = Z - 8 * bz;
+                // off this block's lower faces the edge is this block's (its cell here is in the grid)
+                const bool inner = (axis == 0 || lx >= 1) && (axis == 1 || ly >= 1) && (axis == 2 || lz >= 1);
+                int oa = a, slot = weld_slot(lx, ly, lz, axis);
+                if (!inner) {
+                    const int olin = edge_owner(g, X, Y, Z, axis, wb.flags);
+                    oa = wb.block_to_active[olin];
+                    int obx, oby, obz;
+                    block_coord(g, olin, obx, oby, obz);
+                    slot = weld_slot(X - 8 * obx, Y - 8 * oby, Z - 8 * obz, axis);
+                }
                 indices[v + j] = wb.base[oa] + weld_rank(wb, oa, slot);
             }
             v += 3;
