@@ -682,6 +682,7 @@ struct QuadSmem {
 struct QuadVerts {
     float3 v[4];
     float3 qc;
+    unsigned vi[4];  // the four cell vertex indices (the indexed output's corners)
 };
 
 __device__ __forceinline__ float3 cell_min_of_packet(const GridView& g, const int* list, unsigned base, int packet) {
@@ -701,8 +702,10 @@ __device__ __forceinline__ bool quad_vertices(const GridView& g, const int* list
     for (int j = 0; j < 4; ++j) vi[j] = B.vert_offsets[q[j]];
     if (vi[0] >= maxV || vi[1] >= maxV || vi[2] >= maxV || vi[3] >= maxV) return false;
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < 4; ++j) {
+        Q.vi[j] = vi[j];
         Q.v[j] = decode_vertex(B.cell_verts[vi[j]], cell_min_of_packet(g, list, base, q[j]), g.cell);
+    }
     Q.qc = f3(MUL(0.25f, ADD(ADD(ADD(Q.v[0].x, Q.v[1].x), Q.v[2].x), Q.v[3].x)),
               MUL(0.25f, ADD(ADD(ADD(Q.v[0].y, Q.v[1].y), Q.v[2].y), Q.v[3].y)),
               MUL(0.25f, ADD(ADD(ADD(Q.v[0].z, Q.v[1].z), Q.v[2].z), Q.v[3].z)));
@@ -820,7 +823,10 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quads(GridView g0, SceneView
                 if (!valid) continue;
                 const float3 nt = cross_ff(sub3(Q.v[1], Q.v[0]), sub3(Q.v[2], Q.v[0]));
                 const bool flip = dot3(nt, nref) < 0.f;
-                if (flip) { const float3 t = Q.v[1]; Q.v[1] = Q.v[3]; Q.v[3] = t; }
+                if (flip) {
+                    const float3 t = Q.v[1]; Q.v[1] = Q.v[3]; Q.v[3] = t;
+                    const unsigned u = Q.vi[1]; Q.vi[1] = Q.vi[3]; Q.vi[3] = u;
+                }
                 unsigned char fl = S.q_flags[i] | (flip ? 1 : 0);
                 bool alt = false;
                 if (QP.adaptive_diagonal) {
@@ -847,6 +853,11 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quads(GridView g0, SceneView
                         quv[1] = u0[1];
                         quv[2] = make_float2(MUL(ADD(u0[2].x, u1[1].x), 0.5f), MUL(ADD(u0[2].y, u1[1].y), 0.5f));
                         quv[3] = u1[2];
+                    }
+                    if (mask & OUT_WELDED) {  // indexed output: the corners' cell vertices
+#pragma unroll
+                        for (int j = 0; j < 6; ++j) out.indices[w + j] = Q.vi[alt ? order_b[j] : order_a[j]];
+                        continue;
                     }
 #pragma unroll
                     for (int j = 0; j < 6; ++j) {
@@ -908,6 +919,24 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quads(GridView g0, SceneView
             }
             __syncthreads();
         }
+    }
+}
+
+// Indexed dual-contouring output: every surface cell's vertex, decoded as the quads decode it
+// (:1851-1875), at its cell vertex index; the quads then write indices instead of positions.
+__global__ void __launch_bounds__(256) k_dc_weld_vertices(GridView g, ActiveView av, DcBuffers B, unsigned max_cells,
+                                                          float4* __restrict__ verts, unsigned max_verts) {
+    const long long n = (long long)active_count(av) * 512;
+    for (long long pk = blockIdx.x * (long long)blockDim.x + threadIdx.x; pk < n; pk += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(pk >> 9), tid = (int)(pk & 511);
+        int bx, by, bz;
+        block_coord(g, av.list[a], bx, by, bz);
+        const CellInfo c = cell_info(g, bx, by, bz, tid);
+        if (c.oob || !surface_mask(B.masks[pk])) continue;
+        const unsigned vi = B.vert_offsets[pk];
+        if (vi >= max_verts || vi >= max_cells) continue;
+        const float3 p = decode_vertex(B.cell_verts[vi], grid_loc(g, c.x, c.y, c.z), g.cell);
+        verts[vi] = make_float4(p.x, p.y, p.z, 1.f);
     }
 }
 

@@ -553,7 +553,7 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
     if (!out->primitive_ids) mask &= ~OUT_PRIMIDS;
     if (!out->normals) mask &= ~OUT_NORMALS;
 
-    const bool welded = !dc && (C.out_mask & OUT_WELDED);
+    const bool welded = (C.out_mask & OUT_WELDED) != 0;
     if (welded && (!out->indices || (mask & (OUT_COLORS | OUT_UVS | OUT_PRIMIDS | OUT_NORMALS))))
         return SDF_ERR_INVALID;  // an indexed mesh has per-vertex positions only, and needs its indices
     if (!dc) {
@@ -654,6 +654,11 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
         k_dc_quads<<<persistent_grid(k_dc_quads, BLK_THREADS, nb, quad_smem), BLK_THREADS, quad_smem, st>>>(
             gv, sv, time, av, B, nullptr, E.packet_counts, E.block_offsets, mo, mask, qp, &ctrl->tickets[2], diag);
         check_launch();
+        if (welded) {  // indexed output: the cell vertices themselves
+            k_dc_weld_vertices<<<persistent_grid(k_dc_weld_vertices, 256, nb * 2), 256, 0, st>>>(
+                gv, av, B, (unsigned)E.dc_cap, mo.verts, mo.maxV);
+            check_launch();
+        }
         if (E.timing) cudaEventRecord(E.ev[4], st);
     }
     record(cudaMemcpyAsync(E.h_ctrl, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
@@ -674,7 +679,7 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
         stats->bvh_cap_hits = (int64_t)h.diag.cap_hits;
         stats->scouted_blocks = culled ? (int64_t)h.diag.scouted : (int64_t)nb;
         stats->dc_fp64_cells = (int64_t)h.diag.fp64_cells;
-        stats->welded_vertices = welded ? (int64_t)h.welded_vertices : 0;
+        stats->welded_vertices = welded ? (int64_t)(dc ? h.dc_vertices : h.welded_vertices) : 0;
         stats->ms_total = std::chrono::duration<float, std::milli>(t1 - t0).count();
         if (E.timing) {
             cudaEventElapsedTime(&stats->ms_scout, E.ev[0], E.ev[1]);
@@ -686,7 +691,7 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
     if (h.diag.timeout) return SDF_ERR_TIMEOUT;
     if (h.diag.stack_overflow) return SDF_ERR_STACK;
     if (h.total_vertices > out->max_vertices || (dc && h.dc_vertices > E.dc_cap) ||
-        (welded && h.welded_vertices > out->max_vertices))
+        (welded && (dc ? h.dc_vertices : h.welded_vertices) > out->max_vertices))
         return SDF_ERR_CAPACITY;
     return SDF_OK;
 }

@@ -184,10 +184,11 @@ typedef enum sdf_status {
 
 /* output stream mask */
 enum { SDF_OUT_COLORS = 1, SDF_OUT_INDICES = 2, SDF_OUT_UVS = 4, SDF_OUT_PRIMIDS = 8, SDF_OUT_NORMALS = 16,
-       /* indexed marching-cubes mesh (no counterpart in the reference, whose index buffer is the
-        * identity): `vertices` receives one vertex per crossed grid edge (stats.welded_vertices of
-        * them), `indices` (required) three per triangle, the soup's triangles in the soup's order;
-        * no colours, UVs, primitive ids or normals; max_vertices bounds both arrays */
+       /* indexed mesh (no counterpart in the reference, whose index buffer is the identity):
+        * `vertices` receives the shared vertices (stats.welded_vertices of them: one per crossed grid
+        * edge for marching cubes, one per surface cell for dual contouring), `indices` (required)
+        * three per triangle, the soup's triangles in the soup's order; no colours, UVs, primitive
+        * ids or normals; max_vertices bounds both arrays */
        SDF_OUT_WELDED = 32 };
 enum { SDF_TECH_MARCHING_CUBES = 0, SDF_TECH_DUAL_CONTOURING = 1 };
 /* DC vertex solver: the reference's feature-clustering + regularised QEF, or the mass-point QEF */

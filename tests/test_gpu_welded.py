@@ -122,3 +122,30 @@ def test_welded_refuses_attributes_and_missing_indices():
     with pytest.raises(RuntimeError, match="SDF_ERR_INVALID"):
         eng.extract(MeshBuffers(100_000, 0))
     eng.close()
+
+
+@pytest.mark.parametrize("solver", [0, 1])
+def test_welded_dual_contouring_matches_soup(solver):
+    """Dual contouring is indexed by nature: the welded output is the surface cells' vertices and six
+    indices per quad (after the winding flip and the diagonal choice); every corner is its soup
+    vertex bit for bit."""
+    from cudasdf_b200 import _lib as L
+    from cudasdf_b200 import scenes as S
+    from cudasdf_b200.engine import Engine, MeshBuffers, make_config
+    prims = S.config_scene(2)
+    kw = dict(technique=L.TECH_DC, dc_solver=solver, projection_iters=3 if solver else 0,
+              adaptive_diagonal=1 if solver else 0)
+    soup = H.engine_run(prims, 96, L.TECH_DC, L.OUT_INDICES, debug=False, **{k: v for k, v in kw.items()
+                                                                               if k != "technique"})
+    eng = Engine()
+    eng.configure(make_config(S.cell_size_for(96), out_mask=L.OUT_INDICES | L.OUT_WELDED, **kw))
+    eng.set_scene(prims)
+    buf = MeshBuffers(2_000_000, L.OUT_INDICES)
+    st = eng.extract(buf)
+    V, U = int(st["total_vertices"]), int(st["welded_vertices"])
+    assert V == int(soup["stats"]["total_vertices"]) and U == int(st["dc_cell_vertices"]) and 0 < U < V
+    idx = buf.indices[:V].cpu().numpy().view(np.uint32)
+    assert idx.max() < U
+    verts = buf.vertices[:U].cpu().numpy()
+    assert verts[idx].tobytes() == soup["verts"].tobytes()
+    eng.close()
