@@ -536,7 +536,16 @@ def cpu_baseline(args):
     O.mc_blocks(sc, g, sample, 0.0, cores)
     t_mc = (time.perf_counter() - t0) / max(len(sample), 1) * nact
     total = t_scout + t_mc
+    # the same on one thread, on a sixteenth of the sample
+    t0 = time.perf_counter()
+    O.scout_range(sc, g, 0, max(scout_n // 16, 1), 0.0, 1)
+    t1_scout = (time.perf_counter() - t0) / max(scout_n // 16, 1) * nblocks
+    sample1 = sample[:max(len(sample) // 16, 1)]
+    t0 = time.perf_counter()
+    O.mc_blocks(sc, g, sample1, 0.0, 1)
+    t1_mc = (time.perf_counter() - t0) / max(len(sample1), 1) * nact
     return {"value": float(res) ** 3 / total / 1e9, "unit": "Gvoxels/s", "cores": cores, "kind": "port",
+            "value_1thread": float(res) ** 3 / (t1_scout + t1_mc) / 1e9,
             "sample": f"scout of {scout_n} of {nblocks} blocks + marching cubes of {len(sample)} of {nact} active "
                       f"blocks, scaled to the full {res}^3 extraction ({total:.1f} s estimated)"}
 
@@ -722,6 +731,7 @@ def main():
                  "stage_ms": r["stages"],
                  "plain": {"value": r["plain"]["value"], "ms_per_step": r["plain"]["ms"],
                            "stage_ms": r["plain_stages"]},
+                 "triangles_per_s": (st["total_vertices"] // 3) / (r["ms"] * 1e-3),
                  "bvh_cap_hits": st["bvh_cap_hits"], "clocks": r["clocks"],
                  "dynamic_scene": r.get("dynamic_scene"), "welded": r.get("welded"),
                  "gpu_launches": r["launches_per_step"] * args.steps})
