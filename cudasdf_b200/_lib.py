@@ -110,6 +110,7 @@ BATCH_SYMBOLS = ["sdf_batch_create", "sdf_batch_destroy", "sdf_batch_set_scenes"
 STATIC_SCOUT_SYMBOLS = ["sdf_scout_active_blocks_static", "sdf_scout_static_max_blocks"]
 ENGINE_SYMBOLS = ["sdf_engine_create", "sdf_engine_destroy", "sdf_engine_configure", "sdf_engine_set_scene",
                   "sdf_engine_set_scene_device",
+                  "sdf_engine_set_scene_async", "sdf_engine_extract_async", "sdf_engine_extract_wait",
                   "sdf_engine_extract", "sdf_engine_set_timing", "sdf_engine_set_debug", "sdf_engine_get_bvh",
                   "sdf_engine_buffer", "sdf_engine_read_buffer", "sdf_engine_eval", "sdf_engine_eval_distance", "sdf_engine_eval_normals", "sdf_engine_count_work", "sdf_measure_fp32_peak", "sdf_extract", "sdf_last_error", "sdf_version"]
 
@@ -149,6 +150,12 @@ def lib():
     L.sdf_engine_set_scene.restype = i
     L.sdf_engine_set_scene_device.argtypes = [vp, vp, i, vp]
     L.sdf_engine_set_scene_device.restype = i
+    L.sdf_engine_set_scene_async.argtypes = [vp, vp, i, vp]
+    L.sdf_engine_set_scene_async.restype = i
+    L.sdf_engine_extract_async.argtypes = [vp, f, ctypes.POINTER(SdfOutputs), vp, ctypes.POINTER(ctypes.c_uint64)]
+    L.sdf_engine_extract_async.restype = i
+    L.sdf_engine_extract_wait.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(SdfStats)]
+    L.sdf_engine_extract_wait.restype = i
     L.sdf_engine_extract.argtypes = [vp, f, ctypes.POINTER(SdfOutputs), vp, ctypes.POINTER(SdfStats)]
     L.sdf_engine_extract.restype = i
     L.sdf_engine_set_timing.argtypes = [vp, i]

@@ -108,7 +108,30 @@ struct EngineImpl {
     unsigned* weld_totals = nullptr;
     unsigned* weld_base = nullptr;
     size_t weld_cap = 0;
-    Ctrl* h_ctrl = nullptr;                // pinned read-back
+    Ctrl* h_ctrl = nullptr;                // pinned read-back, one Ctrl per extraction slot
+    // extractions in flight (sdf_engine_extract_async): each slot owns a read-back Ctrl and an event
+    struct Pending {
+        bool used = false;
+        uint64_t ticket = 0;
+        cudaEvent_t done = nullptr;
+        int nb = 0;
+        bool dc = false, welded = false, culled = false;
+        uint32_t max_vertices = 0;
+        size_t dc_cap = 0;
+        std::chrono::high_resolution_clock::time_point t0;
+    };
+    static constexpr int ASYNC_SLOTS = 4;
+    Pending pend[ASYNC_SLOTS];
+    uint64_t next_ticket = 0;
+    // pinned image of the uploaded scene (sdf_engine_set_scene_async uploads from it in stream order)
+    sdf_primitive* h_scene_prims = nullptr;
+    size_t h_scene_prims_cap = 0;
+    sdf_bvh_node* h_scene_nodes = nullptr;
+    size_t h_scene_nodes_cap = 0;
+    cudaEvent_t scene_ev = nullptr;        // the last upload from the image
+    bool scene_ev_pending = false;
+    uint64_t scene_gen = 0;                // host scene builds so far
+    uint64_t image_gen = ~0ull;            // the build the pinned image holds
     bool timing = false;
     int debug = 0;
     cudaEvent_t ev[8] = {};
@@ -144,6 +167,14 @@ struct EngineImpl {
         h_bvh_ctl = nullptr;
         if (h_ctrl) cudaFreeHost(h_ctrl);
         h_ctrl = nullptr;
+        for (auto& pd : pend)
+            if (pd.done) { cudaEventDestroy(pd.done); pd.done = nullptr; pd.used = false; }
+        if (h_scene_prims) cudaFreeHost(h_scene_prims);
+        if (h_scene_nodes) cudaFreeHost(h_scene_nodes);
+        h_scene_prims = nullptr; h_scene_nodes = nullptr;
+        h_scene_prims_cap = h_scene_nodes_cap = 0;
+        if (scene_ev) { cudaEventDestroy(scene_ev); scene_ev = nullptr; }
+        scene_ev_pending = false;
         for (auto& e : ev)
             if (e) { cudaEventDestroy(e); e = nullptr; }
         delete sur;
@@ -276,11 +307,13 @@ sdf_status sdf_engine_create(sdf_engine** out, int device) {
     if (device >= 0 && cudaSetDevice(device) != cudaSuccess) return SDF_ERR_CUDA;
     sdf_engine* e = new sdf_engine();
     cudaGetDevice(&e->impl.device);
-    if (cudaMallocHost(&e->impl.h_ctrl, sizeof(sdfb::Ctrl)) != cudaSuccess) {
+    if (cudaMallocHost(&e->impl.h_ctrl, sizeof(sdfb::Ctrl) * EngineImpl::ASYNC_SLOTS) != cudaSuccess) {
         delete e;
         return SDF_ERR_NOMEM;
     }
     for (auto& ev : e->impl.ev) cudaEventCreate(&ev);
+    for (auto& pd : e->impl.pend) cudaEventCreateWithFlags(&pd.done, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&e->impl.scene_ev, cudaEventDisableTiming);
     *out = e;
     return SDF_OK;
 }
@@ -350,19 +383,17 @@ sdf_status sdf_engine_configure(sdf_engine* e, const sdf_config* cfg) {
     return s;
 }
 
-sdf_status sdf_engine_set_scene(sdf_engine* e, const sdf_primitive* prims, int count) {
-    if (!e || count < 0 || (count > 0 && !prims)) return SDF_ERR_INVALID;
-    EngineImpl& E = e->impl;
-    cudaSetDevice(E.device);
-    // an unchanged scene (byte-identical primitives) keeps its host BVH and its trained surrogate; the
-    // upload below still runs
-    const bool same = count > 0 && E.scene.size() == (size_t)count && E.d_prims &&
+// The host part of a scene change (CudaSDFMesh::UpdateBVH): an unchanged scene (byte-identical
+// primitives) keeps its host BVH and its trained surrogate; the upload that follows still runs.
+static sdf_status scene_prepare(EngineImpl& E, const sdf_primitive* prims, int count) {
+    const bool same = count > 0 && !E.device_scene && E.scene.size() == (size_t)count && E.d_prims &&
                       memcmp(E.scene.data(), prims, (size_t)count * sizeof(sdf_primitive)) == 0;
     if (!same) {
         E.scene.assign(prims, prims + count);
         if (E.sur) E.sur->certified = E.sur->enabled = false;  // a new scene needs a new surrogate
         E.nbvh = sdfb::prepare_scene(prims, count, E.sorted, E.nodes);
         E.depth = sdfb::bvh_depth(E.nodes);
+        ++E.scene_gen;
     }
     if (E.depth + 1 > sdfb::MAP_STACK) return SDF_ERR_STACK;
     if (E.prims_cap < E.sorted.size()) {
@@ -373,6 +404,62 @@ sdf_status sdf_engine_set_scene(sdf_engine* e, const sdf_primitive* prims, int c
         if (sdfb::dev_alloc(E.d_nodes, E.nodes.size() * 2) != SDF_OK) return SDF_ERR_NOMEM;
         E.nodes_cap = E.nodes.size() * 2;
     }
+    return SDF_OK;
+}
+
+sdf_status sdf_engine_set_scene_async(sdf_engine* e, const sdf_primitive* prims, int count, void* stream) {
+    if (!e || count < 0 || (count > 0 && !prims)) return SDF_ERR_INVALID;
+    EngineImpl& E = e->impl;
+    cudaSetDevice(E.device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const sdf_status s = scene_prepare(E, prims, count);
+    if (s != SDF_OK) return s;
+    // refresh the pinned image when the scene changed (after the last upload from it has left)
+    if (E.image_gen != E.scene_gen || !E.h_scene_prims) {
+        if (E.scene_ev_pending) cudaEventSynchronize(E.scene_ev);
+        E.scene_ev_pending = false;
+        if (E.h_scene_prims_cap < E.sorted.size()) {
+            if (E.h_scene_prims) cudaFreeHost(E.h_scene_prims);
+            E.h_scene_prims = nullptr;
+            E.h_scene_prims_cap = 0;
+            if (cudaMallocHost(&E.h_scene_prims, std::max<size_t>(1, E.sorted.size()) * sizeof(sdf_primitive)) !=
+                cudaSuccess)
+                return SDF_ERR_NOMEM;
+            E.h_scene_prims_cap = std::max<size_t>(1, E.sorted.size());
+        }
+        if (E.h_scene_nodes_cap < E.nodes.size() || !E.h_scene_nodes) {
+            if (E.h_scene_nodes) cudaFreeHost(E.h_scene_nodes);
+            E.h_scene_nodes = nullptr;
+            E.h_scene_nodes_cap = 0;
+            if (cudaMallocHost(&E.h_scene_nodes, std::max<size_t>(1, E.nodes.size()) * sizeof(sdf_bvh_node)) !=
+                cudaSuccess)
+                return SDF_ERR_NOMEM;
+            E.h_scene_nodes_cap = std::max<size_t>(1, E.nodes.size());
+        }
+        if (!E.sorted.empty()) memcpy(E.h_scene_prims, E.sorted.data(), E.sorted.size() * sizeof(sdf_primitive));
+        if (!E.nodes.empty()) memcpy(E.h_scene_nodes, E.nodes.data(), E.nodes.size() * sizeof(sdf_bvh_node));
+        E.image_gen = E.scene_gen;
+    }
+    if (!E.sorted.empty() && cudaMemcpyAsync(E.d_prims, E.h_scene_prims, E.sorted.size() * sizeof(sdf_primitive),
+                                             cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return SDF_ERR_CUDA;
+    if (!E.nodes.empty() && cudaMemcpyAsync(E.d_nodes, E.h_scene_nodes, E.nodes.size() * sizeof(sdf_bvh_node),
+                                            cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return SDF_ERR_CUDA;
+    cudaEventRecord(E.scene_ev, st);
+    E.scene_ev_pending = true;
+    E.nprims = (int)E.sorted.size();
+    E.nnodes = (int)E.nodes.size();
+    E.device_scene = false;
+    return SDF_OK;
+}
+
+sdf_status sdf_engine_set_scene(sdf_engine* e, const sdf_primitive* prims, int count) {
+    if (!e || count < 0 || (count > 0 && !prims)) return SDF_ERR_INVALID;
+    EngineImpl& E = e->impl;
+    cudaSetDevice(E.device);
+    const sdf_status s = scene_prepare(E, prims, count);
+    if (s != SDF_OK) return s;
     if (!E.sorted.empty() &&
         cudaMemcpy(E.d_prims, E.sorted.data(), E.sorted.size() * sizeof(sdf_primitive), cudaMemcpyHostToDevice) !=
             cudaSuccess)
@@ -491,13 +578,11 @@ int sdf_engine_get_bvh(sdf_engine* e, sdf_bvh_node* nodes_out, int capacity, int
     return E.nnodes;
 }
 
-sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out, void* stream_ptr, sdf_stats* stats) {
+// Enqueues one extraction on `st` (no host synchronisation): the final counts are copied into the
+// slot's pinned Ctrl and the slot's event is recorded after them.
+static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* out, cudaStream_t st,
+                                 EngineImpl::Pending& P, sdfb::Ctrl* h_slot) {
     using namespace sdfb;
-    if (!e || !out || !out->vertices) return SDF_ERR_INVALID;
-    EngineImpl& E = e->impl;
-    if (!E.configured) return SDF_ERR_INVALID;
-    cudaSetDevice(E.device);
-    cudaStream_t st = static_cast<cudaStream_t>(stream_ptr);
     const sdf_config& C = E.cfg;
     const bool dc = C.technique == SDF_TECH_DUAL_CONTOURING;
     if (dc || (E.debug & 1)) {
@@ -661,27 +746,44 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
         }
         if (E.timing) cudaEventRecord(E.ev[4], st);
     }
-    record(cudaMemcpyAsync(E.h_ctrl, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
-    const cudaError_t err = cudaStreamSynchronize(st);
+    record(cudaMemcpyAsync(h_slot, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+    if (cudaEventRecord(P.done, st) != cudaSuccess) return SDF_ERR_CUDA;
+    P.nb = nb;
+    P.dc = dc;
+    P.welded = welded;
+    P.culled = culled;
+    P.max_vertices = out->max_vertices;
+    P.dc_cap = E.dc_cap;
+    P.t0 = t0;
+    return SDF_OK;
+}
+
+// Waits for the extraction of a slot and turns its read-back into stats and a status. The stage
+// times are the engine's timing events, valid for the most recent extraction only.
+static sdf_status engine_collect(EngineImpl& E, int slot, sdf_stats* stats, bool stage_times) {
+    using namespace sdfb;
+    EngineImpl::Pending& P = E.pend[slot];
+    const cudaError_t err = cudaEventSynchronize(P.done);
     auto t1 = std::chrono::high_resolution_clock::now();
+    P.used = false;
     if (err != cudaSuccess) {
         record(err);
         return SDF_ERR_CUDA;
     }
-    const Ctrl& h = *E.h_ctrl;
+    const Ctrl& h = E.h_ctrl[slot];
     if (stats) {
         memset(stats, 0, sizeof(*stats));
-        stats->total_blocks = nb;
+        stats->total_blocks = P.nb;
         stats->active_blocks = h.active_count;
         stats->total_vertices = h.total_vertices;
-        stats->written_vertices = std::min<int64_t>(h.total_vertices, out->max_vertices);
+        stats->written_vertices = std::min<int64_t>(h.total_vertices, P.max_vertices);
         stats->dc_cell_vertices = h.dc_vertices;
         stats->bvh_cap_hits = (int64_t)h.diag.cap_hits;
-        stats->scouted_blocks = culled ? (int64_t)h.diag.scouted : (int64_t)nb;
+        stats->scouted_blocks = P.culled ? (int64_t)h.diag.scouted : (int64_t)P.nb;
         stats->dc_fp64_cells = (int64_t)h.diag.fp64_cells;
-        stats->welded_vertices = welded ? (int64_t)(dc ? h.dc_vertices : h.welded_vertices) : 0;
-        stats->ms_total = std::chrono::duration<float, std::milli>(t1 - t0).count();
-        if (E.timing) {
+        stats->welded_vertices = P.welded ? (int64_t)(P.dc ? h.dc_vertices : h.welded_vertices) : 0;
+        stats->ms_total = std::chrono::duration<float, std::milli>(t1 - P.t0).count();
+        if (E.timing && stage_times) {
             cudaEventElapsedTime(&stats->ms_scout, E.ev[0], E.ev[1]);
             cudaEventElapsedTime(&stats->ms_field, E.ev[1], E.ev[2]);
             cudaEventElapsedTime(&stats->ms_scan, E.ev[2], E.ev[3]);
@@ -690,10 +792,46 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
     }
     if (h.diag.timeout) return SDF_ERR_TIMEOUT;
     if (h.diag.stack_overflow) return SDF_ERR_STACK;
-    if (h.total_vertices > out->max_vertices || (dc && h.dc_vertices > E.dc_cap) ||
-        (welded && (dc ? h.dc_vertices : h.welded_vertices) > out->max_vertices))
+    if (h.total_vertices > P.max_vertices || (P.dc && h.dc_vertices > P.dc_cap) ||
+        (P.welded && (P.dc ? h.dc_vertices : h.welded_vertices) > P.max_vertices))
         return SDF_ERR_CAPACITY;
     return SDF_OK;
+}
+
+sdf_status sdf_engine_extract_async(sdf_engine* e, float time, const sdf_outputs* out, void* stream,
+                                    uint64_t* ticket) {
+    if (!e || !out || !out->vertices || !ticket) return SDF_ERR_INVALID;
+    EngineImpl& E = e->impl;
+    if (!E.configured) return SDF_ERR_INVALID;
+    cudaSetDevice(E.device);
+    const int slot = (int)(E.next_ticket % EngineImpl::ASYNC_SLOTS);
+    EngineImpl::Pending& P = E.pend[slot];
+    if (P.used) {  // the oldest extraction still holds the slot: it must finish first
+        cudaEventSynchronize(P.done);
+        P.used = false;
+    }
+    const sdf_status s = engine_enqueue(E, time, out, static_cast<cudaStream_t>(stream), P, &E.h_ctrl[slot]);
+    if (s != SDF_OK) return s;
+    P.used = true;
+    P.ticket = E.next_ticket;
+    *ticket = E.next_ticket++;
+    return SDF_OK;
+}
+
+sdf_status sdf_engine_extract_wait(sdf_engine* e, uint64_t ticket, sdf_stats* stats) {
+    if (!e) return SDF_ERR_INVALID;
+    EngineImpl& E = e->impl;
+    cudaSetDevice(E.device);
+    const int slot = (int)(ticket % EngineImpl::ASYNC_SLOTS);
+    if (!E.pend[slot].used || E.pend[slot].ticket != ticket) return SDF_ERR_INVALID;  // unknown or collected
+    return engine_collect(E, slot, stats, ticket + 1 == E.next_ticket);
+}
+
+sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out, void* stream, sdf_stats* stats) {
+    uint64_t t = 0;
+    const sdf_status s = sdf_engine_extract_async(e, time, out, stream, &t);
+    if (s != SDF_OK) return s;
+    return sdf_engine_extract_wait(e, t, stats);
 }
 
 const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes) {

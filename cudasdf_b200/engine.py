@@ -104,6 +104,30 @@ class Engine:
         self._scene_keep = prims
         L.check(self._lib.sdf_engine_set_scene_device(self.h, prims.data_ptr(), n, sp), "sdf_engine_set_scene_device")
 
+    def set_scene_async(self, prims: np.ndarray, stream=None):
+        """set_scene with the upload enqueued on `stream` (sdf_engine_set_scene_async)."""
+        p = np.ascontiguousarray(prims, dtype=PRIM_DTYPE)
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        L.check(self._lib.sdf_engine_set_scene_async(self.h, p.ctypes.data, len(p), sp), "sdf_engine_set_scene_async")
+
+    def extract_async(self, out: MeshBuffers, time: float = 0.0, stream=None) -> int:
+        """Enqueues an extraction; returns its ticket for extract_wait."""
+        o = out.c_struct()
+        t = ctypes.c_uint64(0)
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        L.check(self._lib.sdf_engine_extract_async(self.h, float(time), ctypes.byref(o), sp, ctypes.byref(t)),
+                "sdf_engine_extract_async")
+        return t.value
+
+    def extract_wait(self, ticket: int, allow_capacity=False) -> dict:
+        st = L.SdfStats()
+        rc = self._lib.sdf_engine_extract_wait(self.h, ctypes.c_uint64(ticket), ctypes.byref(st))
+        if not (allow_capacity and rc == L.SDF_ERR_CAPACITY):
+            L.check(rc, "sdf_engine_extract_wait")
+        d = st.as_dict()
+        d["status"] = rc
+        return d
+
     def set_timing(self, on: bool):
         self._lib.sdf_engine_set_timing(self.h, 1 if on else 0)
 

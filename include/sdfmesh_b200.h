@@ -251,6 +251,20 @@ sdf_status sdf_engine_set_scene_device(sdf_engine* e, const sdf_primitive* prims
 /* One extraction on `stream` (a cudaStream_t, NULL = legacy default stream). The only host
  * synchronisation is the final count read-back into *stats. */
 sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out, void* stream, sdf_stats* stats);
+/* The extraction of sdf_engine_extract split in two, so that a caller can keep the GPU busy while it
+ * reads back earlier results: _async enqueues the whole extraction on `stream` and returns without
+ * waiting (a ticket names it); _wait blocks until that extraction has finished and fills `stats`,
+ * returning the status sdf_engine_extract would have. Extractions on one stream run one after another;
+ * each needs its own output buffers until the caller has read them. Up to four may be pending; a
+ * fifth _async first waits for the oldest. Stage times are filled for the most recent one only. No
+ * counterpart in the reference, whose Update blocks on its counts (CudaSDFMesh.cpp:466-468). */
+sdf_status sdf_engine_extract_async(sdf_engine* e, float time, const sdf_outputs* out, void* stream,
+                                    uint64_t* ticket);
+sdf_status sdf_engine_extract_wait(sdf_engine* e, uint64_t ticket, sdf_stats* stats);
+/* sdf_engine_set_scene with the upload enqueued on `stream` from a pinned copy of the prepared scene
+ * (refreshed when the primitives change), so it neither blocks the host nor waits for earlier work.
+ * Use the extraction stream. */
+sdf_status sdf_engine_set_scene_async(sdf_engine* e, const sdf_primitive* prims, int count, void* stream);
 /* Enables per-stage CUDA-event timing inside sdf_engine_extract. */
 void sdf_engine_set_timing(sdf_engine* e, int enabled);
 /* Debug outputs: bit 0 also writes the per-cell vertex counts/offsets of the drop-in layout in
