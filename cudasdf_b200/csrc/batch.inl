@@ -62,7 +62,7 @@ struct BatchGroup {
 template <class K>
 static int capped_grid(K kernel, int threads, long long items, size_t smem, int cap) {
     int per_sm = 0;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    opt_in_smem(kernel, smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
     if (per_sm < 1) per_sm = 1;
     if (cap > 0 && cap < per_sm) per_sm = cap;
@@ -177,6 +177,7 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
                                                                 &ctrl->total_vertices, B.first);
     record(cudaMemcpyAsync(B.h_ctrl, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
     record(cudaMemcpyAsync(B.h_first, B.first, (B.n + 1) * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    check_launch();
 }
 
 struct BatchImpl {
@@ -437,6 +438,7 @@ sdf_status sdf_batch_extract(sdf_batch* b, float time, const sdf_outputs* mc_out
     auto t0 = std::chrono::high_resolution_clock::now();
     const bool replay = I.exec && time == I.graph_time && same_outputs(mc_out, I.graph_out[0]) &&
                         same_outputs(dc_out, I.graph_out[1]);
+    const unsigned failures_before = g_launch_failures;
     if (replay) {
         record(cudaGraphLaunch(I.exec, st));
     } else {
@@ -445,6 +447,7 @@ sdf_status sdf_batch_extract(sdf_batch* b, float time, const sdf_outputs* mc_out
         enqueue_group(I.g[1], G, time, dc_out, I.out_mask, st);
     }
     const cudaError_t err = cudaStreamSynchronize(st);
+    if (g_launch_failures != failures_before) return SDF_ERR_CUDA;  // a kernel was not launched
     auto t1 = std::chrono::high_resolution_clock::now();
     if (err != cudaSuccess) {
         record(err);

@@ -583,6 +583,7 @@ int sdf_engine_get_bvh(sdf_engine* e, sdf_bvh_node* nodes_out, int capacity, int
 static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* out, cudaStream_t st,
                                  EngineImpl::Pending& P, sdfb::Ctrl* h_slot) {
     using namespace sdfb;
+    const unsigned failures_before = g_launch_failures;
     const sdf_config& C = E.cfg;
     const bool dc = C.technique == SDF_TECH_DUAL_CONTOURING;
     if (dc || (E.debug & 1)) {
@@ -746,6 +747,8 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
         }
         if (E.timing) cudaEventRecord(E.ev[4], st);
     }
+    check_launch();
+    if (g_launch_failures != failures_before) return SDF_ERR_CUDA;  // a kernel was not launched
     record(cudaMemcpyAsync(h_slot, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
     if (cudaEventRecord(P.done, st) != cudaSuccess) return SDF_ERR_CUDA;
     P.nb = nb;

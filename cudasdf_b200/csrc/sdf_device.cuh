@@ -397,6 +397,11 @@ struct Diag {
     int timeout;                    // a bounded wait gave up
 };
 
+// The stacks of map_multi (every point count shares them: a warp runs one walk at a time), 2 KB per
+// warp of the CTA.
+constexpr int MULTI_STACK_UINT4 = MAP_STACK * 2;  // uint4 per warp
+__shared__ uint4 s_multi_stack[MAP_WARPS * MULTI_STACK_UINT4];
+
 // map() for the 32 points of a warp. Must be called by all 32 lanes together (warp-uniform control
 // flow); lanes with valid == false take part in the walk but own no point.
 template <bool ATTR, bool COUNT = false>
@@ -634,31 +639,191 @@ __device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float 
     d1 = s1.d;
 }
 
+// map() distance for NP points per lane (32 x NP per warp) that are close together, such as the four
+// points of computeNormal's stencil: one shared stack whose entries carry NP lane masks, so the pop,
+// the node loads, the ballots and the push are shared by the NP walks, while every point makes its
+// own prune decision at every node it pops: each point's sequence of pops is its own depth-first walk
+// with the 64-entry stack and the 256-pop cap, as in map_warp. Leaf steps evaluate a lane's hit
+// points one after another. Must be called by all 32 lanes.
+template <int NP>
+__device__ __forceinline__ void map_multi(const SceneView& sc, const float3 (&p)[NP], bool valid, float time,
+                                          float (&d)[NP], Diag* diag) {
+    static_assert(NP >= 1 && NP <= 7, "a stack entry holds the node and NP masks in two uint4");
+    constexpr int W4 = (NP + 1 + 3) / 4;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned live = __ballot_sync(FULL, valid);
+    int it[NP];
+    PruneBound b[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+        d[i] = 1e10f;
+        it[i] = 0;
+    }
+    bool overflow = blockDim.x > 32 * MAP_WARPS;
+    if (sc.nnodes > 0 && live && !overflow) {
+#pragma unroll
+        for (int i = 0; i < NP; ++i) b[i].set(d[i]);
+        uint4(*stk)[W4] = reinterpret_cast<uint4(*)[W4]>(s_multi_stack + (threadIdx.x >> 5) * MULTI_STACK_UINT4);
+        int sp = 0;
+        int node = 0;
+        unsigned m[NP];
+#pragma unroll
+        for (int i = 0; i < NP; ++i) m[i] = live;
+        bool have = true;
+        for (;;) {
+            if (!have) {
+                if (sp == 0) break;
+                --sp;
+                unsigned w[4 * W4];
+#pragma unroll
+                for (int k = 0; k < W4; ++k) {
+                    const uint4 e = stk[sp][k];
+                    w[4 * k] = e.x;
+                    w[4 * k + 1] = e.y;
+                    w[4 * k + 2] = e.z;
+                    w[4 * k + 3] = e.w;
+                }
+                node = (int)w[0];
+#pragma unroll
+                for (int i = 0; i < NP; ++i) m[i] = w[i + 1];
+            }
+            have = false;
+            bool alive[NP];
+            bool any = false;
+#pragma unroll
+            for (int i = 0; i < NP; ++i) {
+                const bool pops = ((m[i] >> lane) & 1u) && it[i] < MAP_CAP;
+                if (pops) it[i]++;
+                alive[i] = pops && b[i].alive();
+                any |= alive[i];
+            }
+            if (!__any_sync(FULL, any)) continue;
+            const float4 na = __ldg(sc.nodes + 2 * node);
+            const float4 nb = __ldg(sc.nodes + 2 * node + 1);
+            unsigned hits = 0;
+            unsigned hm[NP];
+#pragma unroll
+            for (int i = 0; i < NP; ++i) {
+                const bool h = alive[i] && b[i].closer(p[i], na, nb);
+                hits |= (h ? 1u : 0u) << i;
+                hm[i] = __ballot_sync(FULL, h);
+            }
+            if (!__any_sync(FULL, hits != 0u)) continue;
+            const int left = __float_as_int(nb.z), right = __float_as_int(nb.w);
+            if (right == -1) {
+                const float4* pr = sc.prims + (size_t)left * PRIM_ROWS;
+                const Leaf L = load_leaf(pr);
+                // the lane's hit points in turn, selected by unrolled compares (state stays in registers)
+                while (__any_sync(FULL, hits != 0u)) {
+                    if (hits) {
+                        const int sel = __ffs(hits) - 1;
+                        hits &= hits - 1u;
+                        float3 ps = p[0];
+                        MapState<false> t;
+                        t.d = d[0];
+#pragma unroll
+                        for (int i = 1; i < NP; ++i)
+                            if (sel == i) {
+                                ps = p[i];
+                                t.d = d[i];
+                            }
+                        float3 pre;
+                        const float dp = leaf_distance(L, ps, time, pre);
+                        combine<false>(t, L.op, L.pos.w, pr, left, dp, pre);
+#pragma unroll
+                        for (int i = 0; i < NP; ++i)
+                            if (sel == i) {
+                                d[i] = t.d;
+                                b[i].set(t.d);
+                            }
+                    }
+                }
+            } else {
+                if (sp + 2 > MAP_STACK) { overflow = true; break; }  // the reference's stack holds both
+                __syncwarp();  // every lane has read stk[sp] (popped above) before it is overwritten
+                if (lane == 0) {
+                    unsigned w[4 * W4];
+                    w[0] = (unsigned)right;
+#pragma unroll
+                    for (int i = 0; i < NP; ++i) w[i + 1] = hm[i];
+#pragma unroll
+                    for (int i = NP + 1; i < 4 * W4; ++i) w[i] = 0u;
+#pragma unroll
+                    for (int k = 0; k < W4; ++k) stk[sp][k] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
+                }
+                __syncwarp();
+                ++sp;
+                node = left;
+#pragma unroll
+                for (int i = 0; i < NP; ++i) m[i] = hm[i];
+                have = true;
+            }
+        }
+        if (diag) {
+            unsigned ncap = 0;
+#pragma unroll
+            for (int i = 0; i < NP; ++i) ncap += __popc(__ballot_sync(FULL, valid && it[i] >= MAP_CAP));
+            if (lane == 0 && ncap) atomicAdd(&diag->cap_hits, (unsigned long long)ncap);
+        }
+    }
+    if (diag && overflow && lane == 0) atomicExch(&diag->stack_overflow, 1);
+    // non-union primitives: a linear pass in scene order (:703-803), one point at a time
+    if (valid) {
+        for (int j = sc.nbvh; j < sc.nprims; ++j) {
+            const float4* pr = sc.prims + (size_t)j * PRIM_ROWS;
+            const Leaf L = load_leaf(pr);
+#pragma unroll 1
+            for (int sel = 0; sel < NP; ++sel) {
+                float3 ps = p[0];
+                MapState<false> t;
+                t.d = d[0];
+#pragma unroll
+                for (int i = 1; i < NP; ++i)
+                    if (sel == i) {
+                        ps = p[i];
+                        t.d = d[i];
+                    }
+                float3 pre;
+                const float dp = leaf_distance(L, ps, time, pre);
+                combine<false>(t, L.op, L.pos.w, pr, j, dp, pre);
+#pragma unroll
+                for (int i = 0; i < NP; ++i)
+                    if (sel == i) d[i] = t.d;
+            }
+        }
+    }
+}
+
 // computeNormal (MarchingCubesKernels.cu:814-844) for the 32 points of a warp, with the distance at
-// p itself already known (map() at p, with or without attributes: the distance is the same).
+// p itself already known (map() at p, with or without attributes: the distance is the same); the
+// three offset points walk the BVH together (map_multi).
 __device__ __forceinline__ float3 normal_warp_at(const SceneView& sc, float3 p, float d0, bool valid, float time,
                                                  float cell, Diag* diag) {
     const float h = MUL(cell, 0.001f);
-    MapState<false> sx, sy, sz;
-    map_warp<false>(sc, f3(ADD(p.x, h), p.y, p.z), valid, time, sx, diag);
-    map_warp<false>(sc, f3(p.x, ADD(p.y, h), p.z), valid, time, sy, diag);
-    map_warp<false>(sc, f3(p.x, p.y, ADD(p.z, h)), valid, time, sz, diag);
-    const float3 g = f3(SUB(sx.d, d0), SUB(sy.d, d0), SUB(sz.d, d0));
+    const float3 pts[3] = {f3(ADD(p.x, h), p.y, p.z), f3(p.x, ADD(p.y, h), p.z), f3(p.x, p.y, ADD(p.z, h))};
+    float d[3];
+    map_multi<3>(sc, pts, valid, time, d, diag);
+    const float3 g = f3(SUB(d[0], d0), SUB(d[1], d0), SUB(d[2], d0));
     const float len = SQRT(dot3(g, g));
     if (len > 1e-6f) return f3(DIV(g.x, len), DIV(g.y, len), DIV(g.z, len));
     return f3(0.f, 1.f, 0.f);
 }
 
+// map() at computeNormal's four points (p, then p + h along x, y, z), walked together.
+__device__ __forceinline__ void stencil4_warp(const SceneView& sc, float3 p, bool valid, float time, float cell,
+                                              float (&d)[4], Diag* diag) {
+    const float h = MUL(cell, 0.001f);
+    const float3 pts[4] = {p, f3(ADD(p.x, h), p.y, p.z), f3(p.x, ADD(p.y, h), p.z), f3(p.x, p.y, ADD(p.z, h))};
+    map_multi<4>(sc, pts, valid, time, d, diag);
+}
+
 // computeNormal (MarchingCubesKernels.cu:814-844) for the 32 points of a warp.
 __device__ __forceinline__ float3 normal_warp(const SceneView& sc, float3 p, bool valid, float time, float cell,
                                               Diag* diag) {
-    const float h = MUL(cell, 0.001f);
-    MapState<false> s0, sx, sy, sz;
-    map_warp<false>(sc, p, valid, time, s0, diag);
-    map_warp<false>(sc, f3(ADD(p.x, h), p.y, p.z), valid, time, sx, diag);
-    map_warp<false>(sc, f3(p.x, ADD(p.y, h), p.z), valid, time, sy, diag);
-    map_warp<false>(sc, f3(p.x, p.y, ADD(p.z, h)), valid, time, sz, diag);
-    const float3 g = f3(SUB(sx.d, s0.d), SUB(sy.d, s0.d), SUB(sz.d, s0.d));
+    float d[4];
+    stencil4_warp(sc, p, valid, time, cell, d, diag);
+    const float3 g = f3(SUB(d[1], d[0]), SUB(d[2], d[0]), SUB(d[3], d[0]));
     const float len = SQRT(dot3(g, g));
     if (len > 1e-6f) return f3(DIV(g.x, len), DIV(g.y, len), DIV(g.z, len));
     return f3(0.f, 1.f, 0.f);

@@ -32,7 +32,14 @@ static std::mutex g_mutex;
 static void record(cudaError_t e) {
     if (e != cudaSuccess && g_last_error == 0) g_last_error = (int)e;
 }
-static void check_launch() { record(cudaGetLastError()); }
+static unsigned g_launch_failures = 0;  // launches refused so far (an enqueue compares before / after)
+static void check_launch() {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        record(e);
+        ++g_launch_failures;
+    }
+}
 
 static int num_sms() {
     static int n = 0;
@@ -45,10 +52,18 @@ static int num_sms() {
     return n;
 }
 
+// Static plus dynamic shared memory above 48 KB per block needs the kernel's opt-in.
+template <class K>
+static void opt_in_smem(K kernel, size_t dyn_smem) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kernel) == cudaSuccess && fa.sharedSizeBytes + dyn_smem > 48 * 1024)
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
+}
+
 template <class K>
 static int persistent_grid(K kernel, int threads, int work_items, size_t dyn_smem = 0) {
     int per_sm = 0;
-    if (dyn_smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
+    opt_in_smem(kernel, dyn_smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, dyn_smem);
     if (per_sm < 1) per_sm = 1;
     const int g = num_sms() * per_sm;
