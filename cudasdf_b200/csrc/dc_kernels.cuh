@@ -48,9 +48,11 @@ __global__ void k_dc_block_map(const int* __restrict__ list, const int* __restri
 
 // dcMarkCells (:1312-1346): corner masks + has-vertex counts. With fields_out the block field is
 // also stored for the solve pass.
+// rows_ready: the block rows in fields_out are already complete (the engine's shared-halo block field);
+// the kernel then only classifies the cells
 __global__ void __launch_bounds__(BLK_THREADS) k_dc_mark(GridView g0, SceneView sc0, float time, ActiveView av,
                                                          float* __restrict__ fields_out, DcBuffers B, unsigned* ticket,
-                                                         Diag* diag) {
+                                                         Diag* diag, bool rows_ready = false) {
     __shared__ __align__(16) float s_field[FIELD_STRIDE];
     __shared__ int s_item;
     const int n = active_count(av);
@@ -62,10 +64,16 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_mark(GridView g0, SceneView 
         int lin;
         unsigned bbase;
         resolve(av, av.list[a], g, sc, lin, bbase);
-        eval_block_field(g, sc, time, lin, s_field, diag);
+        if (rows_ready) {
+            const float4* src = reinterpret_cast<const float4*>(fields_out + (size_t)a * FIELD_STRIDE);
+            float4* dst = reinterpret_cast<float4*>(s_field);
+            for (int i = threadIdx.x; i < FIELD_STRIDE / 4; i += blockDim.x) dst[i] = src[i];
+        } else {
+            eval_block_field(g, sc, time, lin, s_field, diag);
+        }
         if (threadIdx.x < FIELD_STRIDE - FIELD_N) s_field[FIELD_N + threadIdx.x] = 0.f;
         __syncthreads();
-        if (fields_out) {
+        if (fields_out && !rows_ready) {
             float4* dst = reinterpret_cast<float4*>(fields_out + (size_t)a * FIELD_STRIDE);
             const float4* src = reinterpret_cast<const float4*>(s_field);
             for (int i = threadIdx.x; i < FIELD_STRIDE / 4; i += blockDim.x) dst[i] = src[i];

@@ -227,7 +227,7 @@ static float surrogate_margin(const EngineImpl& E) { return E.sur->eps + surroga
 template <bool COUNT>
 static sdf_status run_block_field(EngineImpl& E, const sdfb::SceneView& sv, float time, const sdfb::ActiveView& av,
                                   sdfb::Ctrl* ctrl, unsigned* packet_counts, cudaStream_t st,
-                                  unsigned* cell_words = nullptr) {
+                                  unsigned* cell_words = nullptr, bool counts = true) {
     using namespace sdfb;
     const size_t need = (size_t)E.nblocks * HALO_N;
     if (E.miss_cap < need) {
@@ -246,8 +246,8 @@ static sdf_status run_block_field(EngineImpl& E, const sdfb::SceneView& sv, floa
         E.gv, sv, time, av, E.fields, E.miss, &ctrl->halo_misses, &ctrl->tickets[4], &ctrl->diag);
     check_launch();
     k_field_gather<<<persistent_grid(k_field_gather, BLK_THREADS, E.nblocks), BLK_THREADS, 0, st>>>(
-        E.gv, av, E.fields, E.b2a, E.flags, COUNT ? nullptr : E.block_totals, packet_counts, &ctrl->tickets[3],
-        cell_words);
+        E.gv, av, E.fields, E.b2a, E.flags, (COUNT || !counts) ? nullptr : E.block_totals, packet_counts,
+        &ctrl->tickets[3], cell_words);
     check_launch();
     return SDF_OK;
 }
@@ -710,8 +710,11 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
         record(cudaMemsetAsync(E.b2a, 0xFF, (size_t)nb * sizeof(int), st));
         k_dc_block_map<<<(nb + 255) / 256, 256, 0, st>>>(E.list, &ctrl->active_count, nb, nb, E.b2a);
         check_launch();
+        // the block rows by the shared-halo block field (own samples two per lane, halos copied from
+        // active neighbours), then the cells classified from the finished rows
+        if (run_block_field<false>(E, sv, time, av, ctrl, nullptr, st, nullptr, false) != SDF_OK) return SDF_ERR_NOMEM;
         k_dc_mark<<<persistent_grid(k_dc_mark, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(gv, sv, time, av, E.fields, B,
-                                                                                      &ctrl->tickets[0], diag);
+                                                                                      &ctrl->tickets[5], diag, true);
         check_launch();
         const unsigned ncells_max = (unsigned)nb * 512u;
         k_exclusive_scan<<<std::max(1u, scan_tiles(ncells_max)), SCAN_THREADS, 0, st>>>(

@@ -570,7 +570,8 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_gather(GridView g0, Activ
                 row[h] = v;
             }
         }
-        block_counts(g, a, lin, s_field, s_red, nullptr, block_totals, packet_counts, cell_words);
+        if (block_totals || packet_counts || cell_words)  // dual contouring classifies the rows itself
+            block_counts(g, a, lin, s_field, s_red, nullptr, block_totals, packet_counts, cell_words);
     }
 }
 
