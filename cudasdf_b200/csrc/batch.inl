@@ -157,7 +157,14 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
         D.offsets = B.packet_offsets;
         record(cudaMemsetAsync(B.b2a, 0xFF, (size_t)nb * sizeof(int), st));
         k_dc_block_map<<<(nb + 255) / 256, 256, 0, st>>>(B.list, &ctrl->active_count, (int)nb, (int)nb, B.b2a);
-        k_dc_mark<<<G.mark, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, D, &ctrl->tickets[0], diag);
+        // block rows by the shared-halo block field, then the cells classified from the rows
+        k_field_plan<<<num_sms() * 8, 256, 0, st>>>(g0, av, B.flags, B.fields, B.b2a, B.miss, &ctrl->halo_misses);
+        k_field_own<false><<<G.own, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, &ctrl->tickets[3], diag);
+        k_field_miss<false><<<G.miss, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, B.miss, &ctrl->halo_misses,
+                                                            &ctrl->tickets[4], diag);
+        k_field_gather<<<G.gather, BLK_THREADS, 0, st>>>(g0, av, B.fields, B.b2a, B.flags, nullptr, nullptr,
+                                                         &ctrl->tickets[5], nullptr);
+        k_dc_mark<<<G.mark, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, D, &ctrl->tickets[0], diag, true);
         k_exclusive_scan<<<std::max(1u, scan_tiles(nb * 512u)), SCAN_THREADS, 0, st>>>(
             B.packet_counts, B.dc_voff, 0, &ctrl->active_count, 512, scan_state(B.scan(B.scanC_off)),
             &ctrl->dc_vertices, diag);
@@ -285,8 +292,8 @@ static sdf_status build_group(BatchGroup& B, const sdf_batch_scene* scenes, unsi
     if (s == SDF_OK) s = dev_alloc(B.first, (size_t)B.n + 1);
     if (s != SDF_OK) return s;
     const bool dc = B.technique == SDF_TECH_DUAL_CONTOURING;
+    s = dev_alloc(B.miss, nb * HALO_N);  // the shared-halo block field of both techniques
     if (!dc) {
-        s = dev_alloc(B.miss, nb * HALO_N);
         if (s == SDF_OK && !(out_mask & (OUT_COLORS | OUT_UVS | OUT_PRIMIDS | OUT_NORMALS)))
             s = dev_alloc(B.cell_words, nb * 512);
     } else {
