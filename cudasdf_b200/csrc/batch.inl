@@ -81,7 +81,7 @@ static BatchGrids batch_grids(long long blocks, const int ctas[4]) {
     G.gather = capped_grid(k_field_gather, BLK_THREADS, blocks, 0, 0);
     G.emit = capped_grid(k_mc_emit, BLK_THREADS, blocks, 0, ctas[1]);
     G.mark = capped_grid(k_dc_mark, BLK_THREADS, blocks, 0, ctas[0]);
-    G.solve = capped_grid(k_dc_solve, BLK_THREADS, blocks, sizeof(SolveSmem), ctas[2]);
+    G.solve = capped_grid(k_dc_solve, SOLVE_THREADS, blocks, sizeof(SolveSmem), ctas[2]);
     G.quads = capped_grid(k_dc_quads, BLK_THREADS, blocks, sizeof(QuadSmem), ctas[3]);
     G.count_quads = (int)std::min<long long>(std::max(1LL, blocks), (long long)num_sms() * 4);
     G.emit_cells = capped_grid(k_mc_emit_cells, 256, std::max(1LL, blocks * 2), 0, 0);
@@ -170,7 +170,7 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
             &ctrl->dc_vertices, diag);
         DcSolveParams sp = B.sp;
         sp.max_cell_vertices = (unsigned)B.dc_cap;
-        k_dc_solve<<<G.solve, BLK_THREADS, sizeof(SolveSmem), st>>>(g0, sc0, time, av, B.fields, D, sp,
+        k_dc_solve<<<G.solve, SOLVE_THREADS, sizeof(SolveSmem), st>>>(g0, sc0, time, av, B.fields, D, sp,
                                                                     &ctrl->tickets[1], diag);
         k_dc_count_quads<<<G.count_quads, 512, 0, st>>>(g0, av, D, B.packet_counts, B.block_totals);
         k_exclusive_scan<<<std::max(1u, scan_tiles(nb)), SCAN_THREADS, 0, st>>>(

@@ -163,13 +163,15 @@ namespace sdfb {
 // ------------------------------------------------------------------------------------------------
 // dcSolveCellVertices (:1348-1597)
 // ------------------------------------------------------------------------------------------------
-constexpr int DC_HERMITE_CAP = 1536;  // Hermite samples staged per pass
-constexpr int DC_CELL_CAP = 512;
+// threads of a k_dc_solve CTA (measured at 512^3: 23 ms; 31 ms with 128, 49 ms with 64)
+constexpr int SOLVE_THREADS = 256;
+constexpr int DC_CELL_CAP = 2 * SOLVE_THREADS;            // cells per pass (two per thread)
+constexpr int DC_HERMITE_CAP = 6 * SOLVE_THREADS;         // Hermite samples staged per pass
 constexpr int DC_EDGE_KEYS = 729 * 6;   // start corner in the 9^3 lattice x axis x direction
 
 struct SolveSmem {
     float field[FIELD_STRIDE];
-    unsigned warp_sums[BLK_THREADS / 32];
+    unsigned warp_sums[SOLVE_THREADS / 32];
     // solve cells of the current pass
     unsigned short cell_tid[DC_CELL_CAP];
     unsigned cell_vidx[DC_CELL_CAP];
@@ -315,7 +317,8 @@ __device__ __forceinline__ float3 value_gradient_warp(const SceneView& sc, float
 }
 
 // three CTAs per SM (80 registers): measured 23 ms for the 512^3 solve against 29 ms at 116 registers
-__global__ void __launch_bounds__(BLK_THREADS, 3) k_dc_solve(GridView g0, SceneView sc0, float time, ActiveView av,
+// three CTAs per SM (80 registers): measured 23 ms for the 512^3 solve against 29 ms at 116 registers
+__global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, SceneView sc0, float time, ActiveView av,
                                                           const float* __restrict__ fields_in, DcBuffers B,
                                                           DcSolveParams P, unsigned* ticket, Diag* diag) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -364,12 +367,12 @@ __global__ void __launch_bounds__(BLK_THREADS, 3) k_dc_solve(GridView g0, SceneV
                 vi[h] = v;
             }
             unsigned tot_h;
-            const unsigned h_pre = block_exclusive<BLK_THREADS>(hm[0] + hm[1], S.warp_sums, &tot_h);
+            const unsigned h_pre = block_exclusive<SOLVE_THREADS>(hm[0] + hm[1], S.warp_sums, &tot_h);
             const bool fit0 = h_pre + hm[0] <= (unsigned)DC_HERMITE_CAP;
             const bool fit1 = h_pre + hm[0] + hm[1] <= (unsigned)DC_HERMITE_CAP;
             const unsigned take = (want[0] && fit0 ? 1u : 0u) + (want[1] && fit1 ? 1u : 0u);
             unsigned ncells;
-            const unsigned c_pre = block_exclusive<BLK_THREADS>(take, S.warp_sums, &ncells);
+            const unsigned c_pre = block_exclusive<SOLVE_THREADS>(take, S.warp_sums, &ncells);
             int last = -1;  // the last cell (fitting or not wanted) this thread's pair covers
             if (cursor + 2 * (int)threadIdx.x < 512 && fit0) last = cursor + 2 * threadIdx.x;
             if (cursor + 2 * (int)threadIdx.x + 1 < 512 && fit1) last = cursor + 2 * threadIdx.x + 1;

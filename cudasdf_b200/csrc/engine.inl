@@ -728,7 +728,7 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
         sp.projection_iters = C.dc_solver == SDF_DC_SOLVER_MASSPOINT ? C.projection_iters : 0;
         sp.cond_threshold = C.cond_threshold > 0.f ? C.cond_threshold : 1e4f;
         const size_t solve_smem = sizeof(SolveSmem);
-        k_dc_solve<<<persistent_grid(k_dc_solve, BLK_THREADS, nb, solve_smem), BLK_THREADS, solve_smem, st>>>(
+        k_dc_solve<<<persistent_grid(k_dc_solve, SOLVE_THREADS, nb, solve_smem), SOLVE_THREADS, solve_smem, st>>>(
             gv, sv, time, av, E.fields, B, sp, &ctrl->tickets[1], diag);
         check_launch();
         if (E.timing) cudaEventRecord(E.ev[3], st);

@@ -304,7 +304,7 @@ void launchDCSolveCellVertices(sdf_grid* grid, int numActiveBlocks, float time, 
     sp.projection_iters = 0;
     sp.cond_threshold = 1e4f;
     const size_t smem = sizeof(SolveSmem);
-    k_dc_solve<<<persistent_grid(k_dc_solve, BLK_THREADS, numActiveBlocks, smem), BLK_THREADS, smem>>>(
+    k_dc_solve<<<persistent_grid(k_dc_solve, SOLVE_THREADS, numActiveBlocks, smem), SOLVE_THREADS, smem>>>(
         grid_view(*grid), scene_view(*grid), time, av, nullptr, dc_buffers_of(*grid), sp, s.tickets, s.diag);
     check_launch();
 }
