@@ -317,7 +317,6 @@ __device__ __forceinline__ float3 value_gradient_warp(const SceneView& sc, float
 }
 
 // three CTAs per SM (80 registers): measured 23 ms for the 512^3 solve against 29 ms at 116 registers
-// three CTAs per SM (80 registers): measured 23 ms for the 512^3 solve against 29 ms at 116 registers
 __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, SceneView sc0, float time, ActiveView av,
                                                           const float* __restrict__ fields_in, DcBuffers B,
                                                           DcSolveParams P, unsigned* ticket, Diag* diag) {
