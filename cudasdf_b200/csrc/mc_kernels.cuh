@@ -452,17 +452,56 @@ __global__ void __launch_bounds__(256) k_field_plan(GridView g0, ActiveView av, 
     }
 }
 
-// own samples: one CTA per active block, its eight warps on the eight 4 x 4 x 4 bricks (all warps of
-// the SM walk the BVH near the same block, which keeps the nodes they read in L1)
+// one task of the listed halo samples: entries [32 t, 32 t + 32) of the list (all lanes of a warp)
+template <bool COUNT>
+__device__ __forceinline__ void miss_task(const GridView& g0, const SceneView& sc0, float time, const ActiveView& av,
+                                          float* __restrict__ fields, const unsigned* __restrict__ miss, int nmiss,
+                                          int t, Diag* diag) {
+    const int lane = threadIdx.x & 31;
+    const int e = t * 32 + lane;
+    const bool live = e < nmiss;
+    const unsigned m = live ? miss[e] : miss[t * 32];
+    const int a = (int)(m >> 8);
+    GridView g = g0;
+    SceneView sc = sc0;
+    int lin;
+    unsigned bbase;
+    resolve(av, av.list[a], g, sc, lin, bbase);
+    int sx, sy, sz, bx, by, bz;
+    halo_coord((int)(m & 255u), sx, sy, sz);
+    block_coord(g, lin, bx, by, bz);
+    const int gx = bx * 8 + sx, gy = by * 8 + sy, gz = bz * 8 + sz;
+    const bool inside = live && gx < g.w && gy < g.h && gz < g.d;
+    const float3 p = grid_loc(g, gx, gy, gz);
+    // the warp walks one scene's BVH at a time (a batch's tasks can straddle two scenes)
+    unsigned pending = __ballot_sync(0xffffffffu, live);
+    while (pending) {
+        const unsigned lead_base = __shfl_sync(0xffffffffu, bbase, __ffs(pending) - 1);
+        const bool mine = live && bbase == lead_base && ((pending >> lane) & 1u);
+        SceneView scw = sc;
+        if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead_base)].sc;
+        MapState<false> st;
+        map_warp<false, COUNT>(scw, p, mine && inside, time, st, diag);
+        if (mine) fields[(size_t)a * FIELD_STRIDE + (sz * 9 + sy) * 9 + sx] = inside ? st.d : 0.f;
+        pending &= ~__ballot_sync(0xffffffffu, mine);
+    }
+}
+
+// own samples: eight 4 x 4 x 4 bricks of 64 samples per active block, two z-neighbours per lane; each
+// warp claims one brick at a time in (active block, brick) order, so the warps of an SM walk the BVH
+// near the same few blocks (the nodes they read stay in L1) and no warp waits for a block's slowest
+// brick (measured 11.6 ms against 12.3 ms with one CTA per block at 1024^3)
 template <bool COUNT>
 __global__ void __launch_bounds__(BLK_THREADS) k_field_own(GridView g0, SceneView sc0, float time, ActiveView av,
                                                          float* __restrict__ fields, unsigned* ticket, Diag* diag) {
-    __shared__ int s_item;
     const int n = active_count(av);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31;
     for (;;) {
-        const int a = claim(ticket, n, &s_item);
-        if (a < 0) break;
+        int t = 0;
+        if (lane == 0) t = (int)atomicAdd(ticket, 1u);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= n * (OWN_N / 64)) break;
+        const int a = t / (OWN_N / 64), brick = t % (OWN_N / 64);
         GridView g = g0;
         SceneView sc = sc0;
         int lin;
@@ -470,8 +509,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_own(GridView g0, SceneVie
         resolve(av, av.list[a], g, sc, lin, bbase);
         int bx, by, bz;
         block_coord(g, lin, bx, by, bz);
-        // eight 4 x 4 x 4 bricks of 64 samples, one per warp, two z-neighbours per lane
-        for (int brick = warp; brick < OWN_N / 64; brick += nwarps) {
+        {
             const int sx = (brick & 1) * 4 + (lane & 3), sy = ((brick >> 1) & 1) * 4 + ((lane >> 2) & 3);
             const int sz0 = (brick >> 2) * 4 + 2 * (lane >> 4), sz1 = sz0 + 1;
             const int gx = bx * 8 + sx, gy = by * 8 + sy, gz0 = bz * 8 + sz0, gz1 = gz0 + 1;
@@ -500,33 +538,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_miss(GridView g0, SceneVi
         if (lane == 0) t = (int)atomicAdd(ticket, 1u);
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= tasks) break;
-        const int e = t * 32 + lane;
-        const bool live = e < nmiss;
-        const unsigned m = live ? miss[e] : miss[t * 32];
-        const int a = (int)(m >> 8);
-        GridView g = g0;
-        SceneView sc = sc0;
-        int lin;
-        unsigned bbase;
-        resolve(av, av.list[a], g, sc, lin, bbase);
-        int sx, sy, sz, bx, by, bz;
-        halo_coord((int)(m & 255u), sx, sy, sz);
-        block_coord(g, lin, bx, by, bz);
-        const int gx = bx * 8 + sx, gy = by * 8 + sy, gz = bz * 8 + sz;
-        const bool inside = live && gx < g.w && gy < g.h && gz < g.d;
-        const float3 p = grid_loc(g, gx, gy, gz);
-        // the warp walks one scene's BVH at a time (a batch's tasks can straddle two scenes)
-        unsigned pending = __ballot_sync(0xffffffffu, live);
-        while (pending) {
-            const unsigned lead_base = __shfl_sync(0xffffffffu, bbase, __ffs(pending) - 1);
-            const bool mine = live && bbase == lead_base && ((pending >> lane) & 1u);
-            SceneView scw = sc;
-            if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead_base)].sc;
-            MapState<false> st;
-            map_warp<false, COUNT>(scw, p, mine && inside, time, st, diag);
-            if (mine) fields[(size_t)a * FIELD_STRIDE + (sz * 9 + sy) * 9 + sx] = inside ? st.d : 0.f;
-            pending &= ~__ballot_sync(0xffffffffu, mine);
-        }
+        miss_task<COUNT>(g0, sc0, time, av, fields, miss, nmiss, t, diag);
     }
 }
 
