@@ -40,6 +40,9 @@ CONFIGS = {
     "c3": {"config": 3, "technique": 1, "workload": "dc_masspoint_4096prims_512",
            "dc": {"dc_solver": 1, "projection_iters": 3, "adaptive_diagonal": 1, "cond_threshold": 1e4}},
     "c4": {"config": 4, "technique": 0, "workload": "mc_16384prims_1024", "surrogate": True},
+    # the 256^3 scene with the dual-contouring options of c3: a case small enough for kernel captures
+    "c3s": {"config": 2, "technique": 1, "workload": "dc_masspoint_256prims_256",
+            "dc": {"dc_solver": 1, "projection_iters": 3, "adaptive_diagonal": 1, "cond_threshold": 1e4}},
     "c5": {"config": 5, "technique": -1, "workload": "batch_256scenes_mixed_mc_dc", "batch": True},
 }
 

@@ -185,10 +185,45 @@ struct SolveSmem {
     unsigned short edge_rep[DC_EDGE_KEYS];  // key -> representative sample, 0xFFFF if unclaimed
     unsigned short h_rep[DC_HERMITE_CAP];   // sample -> its representative
     unsigned short rep_list[DC_HERMITE_CAP];
+    // computeNormal stencils spread over all warps: map() at (p, p + h x, p + h y, p + h z) of up to
+    // STENCIL_CHUNK centres at a time, one point per lane
+    float st_d[4 * 256];
     int nrep;
     int next_cursor;
     int item;
 };
+constexpr int STENCIL_CHUNK = 256;
+
+// The four-point stencil (MarchingCubesKernels.cu:814-844) of n centres, spread over all warps of the
+// CTA (lane i of the pass takes centre i / 4, offset i % 4), STENCIL_CHUNK centres per round; `use`
+// receives (centre, d0, d1, d2, d3) from one thread per centre. Called by all threads.
+template <class Centre, class Use>
+__device__ __forceinline__ void stencil_all_warps(const SceneView& sc, int n, float cell, float time, float* st_d,
+                                                  Centre centre, Use use, Diag* diag) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const float h = MUL(cell, 0.001f);
+    for (int c0 = 0; c0 < n; c0 += STENCIL_CHUNK) {
+        const int cn = min(STENCIL_CHUNK, n - c0);
+        for (int base = warp * 32; base < 4 * cn; base += nwarps * 32) {
+            const int i = base + lane;
+            const bool valid = i < 4 * cn;
+            float3 p = f3(0.f, 0.f, 0.f);
+            if (valid) {
+                const float3 c = centre(c0 + (i >> 2));
+                const int k = i & 3;
+                p = k == 0 ? c : (k == 1 ? f3(ADD(c.x, h), c.y, c.z) : (k == 2 ? f3(c.x, ADD(c.y, h), c.z)
+                                                                               : f3(c.x, c.y, ADD(c.z, h))));
+            }
+            MapState<false> st;
+            map_warp<false>(sc, p, valid, time, st, diag);
+            if (valid) st_d[i] = st.d;
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < cn; j += blockDim.x)
+            use(c0 + j, st_d[4 * j], st_d[4 * j + 1], st_d[4 * j + 2], st_d[4 * j + 3]);
+        __syncthreads();
+    }
+}
 
 __device__ __forceinline__ float3 hermite_point(const GridView& g, const CellInfo& c, const float cv[8], int e) {
     return edge_point(g, c.x, c.y, c.z, cv, e);
@@ -424,21 +459,22 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
             }
             __syncthreads();
             const int nrep = S.nrep;
-            for (int base = warp * 32; base < nrep; base += nwarps * 32) {
-                const int r = base + lane;
-                const bool valid = r < nrep;
-                const int i = valid ? S.rep_list[r] : 0;
-                float3 p = f3(0.f, 0.f, 0.f);
-                if (valid) {
+            stencil_all_warps(
+                sc, nrep, g.cell, time, S.st_d,
+                [&](int r) {
+                    const int i = S.rep_list[r];
                     const CellInfo c = cell_info(g, bx, by, bz, S.h_cell[i] >> 4);
                     float cv[8];
                     (void)cell_case(S.field, c.lx, c.ly, c.lz, cv);
-                    p = edge_point(g, c.x, c.y, c.z, cv, S.h_cell[i] & 15);
-                }
-                const float3 nrm = normal_warp(sc, p, valid, time, g.cell, diag);
-                if (valid) S.h_n[i] = nrm;
-            }
-            __syncthreads();
+                    return edge_point(g, c.x, c.y, c.z, cv, S.h_cell[i] & 15);
+                },
+                [&](int r, float d0, float d1, float d2, float d3) {
+                    const float3 gr = f3(SUB(d1, d0), SUB(d2, d0), SUB(d3, d0));
+                    const float len = SQRT(dot3(gr, gr));
+                    S.h_n[S.rep_list[r]] = len > 1e-6f ? f3(DIV(gr.x, len), DIV(gr.y, len), DIV(gr.z, len))
+                                                       : f3(0.f, 1.f, 0.f);
+                },
+                diag);
             for (int i = threadIdx.x; i < (int)nh; i += blockDim.x)
                 if (S.h_rep[i] != i) S.h_n[i] = S.h_n[S.h_rep[i]];
             __syncthreads();
@@ -460,14 +496,15 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
             // mass-point mode: project the vertex onto the surface along the gradient
             if (P.solver == SDF_DC_SOLVER_MASSPOINT) {
                 for (int it = 0; it < P.projection_iters; ++it) {
-                    for (int base = warp * 32; base < (int)ncells; base += nwarps * 32) {
-                        const int i = base + lane;
-                        const bool valid = i < (int)ncells;
-                        const float3 x = valid ? S.cell_x[i] : f3(0.f, 0.f, 0.f);
-                        float d;
-                        const float3 gr = value_gradient_warp(sc, x, valid, time, g.cell, d, diag);
-                        if (valid && isfinite(d)) {
+                    stencil_all_warps(
+                        sc, (int)ncells, g.cell, time, S.st_d, [&](int i) { return S.cell_x[i]; },
+                        [&](int i, float d, float d1, float d2, float d3) {
+                            float3 gr = f3(SUB(d1, d), SUB(d2, d), SUB(d3, d));
+                            const float len = SQRT(dot3(gr, gr));
+                            gr = len > 1e-6f ? f3(DIV(gr.x, len), DIV(gr.y, len), DIV(gr.z, len)) : f3(0.f, 0.f, 0.f);
+                            if (!isfinite(d)) return;
                             // keep the step inside the cell's soft-clamp box
+                            const float3 x = S.cell_x[i];
                             const CellInfo c = cell_info(g, bx, by, bz, S.cell_tid[i]);
                             const float3 cmin = grid_loc(g, c.x, c.y, c.z);
                             const float margin = 0.10f * g.cell;
@@ -476,9 +513,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
                                    CLAMP(y.y, cmin.y - margin, cmin.y + g.cell + margin),
                                    CLAMP(y.z, cmin.z - margin, cmin.z + g.cell + margin));
                             S.cell_x[i] = y;
-                        }
-                    }
-                    __syncthreads();
+                        },
+                        diag);
                 }
             }
             // soft clamp, hard clamp to the cell, blend towards the cell centre (:1556-1577)
