@@ -818,7 +818,7 @@ def main():
 # and the smooth-union blend (about 12).
 FLOP_PER_NODE = 12
 # DRAM bytes per active block of the block-field stage, from an ncu capture (see roofline())
-TRAFFIC_PER_ACTIVE_BLOCK = (14.364928e6 + 14.197504e6) / 12524
+TRAFFIC_PER_ACTIVE_BLOCK = (14.046208e6 + 13.871616e6) / 12524
 FLOP_PER_LEAF = 44 + 12 + 12 + 1
 
 
@@ -837,7 +837,7 @@ def roofline(r):
             "peak_source": "measured by the library's FMA loop on this GPU (no FP32 figure in MEASURED_PEAKS.json)",
             "traffic": TRAFFIC_PER_ACTIVE_BLOCK * active,
             "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one k_field_own capture on the "
-                              "256^3 workload (profiles/k_field_own_mc_256prims_256.md), 2.28 KB per active block, "
+                              "256^3 workload (profiles/k_field_own_mc_256prims_256.md), 2.23 KB per active block, "
                               "scaled by this run's active blocks",
             "work": c}
 
