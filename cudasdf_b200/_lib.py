@@ -108,6 +108,7 @@ SURROGATE_SYMBOLS = ["sdf_surrogate_default_config", "sdf_surrogate_train", "sdf
 BATCH_SYMBOLS = ["sdf_batch_create", "sdf_batch_destroy", "sdf_batch_set_scenes", "sdf_batch_extract",
                  "sdf_batch_capture"]
 STATIC_SCOUT_SYMBOLS = ["sdf_scout_active_blocks_static", "sdf_scout_static_max_blocks"]
+EXPORT_SYMBOLS = ["sdf_write_obj"]
 ENGINE_SYMBOLS = ["sdf_engine_create", "sdf_engine_destroy", "sdf_engine_configure", "sdf_engine_set_scene",
                   "sdf_engine_set_scene_device",
                   "sdf_engine_set_scene_async", "sdf_engine_extract_async", "sdf_engine_extract_wait",
@@ -213,6 +214,8 @@ def lib():
     L.sdf_scout_active_blocks_static.argtypes = [G, f]
     L.sdf_scout_active_blocks_static.restype = i
     L.sdf_scout_static_max_blocks.restype = u
+    L.sdf_write_obj.argtypes = [ctypes.c_char_p, vp, ctypes.c_uint64, vp, ctypes.c_uint64, vp]
+    L.sdf_write_obj.restype = i
     L.sdf_last_error.restype = i
     L.sdf_version.restype = ctypes.c_char_p
     _lib = L

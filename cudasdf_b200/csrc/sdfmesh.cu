@@ -368,3 +368,4 @@ const char* sdf_version(void) { return "sdfmesh_b200 0.1 (sm_100a)"; }
 #include "surrogate.inl"
 #include "batch.inl"
 #include "noalloc.inl"
+#include "obj_export.inl"

@@ -431,6 +431,18 @@ sdf_status sdf_batch_extract(sdf_batch* b, float time, const sdf_outputs* mc_out
 sdf_status sdf_batch_capture(sdf_batch* b, float time, const sdf_outputs* mc_out, const sdf_outputs* dc_out,
                              void* stream, int tune);
 
+/* Writes a mesh read back to HOST memory as Wavefront OBJ text, in the format of the reference's
+ * ExportMeshToOBJ (src/main.cpp:1043-1115): "# Exported from CudaSDF", "# Generated: <file name>", a
+ * blank line, "v x y z" per vertex, a blank line, optionally "vt u v" per vertex and a blank line, then
+ * one face line per triangle with 1-based indices ("f a b c", or "f a/a b/b c/c" when uvs is given).
+ * Floats are printed as std::ostream prints them by default (%g, six significant digits).
+ * indices == NULL: the triangle soup of the reference (face k = vertices 3k, 3k+1, 3k+2);
+ * otherwise num_indices / 3 faces from the index buffer (the SDF_OUT_WELDED output).
+ * SDF_ERR_INVALID if the file cannot be written, an index is >= num_vertices, or num_vertices == 0
+ * (the file then holds the header only, as the reference leaves it). No GPU is used. */
+sdf_status sdf_write_obj(const char* path, const sdf_float4* vertices, uint64_t num_vertices, const uint32_t* indices,
+                         uint64_t num_indices, const sdf_float2* uvs);
+
 /* First CUDA error recorded by a drop-in launcher since the last call (cleared on read). */
 int sdf_last_error(void);
 /* Library version string. */

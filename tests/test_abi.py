@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in declared_functions() if not hasattr(L, n)]
     assert not missing, missing
     assert set(_lib.DROPIN_SYMBOLS + _lib.ENGINE_SYMBOLS + _lib.SURROGATE_SYMBOLS + _lib.BATCH_SYMBOLS +
-               _lib.STATIC_SCOUT_SYMBOLS) <= set(declared_functions())
+               _lib.STATIC_SCOUT_SYMBOLS + _lib.EXPORT_SYMBOLS) <= set(declared_functions())
     assert L.sdf_version().startswith(b"sdfmesh_b200")
 
 
