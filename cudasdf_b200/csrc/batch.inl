@@ -78,13 +78,13 @@ static BatchGrids batch_grids(long long blocks, const int ctas[4]) {
     BatchGrids G;
     G.own = capped_grid(k_field_own<false>, BLK_THREADS, blocks, 0, ctas[0]);
     G.miss = capped_grid(k_field_miss<false>, BLK_THREADS, 1LL << 30, 0, ctas[0]);
-    G.gather = capped_grid(k_field_gather, BLK_THREADS, blocks, 0, 0);
+    G.gather = capped_grid(k_field_gather, BLK_THREADS, (blocks + GATHER_WARPS - 1) / GATHER_WARPS, 0, 0);
     G.emit = capped_grid(k_mc_emit, BLK_THREADS, blocks, 0, ctas[1]);
     G.mark = capped_grid(k_dc_mark, BLK_THREADS, blocks, 0, ctas[0]);
     G.solve = capped_grid(k_dc_solve, SOLVE_THREADS, blocks, sizeof(SolveSmem), ctas[2]);
     G.quads = capped_grid(k_dc_quads, BLK_THREADS, blocks, sizeof(QuadSmem), ctas[3]);
     G.count_quads = (int)std::min<long long>(std::max(1LL, blocks), (long long)num_sms() * 4);
-    G.emit_cells = capped_grid(k_mc_emit_cells, 256, std::max(1LL, blocks * 2), 0, 0);
+    G.emit_cells = capped_grid(k_mc_emit_cells, EMIT_WARPS * 32, (blocks + EMIT_WARPS - 1) / EMIT_WARPS, 0, 0);
     return G;
 }
 
@@ -136,12 +136,13 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
                                                             &ctrl->tickets[4], diag);
         const bool flat = B.cell_words && !(m & (OUT_COLORS | OUT_UVS | OUT_PRIMIDS | OUT_NORMALS));
         k_field_gather<<<G.gather, BLK_THREADS, 0, st>>>(g0, av, B.fields, B.b2a, B.flags, B.block_totals, nullptr,
-                                                         &ctrl->tickets[3], flat ? B.cell_words : nullptr);
+                                                         flat ? B.cell_words : nullptr);
         k_exclusive_scan<<<std::max(1u, scan_tiles(nb)), SCAN_THREADS, 0, st>>>(
             B.block_totals, B.block_offsets, 0, &ctrl->active_count, 1, scan_state(B.scan(B.scanB_off)),
             &ctrl->total_vertices, diag);
         if (flat)
-            k_mc_emit_cells<<<G.emit_cells, 256, 0, st>>>(g0, av, B.fields, B.cell_words, B.block_offsets, mo, m);
+            k_mc_emit_cells<<<G.emit_cells, EMIT_WARPS * 32, 0, st>>>(g0, av, B.fields, B.cell_words, B.block_offsets,
+                                                                      mo, m);
         else
             k_mc_emit<<<G.emit, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, B.block_offsets, nullptr, nullptr, mo,
                                                       m, &ctrl->tickets[1], diag);
@@ -162,8 +163,7 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
         k_field_own<false><<<G.own, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, &ctrl->tickets[3], diag);
         k_field_miss<false><<<G.miss, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, B.miss, &ctrl->halo_misses,
                                                             &ctrl->tickets[4], diag);
-        k_field_gather<<<G.gather, BLK_THREADS, 0, st>>>(g0, av, B.fields, B.b2a, B.flags, nullptr, nullptr,
-                                                         &ctrl->tickets[5], nullptr);
+        k_field_gather<<<G.gather, BLK_THREADS, 0, st>>>(g0, av, B.fields, B.b2a, B.flags, nullptr, nullptr, nullptr);
         k_dc_mark<<<G.mark, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, D, &ctrl->tickets[0], diag, true);
         k_exclusive_scan<<<std::max(1u, scan_tiles(nb * 512u)), SCAN_THREADS, 0, st>>>(
             B.packet_counts, B.dc_voff, 0, &ctrl->active_count, 512, scan_state(B.scan(B.scanC_off)),

@@ -245,9 +245,9 @@ static sdf_status run_block_field(EngineImpl& E, const sdfb::SceneView& sv, floa
     k_field_miss<COUNT><<<persistent_grid(k_field_miss<COUNT>, BLK_THREADS, 1 << 30), BLK_THREADS, 0, st>>>(
         E.gv, sv, time, av, E.fields, E.miss, &ctrl->halo_misses, &ctrl->tickets[4], &ctrl->diag);
     check_launch();
-    k_field_gather<<<persistent_grid(k_field_gather, BLK_THREADS, E.nblocks), BLK_THREADS, 0, st>>>(
-        E.gv, av, E.fields, E.b2a, E.flags, (COUNT || !counts) ? nullptr : E.block_totals, packet_counts,
-        &ctrl->tickets[3], cell_words);
+    k_field_gather<<<persistent_grid(k_field_gather, BLK_THREADS, (E.nblocks + GATHER_WARPS - 1) / GATHER_WARPS),
+                     BLK_THREADS, 0, st>>>(E.gv, av, E.fields, E.b2a, E.flags,
+                                           (COUNT || !counts) ? nullptr : E.block_totals, packet_counts, cell_words);
     check_launch();
     return SDF_OK;
 }
@@ -688,7 +688,8 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
             k_weld_indices<<<persistent_grid(k_weld_indices, 256, nb * 2), 256, 0, st>>>(
                 gv, av, E.fields, E.cell_words, E.block_offsets, wb, mo.indices, mo.maxV);
         } else if (flat) {
-            k_mc_emit_cells<<<persistent_grid(k_mc_emit_cells, 256, nb * 2), 256, 0, st>>>(
+            k_mc_emit_cells<<<persistent_grid(k_mc_emit_cells, EMIT_WARPS * 32, (nb + EMIT_WARPS - 1) / EMIT_WARPS),
+                              EMIT_WARPS * 32, 0, st>>>(
                 gv, av, E.fields, E.cell_words, E.block_offsets, mo, mask);
         } else {
             k_mc_emit<<<persistent_grid(k_mc_emit, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(

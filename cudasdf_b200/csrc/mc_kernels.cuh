@@ -542,20 +542,42 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_miss(GridView g0, SceneVi
     }
 }
 
-__global__ void __launch_bounds__(BLK_THREADS) k_field_gather(GridView g0, ActiveView av, float* __restrict__ fields,
+// k_field_gather: one warp per active block (static stride over the active list), no CTA barriers,
+// so 64 blocks per SM are in flight instead of one per CTA. The warp stages the block's row in its own
+// shared memory and fetches the halo entries owned by active neighbours (their loads issued together
+// with the row's); with counts requested it classifies the 512 cells: case codes first, then the
+// triangle validity of the surface cells only (compacted, one cell per lane), then a warp scan in cell
+// order gives each cell's first vertex inside the block. The words and totals are those of
+// block_counts (countActiveBlockTriangles, MarchingCubesKernels.cu:914-970).
+constexpr int GATHER_WARPS = BLK_THREADS / 32;
+constexpr int HALO_PER_LANE = (HALO_N + 31) / 32;          // 7
+constexpr int ROW_VEC = FIELD_STRIDE / 4;                  // 184 float4 per row
+constexpr int ROW_VEC_PER_LANE = (ROW_VEC + 31) / 32;      // 6
+
+struct GatherWarpSmem {
+    float row[FIELD_STRIDE];          // the block's 9^3 row; reused for the 512 cell words at the end
+    unsigned char code[512];          // case code per cell (0 for cells outside the grid)
+    unsigned char vm[512];            // non-degenerate triangle mask per cell
+    unsigned short list[512];         // the block's surface cells (a case with triangles)
+};
+
+__global__ void __launch_bounds__(BLK_THREADS, 4) k_field_gather(GridView g0, ActiveView av, float* __restrict__ fields,
                                                             const int* __restrict__ block_to_active,
                                                             const unsigned* __restrict__ flags,
                                                             unsigned* __restrict__ block_totals,
-                                                            unsigned* __restrict__ packet_counts, unsigned* ticket,
+                                                            unsigned* __restrict__ packet_counts,
                                                             unsigned* __restrict__ cell_words = nullptr) {
-    __shared__ __align__(16) float s_field[FIELD_STRIDE];
-    __shared__ unsigned s_red[BLK_THREADS / 32];
-    __shared__ int s_item;
-    static_assert(HALO_N <= BLK_THREADS, "one halo sample per thread");
+    __shared__ __align__(16) GatherWarpSmem s_warp[GATHER_WARPS];
+    __shared__ unsigned long long s_cases[256];
+    const bool classify = block_totals || packet_counts || cell_words;  // dual contouring classifies itself
+    if (classify) {
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) s_cases[i] = c_mcCases[i];
+        __syncthreads();
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    GatherWarpSmem& W = s_warp[warp];
     const int n = active_count(av);
-    for (;;) {
-        const int a = claim(ticket, n, &s_item);
-        if (a < 0) break;
+    for (int a = blockIdx.x * GATHER_WARPS + warp; a < n; a += gridDim.x * GATHER_WARPS) {
         GridView g = g0;
         SceneView unused;
         int lin;
@@ -564,26 +586,110 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_gather(GridView g0, Activ
         int bx, by, bz;
         block_coord(g, lin, bx, by, bz);
         float* row = fields + (size_t)a * FIELD_STRIDE;
-        {
-            const float4* src = reinterpret_cast<const float4*>(row);
-            float4* dst = reinterpret_cast<float4*>(s_field);
-            for (int i = threadIdx.x; i < FIELD_STRIDE / 4; i += blockDim.x) dst[i] = src[i];
+#pragma unroll
+        for (int k = 0; k < ROW_VEC_PER_LANE; ++k) {
+            const int i = lane + 32 * k;
+            if (i < ROW_VEC) reinterpret_cast<float4*>(W.row)[i] = reinterpret_cast<const float4*>(row)[i];
         }
-        __syncthreads();  // the row is in place before the copied halo entries overwrite their slots
-        if (threadIdx.x < HALO_N) {
-            int hx, hy, hz;
-            halo_coord(threadIdx.x, hx, hy, hz);
-            const int olin = halo_owner(g, bx, by, bz, hx, hy, hz);
-            if (olin >= 0 && flags[bbase + olin]) {
-                const int b = block_to_active[bbase + olin];
-                const int h = (hz * 9 + hy) * 9 + hx;
-                const float v = fields[(size_t)b * FIELD_STRIDE + ((hz & 7) * 9 + (hy & 7)) * 9 + (hx & 7)];
-                s_field[h] = v;
-                row[h] = v;
+        // halo entries owned by active neighbours: flag -> owner's row -> value
+        int src[HALO_PER_LANE];
+#pragma unroll
+        for (int k = 0; k < HALO_PER_LANE; ++k) {
+            const int h = lane + 32 * k;
+            src[k] = -1;
+            if (h < HALO_N) {
+                int hx, hy, hz;
+                halo_coord(h, hx, hy, hz);
+                const int olin = halo_owner(g, bx, by, bz, hx, hy, hz);
+                if (olin >= 0 && flags[bbase + olin]) src[k] = olin;
             }
         }
-        if (block_totals || packet_counts || cell_words)  // dual contouring classifies the rows itself
-            block_counts(g, a, lin, s_field, s_red, nullptr, block_totals, packet_counts, cell_words);
+        float hv[HALO_PER_LANE];
+#pragma unroll
+        for (int k = 0; k < HALO_PER_LANE; ++k) {
+            if (src[k] < 0) continue;
+            int hx, hy, hz;
+            halo_coord(lane + 32 * k, hx, hy, hz);
+            const int b = block_to_active[bbase + src[k]];
+            hv[k] = fields[(size_t)b * FIELD_STRIDE + ((hz & 7) * 9 + (hy & 7)) * 9 + (hx & 7)];
+        }
+        __syncwarp();  // the row is in place before the copied halo entries overwrite their slots
+#pragma unroll
+        for (int k = 0; k < HALO_PER_LANE; ++k) {
+            if (src[k] < 0) continue;
+            int hx, hy, hz;
+            halo_coord(lane + 32 * k, hx, hy, hz);
+            const int h = (hz * 9 + hy) * 9 + hx;
+            W.row[h] = hv[k];
+            row[h] = hv[k];
+        }
+        __syncwarp();
+        if (!classify) continue;
+        // case codes of all cells; the surface cells listed
+        int nlist = 0;
+#pragma unroll 4
+        for (int j = 0; j < 16; ++j) {
+            const int tid = lane + 32 * j;
+            const CellInfo c = cell_info(g, bx, by, bz, tid);
+            int code = 0;
+            if (!c.oob) {
+                float cv[8];
+                code = cell_case(W.row, c.lx, c.ly, c.lz, cv);
+            }
+            const bool surf = (s_cases[code] & 0xF) != 0;
+            W.code[tid] = (unsigned char)code;
+            W.vm[tid] = 0;
+            const unsigned bal = __ballot_sync(0xffffffffu, surf);
+            if (surf) W.list[nlist + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)tid;
+            nlist += __popc(bal);
+        }
+        __syncwarp();
+        // triangle validity of the surface cells, one per lane
+        for (int i = lane; i < nlist; i += 32) {
+            const int tid = W.list[i];
+            const CellInfo c = cell_info(g, bx, by, bz, tid);
+            float cv[8];
+            const int code = cell_case(W.row, c.lx, c.ly, c.lz, cv);
+            W.vm[tid] = (unsigned char)cell_valid_mask(g, c.x, c.y, c.z, cv, s_cases[code]);
+        }
+        __syncwarp();
+        // cells 16 lane .. 16 lane + 15: counts, warp scan in cell order, words
+        const uint4 vm4 = reinterpret_cast<const uint4*>(W.vm)[lane];
+        const uint4 cd4 = reinterpret_cast<const uint4*>(W.code)[lane];
+        const unsigned vmw[4] = {vm4.x, vm4.y, vm4.z, vm4.w}, cdw[4] = {cd4.x, cd4.y, cd4.z, cd4.w};
+        // the vm bytes hold at most 5 bits each, so the popcount of a word is that of its four cells
+        const unsigned sum = 3u * (__popc(vmw[0]) + __popc(vmw[1]) + __popc(vmw[2]) + __popc(vmw[3]));
+        unsigned incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+        if (packet_counts) {
+            uint4* dst = reinterpret_cast<uint4*>(packet_counts + (size_t)a * 512 + 16 * lane);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                dst[q] = make_uint4(3u * __popc(vmw[q] & 0xFFu), 3u * __popc((vmw[q] >> 8) & 0xFFu),
+                                    3u * __popc((vmw[q] >> 16) & 0xFFu), 3u * __popc(vmw[q] >> 24));
+        }
+        if (cell_words) {
+            unsigned* words = reinterpret_cast<unsigned*>(W.row);  // the row is no longer read
+            unsigned pre = incl - sum;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const unsigned code = (cdw[j >> 2] >> (8 * (j & 3))) & 0xFFu;
+                const unsigned vm = (vmw[j >> 2] >> (8 * (j & 3))) & 0xFFu;
+                words[16 * lane + j] = code | (vm << 8) | (pre << 13);
+                pre += 3u * __popc(vm);
+            }
+            __syncwarp();
+            uint4* dst = reinterpret_cast<uint4*>(cell_words + (size_t)a * 512);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) dst[lane + 32 * q] = reinterpret_cast<const uint4*>(words)[lane + 32 * q];
+        }
+        if (block_totals && lane == 0) block_totals[a] = total;
+        __syncwarp();  // the warp's shared memory is free for the next block
     }
 }
 
@@ -607,53 +713,88 @@ __global__ void __launch_bounds__(256) k_fma_peak(float* out, int iters, float a
 
 // ------------------------------------------------------------------------------------------------
 // flat emission (generateActiveBlockTriangles, MarchingCubesKernels.cu:972-1110, positions and
-// identity indices only): one thread per cell of every active block, no block-wide steps. The cell's
-// case, its non-degenerate triangles and its first vertex inside the block come from the word the
-// gather kernel stored; most cells are empty and return after one load. The vertex order is the
-// block emission's: block offset, then cells in order, then the case's triangles in order.
+// identity indices only): one warp per active block (static stride over the active list). The warp
+// loads the block's 512 cell words (coalesced) into its shared memory, lists the cells that emit
+// (about 4 % of them), and each lane then takes one listed cell: its eight corner values from the
+// block's row, its case's non-degenerate triangles, written from the cell's first vertex. The words
+// come from the gather kernel; the vertex order is the block emission's: block offset, then cells in
+// order, then the case's triangles in order.
 // ------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_mc_emit_cells(GridView g0, ActiveView av, const float* __restrict__ fields,
-                                                       const unsigned* __restrict__ cell_words,
-                                                       const unsigned* __restrict__ block_offsets, MeshOut out,
-                                                       unsigned mask) {
+constexpr int EMIT_WARPS = 8;
+
+struct EmitWarpSmem {
+    unsigned words[512];
+    unsigned short list[512];
+};
+
+__global__ void __launch_bounds__(EMIT_WARPS * 32, 5) k_mc_emit_cells(GridView g0, ActiveView av,
+                                                                  const float* __restrict__ fields,
+                                                                  const unsigned* __restrict__ cell_words,
+                                                                  const unsigned* __restrict__ block_offsets,
+                                                                  MeshOut out, unsigned mask) {
     __shared__ unsigned long long s_cases[256];
+    __shared__ __align__(16) EmitWarpSmem s_warp[EMIT_WARPS];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) s_cases[i] = c_mcCases[i];
     __syncthreads();
-    const long long n = (long long)active_count(av) * 512;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const unsigned w = cell_words[i];
-        const unsigned vm = (w >> 8) & 31u;
-        if (!vm) continue;
-        const int a = (int)(i >> 9), tid = (int)(i & 511);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    EmitWarpSmem& W = s_warp[warp];
+    const int n = active_count(av);
+    for (int a = blockIdx.x * EMIT_WARPS + warp; a < n; a += gridDim.x * EMIT_WARPS) {
+        const uint4* src = reinterpret_cast<const uint4*>(cell_words + (size_t)a * 512);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) reinterpret_cast<uint4*>(W.words)[lane + 32 * q] = __ldcs(src + lane + 32 * q);
         GridView g = g0;
         SceneView unused;
         int lin;
         unsigned bbase;
         resolve(av, av.list[a], g, unused, lin, bbase);
+        const unsigned long long base = block_offsets[a];
+        int nlist = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint4 w4 = reinterpret_cast<const uint4*>(W.words)[lane + 32 * q];
+            const unsigned wq[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const bool emits = ((wq[r] >> 8) & 31u) != 0;
+                const unsigned bal = __ballot_sync(0xffffffffu, emits);
+                if (emits)
+                    W.list[nlist + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)(4 * (lane + 32 * q) + r);
+                nlist += __popc(bal);
+            }
+        }
+        __syncwarp();
         int bx, by, bz;
         block_coord(g, lin, bx, by, bz);
-        const CellInfo c = cell_info(g, bx, by, bz, tid);
         const float* f = fields + (size_t)a * FIELD_STRIDE;
-        float cv[8];
+        for (int i = lane; i < nlist; i += 32) {
+            const int tid = W.list[i];
+            const unsigned w = W.words[tid];
+            const unsigned vm = (w >> 8) & 31u;
+            const CellInfo c = cell_info(g, bx, by, bz, tid);
+            float cv[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) cv[k] = __ldg(f + fidx(c.lx + corner_dx(k), c.ly + corner_dy(k), c.lz + corner_dz(k)));
-        const unsigned long long word = s_cases[w & 255u];
-        unsigned long long v = (unsigned long long)block_offsets[a] + (w >> 13);
-        const int nt = (int)(word & 0xF);
-        for (int k = 0; k < nt; ++k) {
-            if (!((vm >> k) & 1u)) continue;
-            if (v + 2 >= out.maxV) break;  // the reference's capacity stop (:1020)
-            float3 p[3];
-            tri_points(g, c.x, c.y, c.z, cv, word, k, p);
+            for (int k = 0; k < 8; ++k)
+                cv[k] = __ldg(f + fidx(c.lx + corner_dx(k), c.ly + corner_dy(k), c.lz + corner_dz(k)));
+            const unsigned long long word = s_cases[w & 255u];
+            unsigned long long v = base + (w >> 13);
+            const int nt = (int)(word & 0xF);
+            for (int k = 0; k < nt; ++k) {
+                if (!((vm >> k) & 1u)) continue;
+                if (v + 2 >= out.maxV) break;  // the reference's capacity stop (:1020)
+                float3 p[3];
+                tri_points(g, c.x, c.y, c.z, cv, word, k, p);
 #pragma unroll
-            for (int j = 0; j < 3; ++j) out.verts[v + j] = make_float4(p[j].x, p[j].y, p[j].z, 1.f);
-            if ((mask & OUT_INDICES) && out.indices) {
-                out.indices[v] = (unsigned)v;
-                out.indices[v + 1] = (unsigned)v + 1;
-                out.indices[v + 2] = (unsigned)v + 2;
+                for (int j = 0; j < 3; ++j) out.verts[v + j] = make_float4(p[j].x, p[j].y, p[j].z, 1.f);
+                if ((mask & OUT_INDICES) && out.indices) {
+                    out.indices[v] = (unsigned)v;
+                    out.indices[v + 1] = (unsigned)v + 1;
+                    out.indices[v + 2] = (unsigned)v + 2;
+                }
+                v += 3;
             }
-            v += 3;
         }
+        __syncwarp();  // the warp's shared memory is free for the next block
     }
 }
 
