@@ -676,17 +676,19 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
             wb.base = E.weld_base;
             wb.flags = E.flags;
             wb.block_to_active = E.b2a;
-            const int wgrid = std::min(nb, num_sms() * 8);
-            k_weld_mark<<<wgrid, 256, 0, st>>>(gv, av, E.fields, wb);
+            const int wblocks = (nb + WELD_WARPS - 1) / WELD_WARPS;
+            k_weld_mark<<<persistent_grid(k_weld_mark, WELD_WARPS * 32, wblocks), WELD_WARPS * 32, 0, st>>>(gv, av,
+                                                                                                     E.fields, wb);
             check_launch();
             unsigned long long* scanD = reinterpret_cast<unsigned long long*>(E.ctrl_region + E.scanD_off);
             k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)nb)), SCAN_THREADS, 0, st>>>(
                 E.weld_totals, E.weld_base, 0, &ctrl->active_count, 1, scan_state(scanD), &ctrl->welded_vertices, diag);
             check_launch();
-            k_weld_vertices<<<wgrid, 256, 0, st>>>(gv, av, E.fields, wb, mo.verts, mo.maxV);
+            k_weld_vertices<<<persistent_grid(k_weld_vertices, WELD_WARPS * 32, wblocks), WELD_WARPS * 32, 0, st>>>(
+                gv, av, E.fields, wb, mo.verts, mo.maxV);
             check_launch();
-            k_weld_indices<<<persistent_grid(k_weld_indices, 256, nb * 2), 256, 0, st>>>(
-                gv, av, E.fields, E.cell_words, E.block_offsets, wb, mo.indices, mo.maxV);
+            k_weld_indices<<<persistent_grid(k_weld_indices, WELD_WARPS * 32, wblocks), WELD_WARPS * 32, 0, st>>>(
+                gv, av, E.cell_words, E.block_offsets, wb, mo.indices, mo.maxV);
         } else if (flat) {
             k_mc_emit_cells<<<persistent_grid(k_mc_emit_cells, EMIT_WARPS * 32, (nb + EMIT_WARPS - 1) / EMIT_WARPS),
                               EMIT_WARPS * 32, 0, st>>>(
