@@ -803,6 +803,7 @@ def main():
     if "e2e" in r:
         line["e2e"] = r["e2e"]
     line["roofline"] = roofline(r)
+    line["stage_roofline"] = stage_roofline(r) if spec["technique"] == 0 else None  # marching cubes stages
     if not args.no_cpu_baseline and world == 1:
         try:
             line["cpu_baseline"] = cpu_baseline(args)
@@ -840,6 +841,40 @@ def roofline(r):
                               "256^3 workload (profiles/k_field_own_mc_256prims_256.md), 2.23 KB per active block, "
                               "scaled by this run's active blocks",
             "work": c}
+
+
+# HBM copy bandwidth used as the denominator of the memory-bound stages
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    """(GB/s, source): the measured copy bandwidth of MEASURED_PEAKS.json when present, else the
+    fallback figure measured earlier on the same kind of GPU."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        v = float(d.get("hbm_gbs") or d["hbm"]["gbs"])
+        return v, "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback (6.65 TB/s; MEASURED_PEAKS.json absent)"
+
+
+def stage_roofline(r):
+    """Achieved HBM fraction of the memory-bound stages by their algorithmic bytes, A active blocks and
+    V vertices (one index per vertex): scan 8 B x A; emission reads the 4-byte cell word of each of the
+    512 A cells and writes 16 B (float4 position) + 4 B (index) per vertex. Classification and counting
+    run inside the block-field stage (the gather kernel, fused with the halo copy), so their time is
+    not separate here; the launch list under profiles/ gives it."""
+    st, stages = r["stats"], r["stages"]
+    a, v = st["active_blocks"], st["total_vertices"]
+    peak, source = hbm_peak()
+    out = {"peak": peak, "unit": "GB/s", "peak_source": source}
+    for name, ms, nbytes in (("scan", stages.get("ms_scan"), 8 * a),
+                             ("emission", stages.get("ms_emit"), 4 * 512 * a + 20 * v)):
+        if ms:
+            gbs = nbytes / (ms * 1e-3) / 1e9
+            out[name] = {"bytes": nbytes, "ms": ms, "achieved": gbs, "frac": gbs / peak}
+    return out
 
 
 if __name__ == "__main__":

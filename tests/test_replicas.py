@@ -51,3 +51,18 @@ def test_two_replicas_report_the_slowest_rank():
     ms_max, value = out[0]
     assert ms_max == 15.0
     assert abs(value - 2 * 1024.0 ** 3 / 15e-3 / 1e9) < 1e-9
+
+
+def test_stage_roofline_arithmetic():
+    """The memory-bound stages' fractions in the bench line: algorithmic bytes / stage time / peak."""
+    import bench
+    r = {"stats": {"active_blocks": 1000, "total_vertices": 30000},
+         "stages": {"ms_scan": 0.01, "ms_emit": 0.1, "ms_field": 1.0, "ms_scout": 0.1}}
+    out = bench.stage_roofline(r)
+    peak = out["peak"]
+    assert out["scan"]["bytes"] == 8000
+    assert abs(out["scan"]["achieved"] - 8000 / 1e-5 / 1e9) < 1e-9
+    assert out["emission"]["bytes"] == 4 * 512 * 1000 + 20 * 30000
+    assert abs(out["emission"]["frac"] - out["emission"]["achieved"] / peak) < 1e-12
+    untimed = bench.stage_roofline({"stats": r["stats"], "stages": {}})  # timing off: no stage entries
+    assert "scan" not in untimed and "emission" not in untimed and untimed["peak"] == peak
