@@ -543,12 +543,12 @@ __global__ void __launch_bounds__(BLK_THREADS) k_field_miss(GridView g0, SceneVi
 }
 
 // k_field_gather: one warp per active block (static stride over the active list), no CTA barriers,
-// so 64 blocks per SM are in flight instead of one per CTA. The warp stages the block's row in its own
-// shared memory and fetches the halo entries owned by active neighbours (their loads issued together
-// with the row's); with counts requested it classifies the 512 cells: case codes first, then the
-// triangle validity of the surface cells only (compacted, one cell per lane), then a warp scan in cell
-// order gives each cell's first vertex inside the block. The words and totals are those of
-// block_counts (countActiveBlockTriangles, MarchingCubesKernels.cu:914-970).
+// so 32 blocks per SM are in flight (four CTAs of eight warps) instead of one per CTA. The warp stages
+// the block's row in its own shared memory and fetches the halo entries owned by active neighbours
+// (their loads issued together with the row's); with counts requested it classifies the 512 cells:
+// case codes first, then the triangle validity of the surface cells only (compacted, one cell per
+// lane), then a warp scan in cell order gives each cell's first vertex inside the block. The words and
+// totals are those of block_counts (countActiveBlockTriangles, MarchingCubesKernels.cu:914-970).
 constexpr int GATHER_WARPS = BLK_THREADS / 32;
 constexpr int HALO_PER_LANE = (HALO_N + 31) / 32;          // 7
 constexpr int ROW_VEC = FIELD_STRIDE / 4;                  // 184 float4 per row

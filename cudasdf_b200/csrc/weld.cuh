@@ -73,7 +73,7 @@ __device__ __forceinline__ bool weld_owns(const GridView& g, int lin, int bx, in
 }
 
 // The three kernels below run one warp per active block (static stride over the active list): no
-// CTA barriers, up to 64 blocks per SM in flight.
+// CTA barriers, 32 to 64 blocks per SM in flight (as their registers allow).
 constexpr int WELD_WARPS = 8;
 
 // whether the edge of slot s (lower sample, axis) is crossed, from the block's row in shared memory
