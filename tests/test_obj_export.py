@@ -128,3 +128,19 @@ def test_extracted_mesh_exports_like_the_reference(tmp_path, welded):
     p = tmp_path / "mesh_export.obj"
     write_obj(p, v, indices=ix, uvs=uv)
     assert p.read_bytes() == OO.obj_text(p.name, v, uv, ix)
+
+
+def test_torch_tensors_and_shapes(tmp_path):
+    """write_obj takes torch tensors like numpy arrays, and refuses arrays of the wrong shape."""
+    _lib_or_skip()
+    import torch
+    from cudasdf_b200.export import write_obj
+    v, uv = _mesh(np.random.default_rng(5), 300)
+    ix = np.random.default_rng(6).integers(0, 300, 600).astype(np.uint32)
+    p = tmp_path / "torch.obj"
+    write_obj(p, torch.from_numpy(v), indices=torch.from_numpy(ix.view(np.int32)), uvs=torch.from_numpy(uv))
+    assert p.read_bytes() == OO.obj_text(p.name, v, uv, ix)
+    with pytest.raises(ValueError):
+        write_obj(tmp_path / "bad.obj", v[:, :3])
+    with pytest.raises(ValueError):
+        write_obj(tmp_path / "bad.obj", v, uvs=uv[:10])
