@@ -1,7 +1,7 @@
 // Dual-contouring stages for sm_100a (MarchingCubesKernels.cu:1112-2044).
 //
-// Same decomposition as marching cubes: one CTA per active block at a time, the block's 9^3 field
-// in shared memory. The per-cell map() work of the reference (4 evaluations per Hermite point for
+// The mark, solve and quad stages run one CTA per active block at a time, with the block's 9^3 field
+// (from the shared-halo block field of marching cubes) in shared memory. The per-cell map() work of the reference (4 evaluations per Hermite point for
 // its normal, 4 at the solved vertex, 4 + 1 per quad, 24 per quad for output normals) is irregular,
 // so it is first compacted into per-block lists in shared memory and then evaluated 32 points per
 // warp-coherent call. Every arithmetic step follows the reference's order (see sdf_device.cuh).
