@@ -69,3 +69,53 @@ def test_header_compiles_as_c():
         assert out.returncode == 0
         sizes = [int(x) for x in out.stdout.split()]
         assert sizes == [ctypes.sizeof(t) for t in structs.values()], dict(zip(structs, sizes))
+
+
+def test_c_host_links_and_writes_obj():
+    """A C program links the library and calls it through the header alone: the version string and
+    the OBJ writer (host memory only, so no GPU is needed); the file matches the restatement of the
+    reference's writer."""
+    import subprocess
+    import tempfile
+
+    import numpy as np
+
+    from cudasdf_b200 import _lib
+    from oracle import obj_oracle
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libsdfmesh_b200.so not built")
+    src = r'''
+#include <stdio.h>
+#include <string.h>
+#include "sdfmesh_b200.h"
+int main(int argc, char** argv) {
+    sdf_float4 v[6];
+    sdf_float2 uv[6];
+    for (int i = 0; i < 6; ++i) {
+        v[i].x = 0.125f * i; v[i].y = -1.5f + i; v[i].z = 1e-5f * (i + 1); v[i].w = 1.f;
+        uv[i].x = 0.1f * i; uv[i].y = 1.f - 0.1f * i;
+    }
+    const uint32_t idx[6] = {0, 1, 2, 2, 1, 5};
+    if (strncmp(sdf_version(), "sdfmesh_b200", 12) != 0) return 2;
+    if (sdf_write_obj(argv[1], v, 6, NULL, 0, uv) != SDF_OK) return 3;
+    if (sdf_write_obj(argv[2], v, 6, idx, 6, NULL) != SDF_OK) return 4;
+    if (sdf_write_obj(argv[2], v, 5, idx, 6, NULL) != SDF_ERR_INVALID) return 5;  /* index 5 of 5 vertices */
+    return 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        c, exe = os.path.join(d, "host.c"), os.path.join(d, "host")
+        open(c, "w").write(src)
+        libdir = os.path.dirname(_lib.LIB_PATH)
+        r = subprocess.run(["/usr/bin/gcc", "-std=c11", "-Wall", "-I", os.path.dirname(HEADER), c, "-o", exe,
+                            "-L", libdir, "-lsdfmesh_b200", "-Wl,-rpath," + libdir], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        soup, indexed = os.path.join(d, "soup.obj"), os.path.join(d, "indexed.obj")
+        out = subprocess.run([exe, soup, indexed], capture_output=True, text=True)
+        assert out.returncode == 0, (out.returncode, out.stderr)
+        i = np.arange(6, dtype=np.float32)
+        v = np.stack([np.float32(0.125) * i, np.float32(-1.5) + i, np.float32(1e-5) * (i + 1), np.ones(6, np.float32)], 1)
+        uv = np.stack([np.float32(0.1) * i, np.float32(1.0) - np.float32(0.1) * i], 1)
+        assert open(soup, "rb").read() == obj_oracle.obj_text("soup.obj", v, uv)
+        assert open(indexed, "rb").read() == obj_oracle.obj_text("indexed.obj", v, None,
+                                                                np.array([0, 1, 2, 2, 1, 5], np.uint32))
