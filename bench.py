@@ -40,6 +40,9 @@ CONFIGS = {
     "c3": {"config": 3, "technique": 1, "workload": "dc_masspoint_4096prims_512",
            "dc": {"dc_solver": 1, "projection_iters": 3, "adaptive_diagonal": 1, "cond_threshold": 1e4}},
     "c4": {"config": 4, "technique": 0, "workload": "mc_16384prims_1024", "surrogate": True},
+    # the 16,384-primitive scene of c4 on a 256^3 grid, surrogate on: a case small enough for captures of
+    # the surrogate's tensor-core kernels and of the memory-bound stages
+    "c4s": {"config": 4, "technique": 0, "workload": "mc_16384prims_256", "surrogate": True, "res": 256},
     # the 256^3 scene with the dual-contouring options of c3: a case small enough for kernel captures
     "c3s": {"config": 2, "technique": 1, "workload": "dc_masspoint_256prims_256",
             "dc": {"dc_solver": 1, "projection_iters": 3, "adaptive_diagonal": 1, "cond_threshold": 1e4}},
@@ -206,7 +209,7 @@ def run_ours(args, rank, world):
 
     spec = CONFIGS[args.config]
     cfg_id, tech = spec["config"], spec["technique"]
-    res = S.config_resolution(cfg_id)
+    res = spec.get("res") or S.config_resolution(cfg_id)
     cell = S.cell_size_for(res)
     prims = S.config_scene(cfg_id)
     mask = L.OUT_INDICES
@@ -557,95 +560,74 @@ def count_work(eng, buf, res):
             "lane_efficiency_leaves": int(c[1]) / max(32 * int(c[6]), 1)}
 
 
+def cpu_full_extraction(cfg_id, res, cores):
+    """One whole extraction of the workload by the CPU restatement of the reference's algorithm
+    (oracle/sdf_oracle.c: scout of every block, then the block field, cases, counts, scan and vertex
+    and index emission of every active block), OpenMP over `cores` host threads. Returns
+    (seconds, active blocks, vertices)."""
+    from cudasdf_b200 import scenes as S
+    from oracle import oracle as O
+    sc = O.Scene(S.config_scene(cfg_id))
+    g = O.make_grid(S.cell_size_for(res))
+    t0 = time.perf_counter()
+    out = O.run(sc, g, 0.0, 0, 1.0, O.OR_INDICES, max_vertices=200_000_000, nthreads=cores)
+    return time.perf_counter() - t0, out["nActive"], out["totalVertices"]
+
+
 def cpu_baseline(args):
-    """The CPU oracle (the reference's algorithm restated in C, OpenMP over all host threads) on a
-    bounded sample of the same workload: a slice of the scout plus a sample of the active blocks."""
+    """The CPU oracle (the reference's algorithm restated in C, OpenMP over all host threads): one whole
+    extraction of the same workload, timed; the one-thread figure is a sample (a slice of the scout and
+    a sample of the active blocks' marching cubes) scaled to the grid."""
     import numpy as np
 
     from cudasdf_b200 import scenes as S
     from oracle import oracle as O
     spec = CONFIGS[args.config]
     cfg_id = spec["config"]
-    res = S.config_resolution(cfg_id)
-    prims = S.config_scene(cfg_id)
-    sc = O.Scene(prims)
+    res = spec.get("res") or S.config_resolution(cfg_id)
+    cores = os.cpu_count() or 1
+    secs, nact, nverts = cpu_full_extraction(cfg_id, res, cores)
+    # one thread, on a sample
+    sc = O.Scene(S.config_scene(cfg_id))
     g = O.make_grid(S.cell_size_for(res))
     nblocks = g.bx * g.by * g.bz
-    cores = os.cpu_count() or 1
-    # scout: a contiguous slice of blocks, all host threads
-    scout_n = min(nblocks, 262144)
+    scout_n = min(nblocks, 16384)
     t0 = time.perf_counter()
-    O.scout_range(sc, g, 0, scout_n, 0.0, cores)
-    t_scout = (time.perf_counter() - t0) / scout_n * nblocks
-    # active-block count of the full grid: the reference run's digest when present, else the oracle
-    gold = os.path.join(ROOT, "tests", "golden", f"full_mc_c{cfg_id}.npz")
-    if os.path.exists(gold):
-        nact = len(np.load(gold)["block_totals"])
-    else:
-        nact = int(O.scout_range(sc, g, 0, nblocks, 0.0, cores))
-    # marching cubes over a sample of active blocks drawn uniformly from the volume, scaled
+    O.scout_range(sc, g, 0, scout_n, 0.0, 1)
+    t1_scout = (time.perf_counter() - t0) / scout_n * nblocks
     rng = np.random.default_rng(0)
     cand = rng.choice(nblocks, size=min(nblocks, 262144), replace=False).astype(np.int32)
     flags = O.scout_flags(sc, g, cand, 0.0, cores)
-    sample = cand[flags][:2048]
+    sample = cand[flags][:128]
     t0 = time.perf_counter()
-    O.mc_blocks(sc, g, sample, 0.0, cores)
-    t_mc = (time.perf_counter() - t0) / max(len(sample), 1) * nact
-    total = t_scout + t_mc
-    # the same on one thread, on a sixteenth of the sample
-    t0 = time.perf_counter()
-    O.scout_range(sc, g, 0, max(scout_n // 16, 1), 0.0, 1)
-    t1_scout = (time.perf_counter() - t0) / max(scout_n // 16, 1) * nblocks
-    sample1 = sample[:max(len(sample) // 16, 1)]
-    t0 = time.perf_counter()
-    O.mc_blocks(sc, g, sample1, 0.0, 1)
-    t1_mc = (time.perf_counter() - t0) / max(len(sample1), 1) * nact
-    return {"value": float(res) ** 3 / total / 1e9, "unit": "Gvoxels/s", "cores": cores, "kind": "port",
+    O.mc_blocks(sc, g, sample, 0.0, 1)
+    t1_mc = (time.perf_counter() - t0) / max(len(sample), 1) * nact
+    return {"value": float(res) ** 3 / secs / 1e9, "unit": "Gvoxels/s", "cores": cores, "kind": "port",
+            "seconds": secs, "vertices": nverts,
             "value_1thread": float(res) ** 3 / (t1_scout + t1_mc) / 1e9,
-            "sample": f"scout of {scout_n} of {nblocks} blocks + marching cubes of {len(sample)} of {nact} active "
-                      f"blocks, scaled to the full {res}^3 extraction ({total:.1f} s estimated)"}
+            "sample": f"one whole {res}^3 extraction ({nblocks} blocks scouted, {nact} active blocks meshed, "
+                      f"{nverts} vertices) in {secs:.1f} s on {cores} threads; value_1thread: a scout slice of "
+                      f"{scout_n} blocks + marching cubes of {len(sample)} active blocks on one thread, scaled"}
 
 
 def run_reference_cpu(args):
     """The reference arm on the host cores: the reference's algorithm (restated in oracle/sdf_oracle.c,
-    OpenMP over all host threads) on a bounded sample of the workload per step - a slice of the
-    scout and a sample of the active blocks' marching cubes, each scaled to the whole grid."""
-    import numpy as np
-
+    OpenMP over all host threads); every step, warm-up and timed, is one whole extraction of the
+    workload (the scout of every block and the marching cubes of every active block)."""
     from cudasdf_b200 import scenes as S
-    from oracle import oracle as O
     spec = CONFIGS[args.config]
     cfg_id = spec["config"]
-    res = S.config_resolution(cfg_id)
-    sc = O.Scene(S.config_scene(cfg_id))
-    g = O.make_grid(S.cell_size_for(res))
-    nblocks = g.bx * g.by * g.bz
+    res = spec.get("res") or S.config_resolution(cfg_id)
     cores = os.cpu_count() or 1
-    gold = os.path.join(ROOT, "tests", "golden", f"full_mc_c{cfg_id}.npz")
-    if os.path.exists(gold):
-        active = np.sort(np.load(gold)["active"]).astype(np.int32)
-    else:
-        flags = O.scout_flags(sc, g, np.arange(nblocks, dtype=np.int32), 0.0, cores)
-        active = np.nonzero(flags)[0].astype(np.int32)
-    scout_n = min(nblocks, 32768)
-    mc_n = min(len(active), 256)
-    rng = np.random.default_rng(0)
-    values = []
+    times = []
+    nact = nverts = 0
     for step in range(args.warmup + args.steps):
-        b0 = (step * scout_n) % max(nblocks - scout_n + 1, 1)
-        t0 = time.perf_counter()
-        O.scout_range(sc, g, b0, b0 + scout_n, 0.0, cores)
-        t_scout = (time.perf_counter() - t0) / scout_n * nblocks
-        sample = rng.choice(active, size=mc_n, replace=False) if mc_n else active
-        t0 = time.perf_counter()
-        O.mc_blocks(sc, g, np.sort(sample), 0.0, cores)
-        t_mc = (time.perf_counter() - t0) / max(mc_n, 1) * len(active)
+        secs, nact, nverts = cpu_full_extraction(cfg_id, res, cores)
         if step >= args.warmup:
-            values.append(float(res) ** 3 / (t_scout + t_mc) / 1e9)
-    v = sum(values) / len(values)
-    return {"value": v, "ms": float(res) ** 3 / (v * 1e9) * 1e3, "cores": cores, "res": res,
-            "sample": f"per step: scout of {scout_n} of {nblocks} blocks + marching cubes of {mc_n} of {len(active)} "
-                      f"active blocks, each scaled to the full {res}^3 extraction"}
+            times.append(secs)
+    ms = sum(times) / len(times) * 1e3
+    return {"value": float(res) ** 3 / (ms * 1e-3) / 1e9, "ms": ms, "cores": cores, "res": res,
+            "sample": f"every step one whole {res}^3 extraction: {nact} active blocks, {nverts} vertices"}
 
 
 def run_reference_batch(args):
@@ -724,7 +706,7 @@ def main():
         line.update({"impl": "reference", "value": r["value"], "ms_per_step": r["ms"],
                      "config": {"workload": spec["workload"], "grid": r["res"], "primitives": nprims,
                                 "outputs": "VBO float4 + EBO uint32", "parallelism": f"{r['cores']} host threads",
-                                "path": "the reference's algorithm (plain exact marching cubes) restated in C, "
+                                "path": "plain exact marching cubes: the reference's algorithm restated in C, "
                                         "OpenMP; the reference's own path is CUDA only (see --impl reference-cuda)"},
                      "cpu_baseline": {"value": r["value"], "unit": "Gvoxels/s", "cores": r["cores"], "kind": "port",
                                       "sample": r["sample"]},
@@ -779,7 +761,8 @@ def main():
     st = r["stats"]
     line = dict(base)
     line.update({"value": r["value"], "ms_per_step": r["ms"],
-                 "config": {"workload": spec["workload"] + ("_surrogate_culled" if "surrogate" in r else ""),
+                 "config": {"workload": spec["workload"],
+                            "path": "surrogate-culled exact marching cubes" if "surrogate" in r else "plain exact",
                             "grid": r["res"], "primitives": r["nprims"], "outputs": "VBO float4 + EBO uint32",
                             "active_blocks": st["active_blocks"], "vertices": st["total_vertices"],
                             "scouted_blocks": st["scouted_blocks"], "parallelism": f"replicas x{world}",
@@ -837,9 +820,9 @@ def roofline(r):
             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": "measured by the library's FMA loop on this GPU (no FP32 figure in MEASURED_PEAKS.json)",
             "traffic": TRAFFIC_PER_ACTIVE_BLOCK * active,
-            "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one k_field_own capture on the "
-                              "256^3 workload (profiles/k_field_own_mc_256prims_256.md), 2.23 KB per active block, "
-                              "scaled by this run's active blocks",
+            "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of k_field_own on "
+                              "the 256^3, 256-primitive workload, 2.23 KB per active block, scaled by this run's "
+                              "active blocks",
             "work": c}
 
 
@@ -864,7 +847,7 @@ def stage_roofline(r):
     V vertices (one index per vertex): scan 8 B x A; emission reads the 4-byte cell word of each of the
     512 A cells and writes 16 B (float4 position) + 4 B (index) per vertex. Classification and counting
     run inside the block-field stage (the gather kernel, fused with the halo copy), so their time is
-    not separate here; the launch list under profiles/ gives it."""
+    not separate here; an ncu launch list of the same command gives the gather kernel's own time."""
     st, stages = r["stats"], r["stages"]
     a, v = st["active_blocks"], st["total_vertices"]
     peak, source = hbm_peak()

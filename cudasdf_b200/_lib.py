@@ -107,7 +107,8 @@ SURROGATE_SYMBOLS = ["sdf_surrogate_default_config", "sdf_surrogate_train", "sdf
                      "sdf_surrogate_get_params", "sdf_surrogate_forward", "sdf_surrogate_gradient"]
 BATCH_SYMBOLS = ["sdf_batch_create", "sdf_batch_destroy", "sdf_batch_set_scenes", "sdf_batch_extract",
                  "sdf_batch_capture"]
-STATIC_SCOUT_SYMBOLS = ["sdf_scout_active_blocks_static", "sdf_scout_static_max_blocks"]
+STATIC_SCOUT_SYMBOLS = ["sdf_scout_active_blocks_static"]
+SCOUT_STATIC_MAX_BLOCKS = 1 << 20  # SDF_SCOUT_STATIC_MAX_BLOCKS of the header
 EXPORT_SYMBOLS = ["sdf_write_obj"]
 ENGINE_SYMBOLS = ["sdf_engine_create", "sdf_engine_destroy", "sdf_engine_configure", "sdf_engine_set_scene",
                   "sdf_engine_set_scene_device",
@@ -213,7 +214,6 @@ def lib():
     L.sdf_batch_capture.restype = i
     L.sdf_scout_active_blocks_static.argtypes = [G, f]
     L.sdf_scout_active_blocks_static.restype = i
-    L.sdf_scout_static_max_blocks.restype = u
     L.sdf_write_obj.argtypes = [ctypes.c_char_p, vp, ctypes.c_uint64, vp, ctypes.c_uint64, vp]
     L.sdf_write_obj.restype = i
     L.sdf_last_error.restype = i

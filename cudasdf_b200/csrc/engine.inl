@@ -620,8 +620,8 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
     const bool culled = E.sur && E.sur->enabled;
     if (culled)
         run_culled_scout_compact(E, sv, time, scanA, ctrl, st);
-    else
-        run_scout_compact(gv, sv, time, E.flags, scanA, E.list, &ctrl->active_count, diag, st);
+    else if (run_scout_compact(gv, sv, time, E.flags, scanA, E.list, &ctrl->active_count, diag, st) != cudaSuccess)
+        return SDF_ERR_CUDA;
     if (E.timing) cudaEventRecord(E.ev[1], st);
     ActiveView av{E.list, &ctrl->active_count, nb};
     MeshOut mo;
@@ -945,7 +945,8 @@ sdf_status sdf_engine_count_work(sdf_engine* e, unsigned long long out[8]) {
     sv.nprims = E.nprims;
     sv.nbvh = E.nbvh;
     sv.nnodes = E.nnodes;
-    run_scout_compact(E.gv, sv, 0.f, E.flags, scanA, E.list, &ctrl->active_count, &ctrl->diag, 0);
+    if (run_scout_compact(E.gv, sv, 0.f, E.flags, scanA, E.list, &ctrl->active_count, &ctrl->diag, 0) != cudaSuccess)
+        return SDF_ERR_CUDA;
     record(cudaMemsetAsync(&ctrl->diag, 0, sizeof(Diag), 0));
     ActiveView av{E.list, &ctrl->active_count, E.nblocks};
     // the engine's block-field stage (own samples, then the halos no active block owns) with counters on

@@ -55,7 +55,9 @@ def decode_word(w):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    # the reference checkout: the first argument, else $CUDASDF_REFERENCE, else "reference" beside the repository
+    ref_root = (sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CUDASDF_REFERENCE")
+                or os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(HERE))), "reference"))
     cases = read_reference_tables(ref_root)
     words = [encode_word(e) for e in cases]
     assert [decode_word(w) for w in words] == cases

@@ -13,7 +13,10 @@
 //    SDF_ERR_CAPACITY before anything is launched.
 //  * Each device that loads the library keeps the array (a little over 4 MiB) until the process exits.
 //  * The first call on a device looks the array up for that device (cudaGetSymbolAddress, with that
-//    device current); make that first call before any stream capture on that device.
+//    device current); make that first call before any stream capture on that device. The address is
+//    kept for the life of the process: after cudaDeviceReset on a device the module is loaded again
+//    and the kept address is stale, so this entry point must not be called on that device again in
+//    the same process (the library's other device memory, like every caller's, is gone too).
 //  * All calls share the one array and it keeps the last call's contents; each call clears the parts
 //    that must start at zero. Calls whose work overlaps on the GPU (two streams, two host threads
 //    without ordering) race on the array: order them.
@@ -21,7 +24,8 @@
 
 namespace sdfb {
 
-constexpr unsigned kStaticScoutMaxBlocks = 1u << 20;  // 1,048,576 8^3 blocks, e.g. a 1024 x 1024 x 512 grid
+constexpr unsigned kStaticScoutMaxBlocks = SDF_SCOUT_STATIC_MAX_BLOCKS;  // 1,048,576 8^3 blocks, e.g. 1024 x 1024 x 512
+static_assert(kStaticScoutMaxBlocks == (1u << 20), "the header's stated limit");
 constexpr unsigned kStaticScoutTiles = (kStaticScoutMaxBlocks + SCAN_TILE - 1) / SCAN_TILE;
 constexpr size_t kStaticStatusBytes = (size_t)(kStaticScoutTiles + 1) * sizeof(unsigned long long);
 constexpr size_t kStaticDiagOffset = (kStaticStatusBytes + 255) & ~size_t(255);
@@ -69,14 +73,9 @@ extern "C" sdf_status sdf_scout_active_blocks_static(sdf_grid* grid, float time)
         record(e);
         return SDF_ERR_CUDA;
     }
-    run_scout_compact(grid_view(*grid), scene_view(*grid), time, flags, status, grid->d_activeBlocks,
-                      grid->d_activeBlockCount, diag, 0);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) {
-        record(e);
-        return SDF_ERR_CUDA;
-    }
-    return SDF_OK;
+    // run_scout_compact reports the first error of its two launches and its memset (a refused launch
+    // leaves the active list and count unwritten)
+    e = run_scout_compact(grid_view(*grid), scene_view(*grid), time, flags, status, grid->d_activeBlocks,
+                          grid->d_activeBlockCount, diag, 0);
+    return e == cudaSuccess ? SDF_OK : SDF_ERR_CUDA;
 }
-
-extern "C" unsigned int sdf_scout_static_max_blocks(void) { return sdfb::kStaticScoutMaxBlocks; }

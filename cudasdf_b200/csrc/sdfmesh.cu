@@ -33,12 +33,13 @@ static void record(cudaError_t e) {
     if (e != cudaSuccess && g_last_error == 0) g_last_error = (int)e;
 }
 static unsigned g_launch_failures = 0;  // launches refused so far (an enqueue compares before / after)
-static void check_launch() {
+static cudaError_t check_launch() {
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         record(e);
         ++g_launch_failures;
     }
+    return e;
 }
 
 static int num_sms() {
@@ -153,19 +154,24 @@ static ScanState scan_state(unsigned long long* region) {
     return st;
 }
 
-static void run_scout_compact(const GridView& gv, const SceneView& sv, float time, unsigned* flags,
-                              unsigned long long* status, int* list, int* count, Diag* diag, cudaStream_t stream) {
+// Returns the first error of its two launches and its memset (each is also recorded).
+static cudaError_t run_scout_compact(const GridView& gv, const SceneView& sv, float time, unsigned* flags,
+                                     unsigned long long* status, int* list, int* count, Diag* diag,
+                                     cudaStream_t stream) {
     const int nblocks = gv.bx * gv.by * gv.bz;
     const int nbricks = ((gv.bx + 3) / 4) * ((gv.by + 3) / 4) * ((gv.bz + 1) / 2);
     const int warps_per_cta = BLK_THREADS / 32;
     k_scout_t<false><<<(nbricks + warps_per_cta - 1) / warps_per_cta, BLK_THREADS, 0, stream>>>(gv, sv, time, flags, diag,
                                                                                           nullptr, 0.f);
-    check_launch();
+    cudaError_t err = check_launch();
     const unsigned tiles = scan_tiles((unsigned)nblocks);
-    record(cudaMemsetAsync(status, 0, (tiles + 1) * sizeof(unsigned long long), stream));
+    const cudaError_t em = cudaMemsetAsync(status, 0, (tiles + 1) * sizeof(unsigned long long), stream);
+    record(em);
+    if (err == cudaSuccess) err = em;
     k_compact<<<std::max(1u, tiles), SCAN_THREADS, 0, stream>>>(flags, (unsigned)nblocks, list, count,
                                                                 scan_state(status), diag);
-    check_launch();
+    const cudaError_t ec = check_launch();
+    return err != cudaSuccess ? err : ec;
 }
 
 }  // namespace sdfb

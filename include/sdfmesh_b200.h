@@ -312,12 +312,15 @@ sdf_status sdf_extract(const sdf_primitive* prims, int count, const sdf_config* 
  * synchronise the device and can fail under the host's fixed memory budget), or an application that
  * owns every allocation through its own allocator. Its working memory is one static device array of
  * the library (a little over 4 MiB, held by every device that loads the library until exit).
- * Limit: sdf_scout_static_max_blocks() 8^3 blocks (1,048,576); larger grids return SDF_ERR_CAPACITY.
- * The first call on a device looks up the array's device address with that device current; make it
- * before any stream capture there. Calls share the array: calls that overlap on the GPU race.
- * Runs on the legacy default stream, like launchScoutActiveBlocks; same outputs. */
+ * Limit: SDF_SCOUT_STATIC_MAX_BLOCKS 8^3 blocks (1,048,576); larger grids return SDF_ERR_CAPACITY
+ * and launch nothing. The first call on a device looks up the array's device address with that
+ * device current; make it before any stream capture there. The address is kept for the process's
+ * life: after cudaDeviceReset on a device, do not call this entry point there again. Calls share the
+ * array and each clears what must start at zero; calls that overlap on the GPU race. A refused launch
+ * or memset returns SDF_ERR_CUDA. Runs on the legacy default stream, like launchScoutActiveBlocks;
+ * same outputs. */
+#define SDF_SCOUT_STATIC_MAX_BLOCKS 1048576u
 sdf_status sdf_scout_active_blocks_static(sdf_grid* grid, float time);
-unsigned int sdf_scout_static_max_blocks(void);
 
 /* ---------------------------------------------------------------------------------------------
  * Learned surrogate culling (no counterpart in the reference). A Fourier-feature MLP

@@ -8,7 +8,9 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE_ROOT = "/root/reference"
+# the reference checkout (read at test time only where present): $CUDASDF_REFERENCE, else a directory
+# named "reference" beside the repository
+REFERENCE_ROOT = os.environ.get("CUDASDF_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
 
 
 def pytest_configure(config):

@@ -314,7 +314,7 @@ def mixed_scene_notrig(seed, n):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", required=True, help="directory for the fixture files")
     ap.add_argument("--skip-full", action="store_true", help="skip the full-size digests")
     ap.add_argument("--only-odd", action="store_true", help="only the non-power-of-two grid fixtures")
     ap.add_argument("--only-types", action="store_true", help="only the per-primitive-type fixtures")

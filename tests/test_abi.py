@@ -119,3 +119,23 @@ int main(int argc, char** argv) {
         assert open(soup, "rb").read() == obj_oracle.obj_text("soup.obj", v, uv)
         assert open(indexed, "rb").read() == obj_oracle.obj_text("indexed.obj", v, None,
                                                                 np.array([0, 1, 2, 2, 1, 5], np.uint32))
+
+
+def test_static_scout_limit_and_error_status_without_a_device():
+    """The header states the allocation-free scout's limit, and without a usable CUDA device the entry
+    point reports SDF_ERR_CUDA (never SDF_OK with its outputs unwritten)."""
+    from conftest import cuda_available
+    from cudasdf_b200 import _lib
+    text = open(HEADER).read()
+    m = re.search(r"#define\s+SDF_SCOUT_STATIC_MAX_BLOCKS\s+(\d+)u", text)
+    assert m and int(m.group(1)) == _lib.SCOUT_STATIC_MAX_BLOCKS
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libsdfmesh_b200.so not built")
+    if cuda_available():
+        pytest.skip("a CUDA device is present: the GPU tests cover the call")
+    L = _lib.lib()
+    grid = _lib.SdfGrid()
+    grid.blocksDim[0], grid.blocksDim[1], grid.blocksDim[2] = 4, 4, 4
+    grid.d_activeBlocks = 1  # never dereferenced on the host
+    grid.d_activeBlockCount = 1
+    assert L.sdf_scout_active_blocks_static(ctypes.byref(grid), 0.0) == _lib.SDF_ERR_CUDA

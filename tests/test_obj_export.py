@@ -144,3 +144,70 @@ def test_torch_tensors_and_shapes(tmp_path):
         write_obj(tmp_path / "bad.obj", v[:, :3])
     with pytest.raises(ValueError):
         write_obj(tmp_path / "bad.obj", v, uvs=uv[:10])
+
+
+def _comma_decimal_locale(d):
+    """Builds a locale whose LC_NUMERIC decimal point is ',' under directory d (for LOCPATH), from a
+    generated ASCII charmap; None when localedef is missing or fails."""
+    localedef = shutil.which("localedef")
+    if localedef is None:
+        return None
+    cm = os.path.join(d, "ascii.cm")
+    with open(cm, "w") as f:
+        f.write("<code_set_name> ASCII_TEST\n<mb_cur_max> 1\n<mb_cur_min> 1\nCHARMAP\n")
+        f.writelines(f"<U{i:04X}> /x{i:02x} CHAR{i}\n" for i in range(128))
+        f.write("END CHARMAP\n")
+    src = os.path.join(d, "comma.def")
+    with open(src, "w") as f:
+        f.write('LC_NUMERIC\ndecimal_point ","\nthousands_sep ""\ngrouping -1\nEND LC_NUMERIC\n')
+    subprocess.run([localedef, "-c", "-f", cm, "-i", src, os.path.join(d, "comma_decimal")],
+                   capture_output=True)
+    return "comma_decimal" if os.path.isdir(os.path.join(d, "comma_decimal")) else None
+
+
+def test_comma_decimal_locale_does_not_change_the_file():
+    """A host application that switched the process to a comma-decimal locale (setlocale(LC_ALL, ...))
+    still gets the reference's bytes: the writer's number formatting ignores LC_NUMERIC."""
+    import tempfile
+    L = _lib_or_skip()
+    gcc = shutil.which("gcc") or "/usr/bin/gcc"
+    with tempfile.TemporaryDirectory() as d:
+        name = _comma_decimal_locale(d)
+        if name is None:
+            pytest.skip("no way to build a comma-decimal locale here")
+        src = r'''
+#include <locale.h>
+#include <stdio.h>
+#include <string.h>
+#include "sdfmesh_b200.h"
+int main(int argc, char** argv) {
+    if (!setlocale(LC_ALL, argv[2])) return 2;
+    char probe[32];
+    snprintf(probe, sizeof probe, "%g", 0.5);
+    if (strcmp(probe, "0,5") != 0) return 3;  /* the locale is in force for printf */
+    sdf_float4 v[6];
+    sdf_float2 uv[6];
+    for (int i = 0; i < 6; ++i) {
+        v[i].x = 0.125f * i - 0.5f; v[i].y = 1.5f + i; v[i].z = 1e-5f * (i + 1); v[i].w = 1.f;
+        uv[i].x = 0.1f * i; uv[i].y = 1.f - 0.25f * i;
+    }
+    return sdf_write_obj(argv[1], v, 6, NULL, 0, uv) == SDF_OK ? 0 : 4;
+}
+'''
+        c, exe = os.path.join(d, "host.c"), os.path.join(d, "host")
+        open(c, "w").write(src)
+        libdir = os.path.dirname(L.LIB_PATH)
+        inc = os.path.join(os.path.dirname(libdir), "include")
+        r = subprocess.run([gcc, "-std=c11", "-Wall", "-I", inc, c, "-o", exe, "-L", libdir, "-lsdfmesh_b200",
+                            "-Wl,-rpath," + libdir], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        path = os.path.join(d, "comma.obj")
+        out = subprocess.run([exe, path, name], capture_output=True, text=True, env=dict(os.environ, LOCPATH=d))
+        assert out.returncode == 0, (out.returncode, out.stderr)
+        i = np.arange(6, dtype=np.float32)
+        v = np.stack([np.float32(0.125) * i - np.float32(0.5), np.float32(1.5) + i, np.float32(1e-5) * (i + 1),
+                      np.ones(6, np.float32)], 1)
+        uv = np.stack([np.float32(0.1) * i, np.float32(1.0) - np.float32(0.25) * i], 1)
+        got = open(path, "rb").read()
+        assert b"," not in got
+        assert got == OO.obj_text("comma.obj", v, uv)

@@ -61,7 +61,7 @@ def test_static_scout_matches_allocating_scout_twice(config, res):
 def test_static_scout_rejects_grids_beyond_its_limit():
     from cudasdf_b200 import _lib as L
     lib = L.lib()
-    limit = lib.sdf_scout_static_max_blocks()
+    limit = L.SCOUT_STATIC_MAX_BLOCKS
     grid = L.SdfGrid()
     grid.blocksDim[0], grid.blocksDim[1], grid.blocksDim[2] = 128, 128, 128  # 2,097,152 blocks
     assert 128 ** 3 > limit
