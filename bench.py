@@ -296,6 +296,8 @@ def run_ours(args, rank, world):
         out["welded"] = welded_output(args, world, eng, buf, V, flush, voxels,
                                       make_config(cell, technique=tech, out_mask=mask | L.OUT_WELDED))
         eng.configure(make_config(cell, technique=tech, out_mask=mask))  # same grid: buffers and surrogate stay
+    if tech == L.TECH_MC and rank == 0:
+        out["dropin"] = dropin_host_timing(args, prims, res, voxels)
     out["fp32_peak"] = fp32_peak_tflops()
     out["counters"] = count_work(eng, buf, res) if rank == 0 else None
     eng.close()
@@ -303,6 +305,35 @@ def run_ours(args, rank, world):
         del buf
         out["dynamic_scene"] = dynamic_scene(args, world, prims, res, cell, tech, mask, spec, V, flush)
     return out
+
+
+DROPIN_HOST = os.path.join(ROOT, "cudasdf_b200", "dropin_host", "_build", "dropin_host")
+
+
+def dropin_host_timing(args, prims, res, voxels):
+    """The drop-in as a user of the reference runs it: the reference's CudaSDFMesh.cpp, unchanged, linked
+    against this library (cudasdf_b200/dropin_host), one Update per step with its host BVH build,
+    primitive and node uploads, per-stage synchronisations and count read-back (VBO + EBO outputs).
+    Host wall time per Update (after one warm-up Update) and the sum of Update's own kernel timers."""
+    import tempfile
+
+    import numpy as np
+    if not os.path.exists(DROPIN_HOST):
+        return {"unavailable": "dropin_host not built (it needs the reference tree at build time)"}
+    with tempfile.TemporaryDirectory() as d:
+        pf = os.path.join(d, "prims.bin")
+        np.ascontiguousarray(prims).tofile(pf)
+        r = subprocess.run([DROPIN_HOST, pf, str(res), "0", "2", str(max(args.steps, 1)), "-"], capture_output=True,
+                           text=True, timeout=900)
+    if r.returncode != 0:
+        return {"unavailable": f"dropin_host exited {r.returncode}: {r.stderr.strip()[-200:]}"}
+    info = json.loads(r.stdout.strip().splitlines()[-1])
+    ms = float(info["ms_update_wall"])
+    return {"value": voxels / (ms * 1e-3) / 1e9, "unit": "Gvoxels/s", "ms_per_step": ms,
+            "ms_kernels": float(info["ms_update_kernels"]), "vertices": int(info["vertices"]),
+            "steps": int(info["repeat"]),
+            "path": "the reference's CudaSDFMesh::Update (CudaSDFMesh.cpp, unchanged) on this library's launch* "
+                    "entry points: host BVH build, uploads and per-stage syncs every step, host wall time"}
 
 
 def streamed_e2e(args, eng, prims, buf, V, mask, flush, world):
@@ -772,7 +803,7 @@ def main():
                            "stage_ms": r["plain_stages"]},
                  "triangles_per_s": (st["total_vertices"] // 3) / (r["ms"] * 1e-3),
                  "bvh_cap_hits": st["bvh_cap_hits"], "clocks": r["clocks"],
-                 "dynamic_scene": r.get("dynamic_scene"), "welded": r.get("welded"),
+                 "dynamic_scene": r.get("dynamic_scene"), "welded": r.get("welded"), "dropin": r.get("dropin"),
                  "gpu_launches": r["launches_per_step"] * args.steps})
     if "surrogate" in r:
         sg = r["surrogate"]

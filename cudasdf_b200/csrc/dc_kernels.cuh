@@ -20,6 +20,7 @@ struct DcBuffers {
     short4* cell_normals_tmp; // smoothing output
     unsigned* counts;         // per packed cell: has-vertex (mark) / quad vertex count (count quads)
     unsigned* offsets;        // per packed cell: scanned counts
+    float4* qef_debug;        // optional, per DC vertex: mass-point QEF vertex before projection, w = 1 if FP64
 };
 
 struct DcSolveParams {
@@ -488,34 +489,58 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
                     S.cell_x[i] = solve_masspoint(g, c, cv, S.h_n + S.cell_h0[i], S.h_cell + S.cell_h0[i], S.cell_m[i],
                                                   P.cond_threshold, &fp64);
                     if (fp64 && diag) atomicAdd(&diag->fp64_cells, 1ull);
+                    if (B.qef_debug)
+                        B.qef_debug[S.cell_vidx[i]] = make_float4(S.cell_x[i].x, S.cell_x[i].y, S.cell_x[i].z,
+                                                                  fp64 ? 1.f : 0.f);
                 } else {
                     S.cell_x[i] = solve_reference(g, c, cv, S, S.cell_h0[i], S.cell_m[i]);
                 }
             }
             __syncthreads();
-            // mass-point mode: project the vertex onto the surface along the gradient
-            if (P.solver == SDF_DC_SOLVER_MASSPOINT) {
-                for (int it = 0; it < P.projection_iters; ++it) {
-                    stencil_all_warps(
-                        sc, (int)ncells, g.cell, time, S.st_d, [&](int i) { return S.cell_x[i]; },
-                        [&](int i, float d, float d1, float d2, float d3) {
-                            float3 gr = f3(SUB(d1, d), SUB(d2, d), SUB(d3, d));
-                            const float len = SQRT(dot3(gr, gr));
-                            gr = len > 1e-6f ? f3(DIV(gr.x, len), DIV(gr.y, len), DIV(gr.z, len)) : f3(0.f, 0.f, 0.f);
-                            if (!isfinite(d)) return;
-                            // keep the step inside the cell's soft-clamp box
-                            const float3 x = S.cell_x[i];
-                            const CellInfo c = cell_info(g, bx, by, bz, S.cell_tid[i]);
-                            const float3 cmin = grid_loc(g, c.x, c.y, c.z);
-                            const float margin = 0.10f * g.cell;
-                            float3 y = f3(x.x - d * gr.x, x.y - d * gr.y, x.z - d * gr.z);
-                            y = f3(CLAMP(y.x, cmin.x - margin, cmin.x + g.cell + margin),
-                                   CLAMP(y.y, cmin.y - margin, cmin.y + g.cell + margin),
-                                   CLAMP(y.z, cmin.z - margin, cmin.z + g.cell + margin));
-                            S.cell_x[i] = y;
-                        },
-                        diag);
+            // mass-point mode: project the vertex onto the surface, x <- x - f(x) n, along the cell's mean
+            // Hermite normal n (the normalised sum of its unit Hermite normals; no step where that sum is
+            // shorter than 1e-6). The steps run in cell-local coordinates y = x - cell corner, starting
+            // from the vertex clamped to the cell widened by 0.1 cell and kept in that box; each step
+            // evaluates map() at the float point corner + y. A fixed direction per cell keeps the step
+            // independent of finite differences of the field at the vertex, and every operation is
+            // rounded on its own, so a float32 restatement on the host reproduces the steps.
+            if (P.solver == SDF_DC_SOLVER_MASSPOINT && P.projection_iters > 0) {
+                const float margin = MUL(0.10f, g.cell), hi = ADD(g.cell, margin);
+                for (int i = threadIdx.x; i < (int)ncells; i += blockDim.x) {
+                    const CellInfo c = cell_info(g, bx, by, bz, S.cell_tid[i]);
+                    const float3 y = sub3(S.cell_x[i], grid_loc(g, c.x, c.y, c.z));
+                    S.cell_x[i] = f3(CLAMP(y.x, -margin, hi), CLAMP(y.y, -margin, hi), CLAMP(y.z, -margin, hi));
                 }
+                __syncthreads();
+                // each cell stays with one lane of one warp for all steps
+                for (int base = warp * 32; base < (int)ncells; base += nwarps * 32) {
+                    const int i = base + lane;
+                    const bool valid = i < (int)ncells;
+                    float3 cm = f3(0.f, 0.f, 0.f), nbar = f3(0.f, 0.f, 0.f), y = f3(0.f, 0.f, 0.f);
+                    bool has_dir = false;
+                    if (valid) {
+                        const CellInfo c = cell_info(g, bx, by, bz, S.cell_tid[i]);
+                        cm = grid_loc(g, c.x, c.y, c.z);
+                        y = S.cell_x[i];
+                        float3 nsum = f3(0.f, 0.f, 0.f);
+                        const int h0 = S.cell_h0[i], m = S.cell_m[i];
+                        for (int q = 0; q < m; ++q) {
+                            float3 n;
+                            if (unit_normal_rn(S.h_n[h0 + q], n)) nsum = add3(nsum, n);
+                        }
+                        has_dir = unit_normal_rn(nsum, nbar);
+                    }
+                    for (int it = 0; it < P.projection_iters; ++it) {
+                        MapState<false> st;
+                        map_warp<false>(sc, add3(cm, y), valid && has_dir, time, st, diag);
+                        if (valid && has_dir && isfinite(st.d)) {
+                            const float3 yn = sub3(y, scl3(nbar, st.d));
+                            y = f3(CLAMP(yn.x, -margin, hi), CLAMP(yn.y, -margin, hi), CLAMP(yn.z, -margin, hi));
+                        }
+                    }
+                    if (valid) S.cell_x[i] = add3(cm, y);
+                }
+                __syncthreads();
             }
             // soft clamp, hard clamp to the cell, blend towards the cell centre (:1556-1577)
             for (int i = threadIdx.x; i < (int)ncells; i += blockDim.x) {
@@ -889,8 +914,10 @@ __global__ void __launch_bounds__(BLK_THREADS, 3) k_dc_quads(GridView g0, SceneV
                 unsigned char fl = S.q_flags[i] | (flip ? 1 : 0);
                 bool alt = false;
                 if (QP.adaptive_diagonal) {
-                    // split along the shorter diagonal: (1,2,3),(1,3,0) instead of (0,1,2),(0,2,3)
-                    const float d02 = len2_3(sub3(Q.v[2], Q.v[0])), d13 = len2_3(sub3(Q.v[3], Q.v[1]));
+                    // split along the shorter diagonal: (1,2,3),(1,3,0) instead of (0,1,2),(0,2,3); squared
+                    // lengths with every operation rounded on its own (a float32 restatement reproduces the choice)
+                    const float3 e02 = sub3(Q.v[2], Q.v[0]), e13 = sub3(Q.v[3], Q.v[1]);
+                    const float d02 = dot3_rn(e02, e02), d13 = dot3_rn(e13, e13);
                     alt = d13 < d02;
                     if (alt) fl |= 4;
                 }

@@ -99,6 +99,8 @@ struct EngineImpl {
     ushort4* dc_verts = nullptr;
     short4* dc_norms = nullptr;
     size_t dc_cap = 0;
+    float4* dc_qef = nullptr;              // debug bit 1: mass-point QEF vertices before projection
+    size_t dc_qef_cap = 0;
     unsigned char* ctrl_region = nullptr;  // Ctrl, then the three scan regions
     size_t ctrl_bytes = 0;
     size_t scanA_off = 0, scanB_off = 0, scanD_off = 0, scanC_off = 0;
@@ -149,7 +151,7 @@ struct EngineImpl {
     void release() {
         void* ptrs[] = {d_prims, d_nodes, flags, list, fields, block_totals, block_offsets, packet_counts,
                         packet_offsets, b2a, masks, dc_voff, dc_verts, dc_norms, ctrl_region, eval_diag, miss,
-                        cell_words, bvh_work, weld_bits, weld_prefix, weld_totals, weld_base};
+                        cell_words, bvh_work, weld_bits, weld_prefix, weld_totals, weld_base, dc_qef};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         d_prims = nullptr; d_nodes = nullptr; flags = nullptr; list = nullptr; fields = nullptr;
@@ -162,6 +164,8 @@ struct EngineImpl {
         bvh_work = nullptr;
         weld_bits = nullptr; weld_prefix = nullptr; weld_totals = nullptr; weld_base = nullptr;
         weld_cap = 0;
+        dc_qef = nullptr;
+        dc_qef_cap = 0;
         prims_cap = nodes_cap = dc_cap = packet_cap = miss_cap = cell_words_cap = bvh_work_cap = 0;
         if (h_bvh_ctl) cudaFreeHost(h_bvh_ctl);
         h_bvh_ctl = nullptr;
@@ -328,7 +332,9 @@ void sdf_engine_set_timing(sdf_engine* e, int enabled) {
     if (e) e->impl.timing = enabled != 0;
 }
 
-// debug bit 0: also write the per-cell counts/offsets of the drop-in layout (marching cubes)
+// debug bit 0: also write the per-cell counts/offsets of the drop-in layout (marching cubes);
+// debug bit 1: keep each mass-point QEF vertex before its projection steps (buffer 11, float4 per DC
+// vertex, w = 1 where the cell was solved in FP64)
 void sdf_engine_set_debug(sdf_engine* e, int flags) {
     if (e) e->impl.debug = flags;
 }
@@ -596,6 +602,10 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
             if (dev_alloc(E.dc_verts, want) != SDF_OK || dev_alloc(E.dc_norms, want) != SDF_OK) return SDF_ERR_NOMEM;
             E.dc_cap = want;
         }
+        if ((E.debug & 2) && E.dc_qef_cap < E.dc_cap) {
+            if (dev_alloc(E.dc_qef, E.dc_cap) != SDF_OK) return SDF_ERR_NOMEM;
+            E.dc_qef_cap = E.dc_cap;
+        }
     }
     cudaGetLastError();
     auto t0 = std::chrono::high_resolution_clock::now();
@@ -710,6 +720,7 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
         B.cell_normals_tmp = nullptr;
         B.counts = E.packet_counts;
         B.offsets = E.packet_offsets;
+        B.qef_debug = (E.debug & 2) ? E.dc_qef : nullptr;
         record(cudaMemsetAsync(E.b2a, 0xFF, (size_t)nb * sizeof(int), st));
         k_dc_block_map<<<(nb + 255) / 256, 256, 0, st>>>(E.list, &ctrl->active_count, nb, nb, E.b2a);
         check_launch();
@@ -861,6 +872,7 @@ const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes) {
         case 8: p = E.fields; b = (size_t)E.nblocks * sdfb::FIELD_STRIDE * 4; break;
         case 9: p = E.d_prims; b = (size_t)E.nprims * sizeof(sdf_primitive); break;
         case 10: p = E.d_nodes; b = (size_t)E.nnodes * sizeof(sdf_bvh_node); break;
+        case 11: p = E.dc_qef; b = E.dc_qef_cap * 16; break;
         default: break;
     }
     if (bytes) *bytes = b;

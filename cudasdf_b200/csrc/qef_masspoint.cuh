@@ -1,53 +1,119 @@
 // Mass-point-centred QEF for dual contouring (no counterpart in the reference's solver).
 //
-// For the Hermite samples (p_i, n_i) of a cell, minimise sum_i (n_i . (x - p_i))^2 with x written
-// as c + y, c the mass point (mean of the p_i). The normal equations A y = b, A = sum n n^T,
-// b = sum n (n . (p_i - c)), are formed in FP32. A symmetric Jacobi eigensolve gives A = V L V^T;
-// y = sum_k v_k (v_k . b) / l_k over the eigenvalues l_k >= l_max / cond_threshold (pseudo-inverse
-// truncation: directions the normals do not constrain stay at the mass point). Cells whose condition
-// number l_max / l_min is above cond_threshold / 16 are solved in FP64 (FP64 on the GPU only for
-// those cells).
+// For the Hermite samples (p_i, n_i) of a cell, minimise sum_i (n_i . (x - p_i))^2 with x written as
+// c + y, c the mass point (mean of the p_i). The normal equations A y = b, A = sum n n^T,
+// b = sum n (n . (p_i - c)), have the eigen-decomposition A = V L V^T.
+//
+// Condition number and the FP32 / FP64 split. The eigenvectors come from a Jacobi sweep of the FP32 A;
+// each eigenvalue is then taken as the Rayleigh quotient sum_i (v_k . n_i)^2 of the unit normals
+// themselves, which is accurate to the rounding of the normals (the diagonal of a Jacobi sweep of the
+// rounded A errs by about cond x 2^-24 relative). cond = l_max / l_min. Cells with cond above
+// cond_threshold form and solve the equations in FP64 (a Jacobi eigensolve and the pseudo-inverse
+// truncated at l_max / cond_threshold: directions the normals do not constrain stay at the mass
+// point); FP64 runs on the GPU only for those cells. Every other cell is solved in FP32:
+// y = sum_k v_k (v_k . r) / l_k, refined twice, where the residual r = sum_i n_i (n_i . (p_i - c - y))
+// is formed from the Hermite samples and not as b - A y from the rounded A (the rounding of A would
+// limit the FP32 solution to about cond x 2^-24 of its size; the Hermite form keeps the error near
+// sqrt(cond) x 2^-24 of a cell).
+//
+// Every FP32 operation of the decision and of the FP32 solve is rounded on its own (no contraction),
+// so a float32 restatement on the host reproduces the condition number, hence the FP32 / FP64 split,
+// bit for bit.
 #pragma once
 
 #include "mc_kernels.cuh"
 
 namespace sdfb {
 
-template <class T>
-__device__ __forceinline__ void jacobi3(T A[3][3], T V[3][3], int sweeps) {
+// a.x*b.x + a.y*b.y + a.z*b.z, each product and sum rounded on its own
+__device__ __forceinline__ float dot3_rn(float3 a, float3 b) {
+    return ADD(ADD(MUL(a.x, b.x), MUL(a.y, b.y)), MUL(a.z, b.z));
+}
+
+// unit normal of a Hermite sample; false (and no normal) when its length is below 1e-6
+__device__ __forceinline__ bool unit_normal_rn(float3 h, float3& n) {
+    const float len = SQRT(dot3_rn(h, h));
+    if (len < 1e-6f) return false;
+    n = f3(DIV(h.x, len), DIV(h.y, len), DIV(h.z, len));
+    return true;
+}
+
+// Cyclic Jacobi eigensolve of a symmetric 3x3 in FP32, every operation rounded on its own: A ends
+// (nearly) diagonal, the columns of V are the eigenvectors.
+__device__ __forceinline__ void jacobi3_rn(float A[3][3], float V[3][3]) {
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) V[i][j] = (i == j) ? T(1) : T(0);
-    for (int s = 0; s < sweeps; ++s) {
-        const T off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
-        const T diag = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
-        if (off <= diag * T(1e-30) || off == T(0)) break;
+        for (int j = 0; j < 3; ++j) V[i][j] = (i == j) ? 1.f : 0.f;
+    for (int s = 0; s < 8; ++s) {
+        const float off = ADD(ADD(MUL(A[0][1], A[0][1]), MUL(A[0][2], A[0][2])), MUL(A[1][2], A[1][2]));
+        const float dg = ADD(ADD(MUL(A[0][0], A[0][0]), MUL(A[1][1], A[1][1])), MUL(A[2][2], A[2][2]));
+        if (off <= MUL(dg, 1e-30f) || off == 0.f) break;
 #pragma unroll
         for (int pq = 0; pq < 3; ++pq) {
             const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
-            const T apq = A[p][q];
-            if (apq == T(0)) continue;
-            const T theta = (A[q][q] - A[p][p]) / (T(2) * apq);
-            const T t = (theta >= T(0) ? T(1) : T(-1)) / (fabs(theta) + sqrt(theta * theta + T(1)));
-            const T c = T(1) / sqrt(t * t + T(1));
-            const T sn = t * c;
-            // A <- J^T A J for the rotation in the (p, q) plane
+            const float apq = A[p][q];
+            if (apq == 0.f) continue;
+            const float theta = DIV(SUB(A[q][q], A[p][p]), MUL(2.f, apq));
+            const float t = DIV(theta >= 0.f ? 1.f : -1.f, ADD(fabsf(theta), SQRT(ADD(MUL(theta, theta), 1.f))));
+            const float c = DIV(1.f, SQRT(ADD(MUL(t, t), 1.f)));
+            const float sn = MUL(t, c);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const T akp = A[k][p], akq = A[k][q];
+                const float akp = A[k][p], akq = A[k][q];
+                A[k][p] = SUB(MUL(c, akp), MUL(sn, akq));
+                A[k][q] = ADD(MUL(sn, akp), MUL(c, akq));
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float apk = A[p][k], aqk = A[q][k];
+                A[p][k] = SUB(MUL(c, apk), MUL(sn, aqk));
+                A[q][k] = ADD(MUL(sn, apk), MUL(c, aqk));
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float vkp = V[k][p], vkq = V[k][q];
+                V[k][p] = SUB(MUL(c, vkp), MUL(sn, vkq));
+                V[k][q] = ADD(MUL(sn, vkp), MUL(c, vkq));
+            }
+        }
+    }
+}
+
+// FP64 Jacobi eigensolve for the ill-conditioned cells
+__device__ __forceinline__ void jacobi3_f64(double A[3][3], double V[3][3], int sweeps) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) V[i][j] = (i == j) ? 1.0 : 0.0;
+    for (int s = 0; s < sweeps; ++s) {
+        const double off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
+        const double diag = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
+        if (off <= diag * 1e-30 || off == 0.0) break;
+#pragma unroll
+        for (int pq = 0; pq < 3; ++pq) {
+            const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
+            const double apq = A[p][q];
+            if (apq == 0.0) continue;
+            const double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
+            const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            const double c = 1.0 / sqrt(t * t + 1.0);
+            const double sn = t * c;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double akp = A[k][p], akq = A[k][q];
                 A[k][p] = c * akp - sn * akq;
                 A[k][q] = sn * akp + c * akq;
             }
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const T apk = A[p][k], aqk = A[q][k];
+                const double apk = A[p][k], aqk = A[q][k];
                 A[p][k] = c * apk - sn * aqk;
                 A[q][k] = sn * apk + c * aqk;
             }
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const T vkp = V[k][p], vkq = V[k][q];
+                const double vkp = V[k][p], vkq = V[k][q];
                 V[k][p] = c * vkp - sn * vkq;
                 V[k][q] = sn * vkp + c * vkq;
             }
@@ -55,88 +121,70 @@ __device__ __forceinline__ void jacobi3(T A[3][3], T V[3][3], int sweeps) {
     }
 }
 
-template <class T>
-__device__ __forceinline__ void pinv_solve(T A[3][3], const T b[3], T cond_threshold, int sweeps, T y[3]) {
-    T V[3][3];
-    jacobi3<T>(A, V, sweeps);
-    const T l0 = A[0][0], l1 = A[1][1], l2 = A[2][2];
-    const T lmax = fmax(fmax(fabs(l0), fabs(l1)), fabs(l2));
-    y[0] = y[1] = y[2] = T(0);
-    if (!(lmax > T(0))) return;
-    const T lcut = lmax / cond_threshold;
-    const T lam[3] = {l0, l1, l2};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        if (!(lam[k] >= lcut)) continue;
-        const T proj = (V[0][k] * b[0] + V[1][k] * b[1] + V[2][k] * b[2]) / lam[k];
-        y[0] += V[0][k] * proj;
-        y[1] += V[1][k] * proj;
-        y[2] += V[2][k] * proj;
-    }
-}
-
 // The mass-point solve for one cell; returns the unclamped vertex. *used_fp64 reports the branch.
-// The Hermite points are taken relative to the cell's corner (an exact subtraction for points of the
-// cell, Sterbenz's lemma), so the mass point and the offsets p_i - c keep the full precision of the
-// cell-sized differences. A backward-stable FP32 solve has a forward error of about
-// cond * 2^-24 relative, so the FP32 branch (with one step of iterative refinement) takes the cells
-// with cond <= cond_threshold / 16 (error below 4e-5 of the vertex offset); every other cell forms
-// the normal equations from the Hermite data again in FP64 and solves them with the FP64 Jacobi
-// eigensolve and the pseudo-inverse truncated at lmax / cond_threshold.
+// The Hermite points are taken relative to the cell's corner, so the mass point and the offsets
+// p_i - c keep the precision of cell-sized differences.
 __device__ float3 solve_masspoint(const GridView& g, const CellInfo& c, const float cv[8],
                                   const float3* __restrict__ hn, const unsigned short* __restrict__ hcell, int m,
                                   float cond_threshold, int* used_fp64 = nullptr) {
     const float3 cmin = grid_loc(g, c.x, c.y, c.z);
+    if (used_fp64) *used_fp64 = 0;
     if (m <= 0) return f3(FMA(0.5f, g.cell, cmin.x), FMA(0.5f, g.cell, cmin.y), FMA(0.5f, g.cell, cmin.z));
     float3 sum = f3(0.f, 0.f, 0.f);
     for (int i = 0; i < m; ++i) sum = add3(sum, sub3(edge_point(g, c.x, c.y, c.z, cv, hcell[i] & 15), cmin));
-    const float3 mq = scl3(sum, 1.f / (float)m);  // mass point relative to the corner
-    float A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, b[3] = {0, 0, 0};
+    const float3 mq = scl3(sum, DIV(1.f, (float)m));  // mass point relative to the corner
+    // normal equations in FP32, for the eigenvectors
+    float A[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
     for (int i = 0; i < m; ++i) {
-        float3 n = hn[i];
-        const float len = sqrtf(n.x * n.x + n.y * n.y + n.z * n.z);
-        if (len < 1e-6f) continue;
-        n = f3(n.x / len, n.y / len, n.z / len);
-        const float3 q = sub3(edge_point(g, c.x, c.y, c.z, cv, hcell[i] & 15), cmin);
-        const float d = n.x * (q.x - mq.x) + n.y * (q.y - mq.y) + n.z * (q.z - mq.z);
+        float3 n;
+        if (!unit_normal_rn(hn[i], n)) continue;
         const float nn[3] = {n.x, n.y, n.z};
 #pragma unroll
-        for (int r = 0; r < 3; ++r) {
+        for (int r = 0; r < 3; ++r)
 #pragma unroll
-            for (int k = 0; k < 3; ++k) A[r][k] += nn[r] * nn[k];
-            b[r] += nn[r] * d;
-        }
+            for (int k = 0; k < 3; ++k) A[r][k] = ADD(A[r][k], MUL(nn[r], nn[k]));
     }
-    // FP32 eigensolve; condition number from its eigenvalues
-    float Af[3][3], Vf[3][3];
+    float V[3][3];
+    jacobi3_rn(A, V);
+    // eigenvalues: Rayleigh quotients of the unit normals
+    float lam[3];
+    float3 vk[3];
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) Af[r][k] = A[r][k];
-    jacobi3<float>(Af, Vf, 8);
-    const float l0 = fabsf(Af[0][0]), l1 = fabsf(Af[1][1]), l2 = fabsf(Af[2][2]);
-    const float lmax = fmaxf(fmaxf(l0, l1), l2), lmin = fminf(fminf(l0, l1), l2);
-    const bool fp64 = !(lmin * (cond_threshold * 0.0625f) >= lmax);
-    if (used_fp64) *used_fp64 = fp64 ? 1 : 0;
+    for (int k = 0; k < 3; ++k) {
+        vk[k] = f3(V[0][k], V[1][k], V[2][k]);
+        float l = 0.f;
+        for (int i = 0; i < m; ++i) {
+            float3 n;
+            if (!unit_normal_rn(hn[i], n)) continue;
+            const float d = dot3_rn(vk[k], n);
+            l = ADD(l, MUL(d, d));
+        }
+        lam[k] = l;
+    }
+    const float lmax = fmaxf(fmaxf(lam[0], lam[1]), lam[2]), lmin = fminf(fminf(lam[0], lam[1]), lam[2]);
+    const bool fp64 = !(MUL(lmin, cond_threshold) >= lmax);  // cond = lmax / lmin > cond_threshold
     if (!fp64) {
-        const float lam[3] = {Af[0][0], Af[1][1], Af[2][2]};
-        float y[3] = {0.f, 0.f, 0.f};
-        // y = A^-1 b, then y += A^-1 (b - A y)
-        for (int pass = 0; pass < 2; ++pass) {
-            float r[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) r[k] = b[k] - (A[k][0] * y[0] + A[k][1] * y[1] + A[k][2] * y[2]);
+        // FP32: y = sum_k v_k (v_k . r) / l_k, r from the Hermite samples, three passes
+        float3 y = f3(0.f, 0.f, 0.f);
+        for (int pass = 0; pass < 3; ++pass) {
+            float3 r = f3(0.f, 0.f, 0.f);
+            for (int i = 0; i < m; ++i) {
+                float3 n;
+                if (!unit_normal_rn(hn[i], n)) continue;
+                const float3 q = sub3(edge_point(g, c.x, c.y, c.z, cv, hcell[i] & 15), cmin);
+                const float e = dot3_rn(n, sub3(sub3(q, mq), y));
+                r = add3(r, scl3(n, e));
+            }
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const float proj = (Vf[0][k] * r[0] + Vf[1][k] * r[1] + Vf[2][k] * r[2]) / lam[k];
-                y[0] += Vf[0][k] * proj;
-                y[1] += Vf[1][k] * proj;
-                y[2] += Vf[2][k] * proj;
+                if (!(lam[k] > 0.f)) continue;
+                y = add3(y, scl3(vk[k], DIV(dot3_rn(vk[k], r), lam[k])));
             }
         }
-        return f3(cmin.x + (mq.x + y[0]), cmin.y + (mq.y + y[1]), cmin.z + (mq.z + y[2]));
+        return f3(ADD(cmin.x, ADD(mq.x, y.x)), ADD(cmin.y, ADD(mq.y, y.y)), ADD(cmin.z, ADD(mq.z, y.z)));
     }
-    // FP64: the same equations from the FP32 Hermite data
+    if (used_fp64) *used_fp64 = 1;
+    // FP64: the equations from the FP32 Hermite data again, eigensolve, truncated pseudo-inverse
     double qd[12][3], sd[3] = {0.0, 0.0, 0.0};
     for (int i = 0; i < m; ++i) {
         const float3 q = sub3(edge_point(g, c.x, c.y, c.z, cv, hcell[i] & 15), cmin);
@@ -144,7 +192,7 @@ __device__ float3 solve_masspoint(const GridView& g, const CellInfo& c, const fl
         sd[0] += q.x; sd[1] += q.y; sd[2] += q.z;
     }
     const double md[3] = {sd[0] / m, sd[1] / m, sd[2] / m};
-    double Ad[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, bd[3] = {0, 0, 0}, yd[3];
+    double Ad[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, bd[3] = {0, 0, 0};
     for (int i = 0; i < m; ++i) {
         const double nx = hn[i].x, ny = hn[i].y, nz = hn[i].z;
         const double len = sqrt(nx * nx + ny * ny + nz * nz);
@@ -158,7 +206,23 @@ __device__ float3 solve_masspoint(const GridView& g, const CellInfo& c, const fl
             bd[r] += nn[r] * d;
         }
     }
-    pinv_solve<double>(Ad, bd, (double)cond_threshold, 24, yd);
+    double Vd[3][3];
+    jacobi3_f64(Ad, Vd, 24);
+    const double l0 = Ad[0][0], l1 = Ad[1][1], l2 = Ad[2][2];
+    const double lmaxd = fmax(fmax(fabs(l0), fabs(l1)), fabs(l2));
+    double yd[3] = {0.0, 0.0, 0.0};
+    if (lmaxd > 0.0) {
+        const double lcut = lmaxd / (double)cond_threshold;
+        const double ld[3] = {l0, l1, l2};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (!(ld[k] >= lcut)) continue;
+            const double proj = (Vd[0][k] * bd[0] + Vd[1][k] * bd[1] + Vd[2][k] * bd[2]) / ld[k];
+            yd[0] += Vd[0][k] * proj;
+            yd[1] += Vd[1][k] * proj;
+            yd[2] += Vd[2][k] * proj;
+        }
+    }
     return f3((float)((double)cmin.x + (md[0] + yd[0])), (float)((double)cmin.y + (md[1] + yd[1])),
               (float)((double)cmin.z + (md[2] + yd[2])));
 }

@@ -274,6 +274,7 @@ static DcBuffers dc_buffers_of(const sdf_grid& g) {
     b.cell_normals_tmp = reinterpret_cast<short4*>(g.d_dcCellNormalsTmp);
     b.counts = g.d_packetVertexCounts;
     b.offsets = g.d_packetVertexOffsets;
+    b.qef_debug = nullptr;
     return b;
 }
 

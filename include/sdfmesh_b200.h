@@ -270,14 +270,16 @@ void sdf_engine_set_timing(sdf_engine* e, int enabled);
 /* Debug outputs: bit 0 also writes the per-cell vertex counts/offsets of the drop-in layout in
  * marching-cubes mode (readable through sdf_engine_buffer 1 and 2) and, in dual-contouring mode,
  * the per-cell vertex normals of the reference's dcSolveCellVertices (sdf_engine_buffer 6), which
- * no output of the engine needs. */
+ * no output of the engine needs; bit 1 keeps, with the mass-point solver, each cell's QEF vertex
+ * before its projection steps (sdf_engine_buffer 11: float4 per DC vertex, w = 1 where FP64 solved
+ * the cell). */
 void sdf_engine_set_debug(sdf_engine* e, int flags);
 /* The scene as uploaded: sorted primitives (count = numPrimitives) and BVH nodes. */
 int sdf_engine_get_bvh(sdf_engine* e, sdf_bvh_node* nodes_out, int capacity, int* num_bvh_primitives);
 /* Device pointer to the last extraction's internal arrays, for inspection: 0 active block list,
  * 1 per-cell vertex counts (compat layout), 2 per-cell offsets, 3 DC corner masks, 4 DC cell vertex
  * offsets, 5 DC cell vertices, 6 DC cell normals, 7 per-block vertex totals, 8 block field rows; and
- * the scene: 9 sorted primitives, 10 BVH nodes. */
+ * the scene: 9 sorted primitives, 10 BVH nodes; 11 mass-point QEF vertices (debug bit 1). */
 const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes);
 /* Copies the first `bytes` bytes of an internal array (ids as for sdf_engine_buffer) to host memory. */
 sdf_status sdf_engine_read_buffer(sdf_engine* e, int which, void* host_dst, size_t bytes);
