@@ -106,7 +106,7 @@ SURROGATE_SYMBOLS = ["sdf_surrogate_default_config", "sdf_surrogate_train", "sdf
                      "sdf_surrogate_audit", "sdf_surrogate_num_params", "sdf_surrogate_set_params",
                      "sdf_surrogate_get_params", "sdf_surrogate_forward", "sdf_surrogate_gradient"]
 BATCH_SYMBOLS = ["sdf_batch_create", "sdf_batch_destroy", "sdf_batch_set_scenes", "sdf_batch_extract",
-                 "sdf_batch_capture"]
+                 "sdf_batch_capture", "sdf_batch_read_buffer"]
 STATIC_SCOUT_SYMBOLS = ["sdf_scout_active_blocks_static"]
 SCOUT_STATIC_MAX_BLOCKS = 1 << 20  # SDF_SCOUT_STATIC_MAX_BLOCKS of the header
 EXPORT_SYMBOLS = ["sdf_write_obj"]
@@ -212,6 +212,8 @@ def lib():
     L.sdf_batch_extract.restype = i
     L.sdf_batch_capture.argtypes = [vp, f, ctypes.POINTER(SdfOutputs), ctypes.POINTER(SdfOutputs), vp, i]
     L.sdf_batch_capture.restype = i
+    L.sdf_batch_read_buffer.argtypes = [vp, i, i, vp, ctypes.POINTER(ctypes.c_size_t)]
+    L.sdf_batch_read_buffer.restype = i
     L.sdf_scout_active_blocks_static.argtypes = [G, f]
     L.sdf_scout_active_blocks_static.restype = i
     L.sdf_write_obj.argtypes = [ctypes.c_char_p, vp, ctypes.c_uint64, vp, ctypes.c_uint64, vp]

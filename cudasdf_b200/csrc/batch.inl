@@ -535,4 +535,39 @@ sdf_status sdf_batch_capture(sdf_batch* b, float time, const sdf_outputs* mc_out
     return SDF_OK;
 }
 
+sdf_status sdf_batch_read_buffer(sdf_batch* b, int technique, int which, void* host_dst, size_t* bytes) {
+    using namespace sdfb;
+    if (!b || !bytes || (technique != SDF_TECH_MARCHING_CUBES && technique != SDF_TECH_DUAL_CONTOURING))
+        return SDF_ERR_INVALID;
+    BatchImpl& I = b->impl;
+    BatchGroup& B = I.g[technique == SDF_TECH_DUAL_CONTOURING ? 1 : 0];
+    if (B.n == 0 || !B.h_ctrl) return SDF_ERR_INVALID;
+    const size_t act = (size_t)std::min<long long>(B.h_ctrl->active_count, B.total_blocks);
+    const void* src = nullptr;
+    size_t have = 0;
+    switch (which) {
+        case 0: src = B.list; have = act * sizeof(int); break;
+        case 1: src = B.block_totals; have = act * sizeof(unsigned); break;
+        case 2: src = B.packet_counts; have = B.packet_counts ? act * 512 * sizeof(unsigned) : 0; break;
+        case 3: src = B.masks; have = B.masks ? act * 512 : 0; break;
+        case 4: src = B.dc_voff; have = B.dc_voff ? act * 512 * sizeof(unsigned) : 0; break;
+        case 5:
+            src = B.dc_verts;
+            have = B.dc_verts ? (size_t)std::min<unsigned long long>(B.h_ctrl->dc_vertices, B.dc_cap) * sizeof(ushort4)
+                              : 0;
+            break;
+        default: return SDF_ERR_INVALID;
+    }
+    const size_t want = std::min(*bytes, have);
+    *bytes = have;
+    if (!host_dst || want == 0) return SDF_OK;
+    cudaSetDevice(I.device);
+    const cudaError_t e = cudaMemcpy(host_dst, src, want, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        record(e);
+        return SDF_ERR_CUDA;
+    }
+    return SDF_OK;
+}
+
 }  // extern "C"

@@ -64,6 +64,7 @@ extern "C" sdf_status sdf_scout_active_blocks_static(sdf_grid* grid, float time)
         g_static_scout_base[dev] = static_cast<unsigned char*>(p);
     }
     unsigned char* base = g_static_scout_base[dev];
+    g_scratch[dev & 15].rows_valid = false;  // the active list is rewritten: drop-in field rows are stale
     unsigned long long* status = reinterpret_cast<unsigned long long*>(base);
     Diag* diag = reinterpret_cast<Diag*>(base + kStaticDiagOffset);
     unsigned* flags = reinterpret_cast<unsigned*>(base + kStaticFlagsOffset);

@@ -13,8 +13,8 @@
 // point); FP64 runs on the GPU only for those cells. Every other cell is solved in FP32:
 // y = sum_k v_k (v_k . r) / l_k, refined twice, where the residual r = sum_i n_i (n_i . (p_i - c - y))
 // is formed from the Hermite samples and not as b - A y from the rounded A (the rounding of A would
-// limit the FP32 solution to about cond x 2^-24 of its size; the Hermite form keeps the error near
-// sqrt(cond) x 2^-24 of a cell).
+// limit the FP32 solution to about cond x 2^-24 of its size), and summed with its rounding errors
+// carried.
 //
 // Every FP32 operation of the decision and of the FP32 solve is rounded on its own (no contraction),
 // so a float32 restatement on the host reproduces the condition number, hence the FP32 / FP64 split,
@@ -28,6 +28,18 @@ namespace sdfb {
 // a.x*b.x + a.y*b.y + a.z*b.z, each product and sum rounded on its own
 __device__ __forceinline__ float dot3_rn(float3 a, float3 b) {
     return ADD(ADD(MUL(a.x, b.x), MUL(a.y, b.y)), MUL(a.z, b.z));
+}
+
+// hi + lo += a * b, the sum kept unevaluated: the product's rounding error (exact by FMA) and the
+// addition's rounding error (exact by Knuth's two-sum) are both carried in lo
+__device__ __forceinline__ void acc2_rn(float& hi, float& lo, float a, float b) {
+    const float p = MUL(a, b);
+    const float pe = FMA(a, b, -p);
+    const float s = ADD(hi, p);
+    const float bb = SUB(s, hi);
+    const float err = ADD(SUB(hi, SUB(s, bb)), SUB(p, bb));
+    hi = s;
+    lo = ADD(lo, ADD(err, pe));
 }
 
 // unit normal of a Hermite sample; false (and no normal) when its length is below 1e-6
@@ -164,17 +176,22 @@ __device__ float3 solve_masspoint(const GridView& g, const CellInfo& c, const fl
     const float lmax = fmaxf(fmaxf(lam[0], lam[1]), lam[2]), lmin = fminf(fminf(lam[0], lam[1]), lam[2]);
     const bool fp64 = !(MUL(lmin, cond_threshold) >= lmax);  // cond = lmax / lmin > cond_threshold
     if (!fp64) {
-        // FP32: y = sum_k v_k (v_k . r) / l_k, r from the Hermite samples, three passes
+        // FP32: y = sum_k v_k (v_k . r) / l_k, r from the Hermite samples, three passes; r is summed with
+        // its rounding errors carried (acc2_rn): near the solution its terms cancel, and an error left
+        // in r along the weakest direction grows by cond in y
         float3 y = f3(0.f, 0.f, 0.f);
         for (int pass = 0; pass < 3; ++pass) {
-            float3 r = f3(0.f, 0.f, 0.f);
+            float3 rh = f3(0.f, 0.f, 0.f), rl = f3(0.f, 0.f, 0.f);
             for (int i = 0; i < m; ++i) {
                 float3 n;
                 if (!unit_normal_rn(hn[i], n)) continue;
                 const float3 q = sub3(edge_point(g, c.x, c.y, c.z, cv, hcell[i] & 15), cmin);
                 const float e = dot3_rn(n, sub3(sub3(q, mq), y));
-                r = add3(r, scl3(n, e));
+                acc2_rn(rh.x, rl.x, n.x, e);
+                acc2_rn(rh.y, rl.y, n.y, e);
+                acc2_rn(rh.z, rl.z, n.z, e);
             }
+            const float3 r = add3(rh, rl);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 if (!(lam[k] > 0.f)) continue;

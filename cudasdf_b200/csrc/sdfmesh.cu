@@ -100,6 +100,23 @@ static SceneView scene_view(const sdf_grid& g) {
 // device scratch for the drop-in launchers (one set per device, grown on demand). The launchers
 // run on the legacy default stream, like the reference's, so one set is enough.
 // ------------------------------------------------------------------------------------------------
+// What a set of block-field rows was computed for: the grid, the scene, the time and the active list.
+struct FieldKey {
+    GridView gv;
+    SceneView sv;
+    float time;
+    const int* list;
+    const int* count;
+    int n;
+};
+static bool same_key(const FieldKey& a, const FieldKey& b) {
+    return a.gv.w == b.gv.w && a.gv.h == b.gv.h && a.gv.d == b.gv.d && a.gv.bx == b.gv.bx && a.gv.by == b.gv.by &&
+           a.gv.bz == b.gv.bz && a.gv.ox == b.gv.ox && a.gv.oy == b.gv.oy && a.gv.oz == b.gv.oz &&
+           a.gv.cell == b.gv.cell && a.sv.prims == b.sv.prims && a.sv.nodes == b.sv.nodes &&
+           a.sv.nprims == b.sv.nprims && a.sv.nbvh == b.sv.nbvh && a.sv.nnodes == b.sv.nnodes && a.time == b.time &&
+           a.list == b.list && a.count == b.count && a.n == b.n;
+}
+
 struct Scratch {
     int device = -1;
     unsigned* flags = nullptr;
@@ -108,6 +125,16 @@ struct Scratch {
     size_t status_cap = 0;
     unsigned* tickets = nullptr;           // 8 work tickets
     Diag* diag = nullptr;
+    // the shared-halo block field of the counting / marking launchers (k_field_plan / own / miss /
+    // gather), kept for the next emission / solve launcher of the same key
+    int* b2a = nullptr;
+    size_t b2a_cap = 0;
+    unsigned* miss = nullptr;
+    size_t miss_cap = 0;
+    float* rows = nullptr;                 // FIELD_STRIDE floats per active block
+    size_t rows_cap = 0;
+    bool rows_valid = false;
+    FieldKey rows_key{};
 };
 static Scratch g_scratch[16];
 
@@ -144,6 +171,82 @@ static bool ensure_status(Scratch& s, size_t words) {
     }
     s.status_cap = words;
     return true;
+}
+
+template <class T>
+static bool ensure_buffer(T*& p, size_t& cap, size_t n) {
+    if (cap >= n) return true;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) {
+        cudaGetLastError();  // an allocation that failed leaves no sticky error
+        return false;
+    }
+    cap = n;
+    return true;
+}
+
+// flags[b] = 1 for every block of the active list (within the grid), the scout's flags for the block
+// field's halo ownership
+__global__ void k_mark_active(ActiveView av, unsigned* __restrict__ flags, int nblocks) {
+    const int n = active_count(av);
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+        const int b = av.list[a];
+        if (b >= 0 && b < nblocks) flags[b] = 1u;
+    }
+}
+
+static FieldKey field_key(const sdf_grid& g, int n, float time) {
+    FieldKey k;
+    k.gv = grid_view(g);
+    k.sv = scene_view(g);
+    k.time = time;
+    k.list = g.d_activeBlocks;
+    k.count = g.d_activeBlockCount;
+    k.n = n;
+    return k;
+}
+
+// The block-field rows of the active list by the engine's shared-halo block field (every sample
+// evaluated once: own samples, then the halo samples no active block owns, then the copies), on the
+// legacy stream; with packet_counts also the per-cell vertex counts of countActiveBlockTriangles.
+// Returns false (nothing launched) when its working memory cannot be allocated; the caller then runs
+// the single-kernel field. The rows stay valid for the next launcher with the same key.
+static bool dropin_block_field(Scratch& s, const sdf_grid& g, int n, float time, unsigned* packet_counts) {
+    const GridView gv = grid_view(g);
+    const size_t nblocks = (size_t)gv.bx * gv.by * gv.bz;
+    s.rows_valid = false;
+    if (!ensure_flags(s, nblocks) || !ensure_buffer(s.b2a, s.b2a_cap, nblocks) ||
+        !ensure_buffer(s.miss, s.miss_cap, (size_t)n * HALO_N) ||
+        !ensure_buffer(s.rows, s.rows_cap, (size_t)n * FIELD_STRIDE))
+        return false;
+    const SceneView sv = scene_view(g);
+    ActiveView av{g.d_activeBlocks, g.d_activeBlockCount, n};
+    record(cudaMemsetAsync(s.flags, 0, nblocks * sizeof(unsigned), 0));
+    record(cudaMemsetAsync(s.tickets, 0, 8 * sizeof(unsigned), 0));
+    k_mark_active<<<std::max(1, std::min((n + 255) / 256, num_sms() * 8)), 256>>>(av, s.flags, (int)nblocks);
+    check_launch();
+    // tickets: 0 own samples, 4 listed halo samples, 5 count of listed halo samples
+    k_field_plan<<<num_sms() * 8, 256>>>(gv, av, s.flags, s.rows, s.b2a, s.miss, &s.tickets[5]);
+    check_launch();
+    k_field_own<false><<<persistent_grid(k_field_own<false>, BLK_THREADS, n), BLK_THREADS>>>(gv, sv, time, av, s.rows,
+                                                                                          &s.tickets[0], s.diag);
+    check_launch();
+    k_field_miss<false><<<persistent_grid(k_field_miss<false>, BLK_THREADS, 1 << 30), BLK_THREADS>>>(
+        gv, sv, time, av, s.rows, s.miss, &s.tickets[5], &s.tickets[4], s.diag);
+    check_launch();
+    k_field_gather<<<persistent_grid(k_field_gather, BLK_THREADS, (n + GATHER_WARPS - 1) / GATHER_WARPS), BLK_THREADS>>>(
+        gv, av, s.rows, s.b2a, s.flags, nullptr, packet_counts, nullptr);
+    check_launch();
+    s.rows_valid = true;
+    s.rows_key = field_key(g, n, time);
+    return true;
+}
+
+// the rows of the last dropin_block_field when they were computed for this grid, scene, time and list
+static const float* cached_rows(const Scratch& s, const sdf_grid& g, int n, float time) {
+    return s.rows_valid && same_key(s.rows_key, field_key(g, n, time)) ? s.rows : nullptr;
 }
 
 // ScanState over a caller- or library-owned region: word 0 is the ticket, words 1.. the tiles
@@ -189,6 +292,7 @@ void launchScoutActiveBlocks(sdf_grid* grid, float time) {
     const SceneView sv = scene_view(*grid);
     const size_t nblocks = (size_t)gv.bx * gv.by * gv.bz;
     Scratch& s = scratch();
+    s.rows_valid = false;  // the active list is rewritten
     if (!ensure_flags(s, nblocks) || !ensure_status(s, scan_tiles((unsigned)nblocks) + 1)) return;
     run_scout_compact(gv, sv, time, s.flags, s.status, grid->d_activeBlocks, grid->d_activeBlockCount, s.diag, 0);
 }
@@ -197,6 +301,8 @@ void launchCountActiveBlockTriangles(sdf_grid* grid, int numActiveBlocks, float 
     if (numActiveBlocks <= 0) return;
     std::lock_guard<std::mutex> lk(g_mutex);
     Scratch& s = scratch();
+    // the shared-halo block field; its rows serve the emission launcher that follows
+    if (dropin_block_field(s, *grid, numActiveBlocks, time, grid->d_packetVertexCounts)) return;
     ActiveView av{grid->d_activeBlocks, grid->d_activeBlockCount, numActiveBlocks};
     record(cudaMemsetAsync(s.tickets, 0, sizeof(unsigned), 0));
     k_mc_field<<<persistent_grid(k_mc_field, BLK_THREADS, numActiveBlocks), BLK_THREADS>>>(
@@ -232,8 +338,11 @@ void launchGenerateActiveBlockTriangles(sdf_grid* grid, int numActiveBlocks, flo
     Scratch& s = scratch();
     ActiveView av{grid->d_activeBlocks, grid->d_activeBlockCount, numActiveBlocks};
     record(cudaMemsetAsync(s.tickets, 0, sizeof(unsigned), 0));
+    // the rows of the counting launcher when it ran for this grid, scene, time and list (the reference's
+    // Update calls count, scan, emission in a row); otherwise the kernel evaluates each block's field
+    const float* rows = cached_rows(s, *grid, numActiveBlocks, time);
     k_mc_emit<<<persistent_grid(k_mc_emit, BLK_THREADS, numActiveBlocks), BLK_THREADS>>>(
-        grid_view(*grid), scene_view(*grid), time, av, nullptr, nullptr, grid->d_packetVertexOffsets, nullptr,
+        grid_view(*grid), scene_view(*grid), time, av, rows, nullptr, grid->d_packetVertexOffsets, nullptr,
         mesh_out_of(*grid), out_mask_of(*grid), s.tickets, s.diag);
     check_launch();
 }
@@ -291,9 +400,12 @@ void launchDCMarkCells(sdf_grid* grid, int numActiveBlocks, float time) {
     std::lock_guard<std::mutex> lk(g_mutex);
     Scratch& s = scratch();
     ActiveView av{grid->d_activeBlocks, grid->d_activeBlockCount, numActiveBlocks};
+    // the shared-halo block field, then the cells classified from the finished rows (kept for the solve)
+    const bool rows = dropin_block_field(s, *grid, numActiveBlocks, time, nullptr);
     record(cudaMemsetAsync(s.tickets, 0, sizeof(unsigned), 0));
     k_dc_mark<<<persistent_grid(k_dc_mark, BLK_THREADS, numActiveBlocks), BLK_THREADS>>>(
-        grid_view(*grid), scene_view(*grid), time, av, nullptr, dc_buffers_of(*grid), s.tickets, s.diag);
+        grid_view(*grid), scene_view(*grid), time, av, rows ? s.rows : nullptr, dc_buffers_of(*grid), s.tickets,
+        s.diag, rows);
     check_launch();
 }
 
@@ -311,8 +423,9 @@ void launchDCSolveCellVertices(sdf_grid* grid, int numActiveBlocks, float time, 
     sp.projection_iters = 0;
     sp.cond_threshold = 1e4f;
     const size_t smem = sizeof(SolveSmem);
+    const float* rows = cached_rows(s, *grid, numActiveBlocks, time);  // the marking launcher's rows
     k_dc_solve<<<persistent_grid(k_dc_solve, SOLVE_THREADS, numActiveBlocks, smem), SOLVE_THREADS, smem>>>(
-        grid_view(*grid), scene_view(*grid), time, av, nullptr, dc_buffers_of(*grid), sp, s.tickets, s.diag);
+        grid_view(*grid), scene_view(*grid), time, av, rows, dc_buffers_of(*grid), sp, s.tickets, s.diag);
     check_launch();
 }
 

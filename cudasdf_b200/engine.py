@@ -302,6 +302,17 @@ class Batch:
         sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
         L.check(self._lib.sdf_batch_capture(self.h, float(time), om, od, sp, 1 if tune else 0), "sdf_batch_capture")
 
+    def read_buffer(self, technique: int, which: int, dtype) -> np.ndarray:
+        """An internal array of one group's last extraction (see sdf_batch_read_buffer) on the host."""
+        n = ctypes.c_size_t(0)
+        L.check(self._lib.sdf_batch_read_buffer(self.h, int(technique), int(which), None, ctypes.byref(n)),
+                "sdf_batch_read_buffer")
+        out = np.zeros(n.value // np.dtype(dtype).itemsize, dtype)
+        n = ctypes.c_size_t(out.nbytes)
+        L.check(self._lib.sdf_batch_read_buffer(self.h, int(technique), int(which), out.ctypes.data,
+                                                ctypes.byref(n)), "sdf_batch_read_buffer")
+        return out
+
     def extract(self, mc: MeshBuffers, dc: MeshBuffers, time: float = 0.0, stream=None, allow_capacity=False):
         """Returns (first_vertex, vertex_count, stats); the counts are exact even when a buffer was too
         small (SDF_ERR_CAPACITY, raised unless allow_capacity)."""

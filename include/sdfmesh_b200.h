@@ -435,6 +435,14 @@ sdf_status sdf_batch_extract(sdf_batch* b, float time, const sdf_outputs* mc_out
  * tune = 0 skips the autotuner (occupancy-limited grids). */
 sdf_status sdf_batch_capture(sdf_batch* b, float time, const sdf_outputs* mc_out, const sdf_outputs* dc_out,
                              void* stream, int tune);
+/* Copies an internal array of the last extraction of one technique's group to host memory, for
+ * inspection (the scenes of a group number their blocks one after another in batch order, scene s
+ * owning [base_s, base_s + blocks_s)): 0 active list (int32 global block ids, ascending, so each scene's
+ * blocks are one run), 1 per-active-block vertex totals (uint32); dual contouring only: 2 per-cell quad
+ * vertex counts (uint32, 512 per active block), 3 corner masks (uint8, 512 per active block), 4 cell
+ * vertex offsets (uint32, 512 per active block, counted over the group), 5 cell vertices (ushort4).
+ * *bytes: in, the capacity of host_dst; out, the bytes the array holds (host_dst may be NULL to ask). */
+sdf_status sdf_batch_read_buffer(sdf_batch* b, int technique, int which, void* host_dst, size_t* bytes);
 
 /* Writes a mesh read back to HOST memory as Wavefront OBJ text, in the format of the reference's
  * ExportMeshToOBJ (src/main.cpp:1043-1115): "# Exported from CudaSDF", "# Generated: <file name>", a

@@ -137,7 +137,8 @@ def fp32_split_and_solve(P, N, m, cmin, cond_threshold=1e4):
     FP64 decision and of its FP32 branch (cudasdf_b200/csrc/qef_masspoint.cuh, solve_masspoint): mass
     point, unit normals, FP32 normal equations, Jacobi eigenvectors, eigenvalues as Rayleigh quotients
     of the unit normals, cond > cond_threshold -> FP64, and for the other cells three passes of
-    y += sum_k v_k (v_k . r) / l_k with r = sum_i n_i (n_i . ((p_i - c) - y)).
+    y += sum_k v_k (v_k . r) / l_k with r = sum_i n_i (n_i . ((p_i - c) - y)), summed with its rounding
+    errors carried (the kernel's acc2_rn).
 
     P: float32 Hermite points minus the cell corner (nc, 12, 3); N: float32 normals as the kernel holds
     them; m: sample counts; cmin: float32 cell corners (nc, 3). Returns (fp64 mask, float32 vertices of
@@ -169,10 +170,21 @@ def fp32_split_and_solve(P, N, m, cmin, cond_threshold=1e4):
         fp64 = ~(lmin * F32(cond_threshold) >= lmax)
         y = np.zeros((nc, 3), F32)
         for _ in range(3):
-            r = np.zeros((nc, 3), F32)
+            rh = np.zeros((nc, 3), F32)
+            rl = np.zeros((nc, 3), F32)
             for i in range(width):
                 e = _dot_rn(n[:, i], (P[:, i] - mq) - y)
-                r = np.where(ok[:, i, None], r + e[:, None] * n[:, i], r)
+                # acc2_rn: the product's rounding error (exact: the product of two floats is exact in
+                # float64) and the two-sum error of the addition go to rl
+                p = (n[:, i] * e[:, None]).astype(F32)
+                pe = (n[:, i].astype(np.float64) * e[:, None].astype(np.float64) - p.astype(np.float64)).astype(F32)
+                s = (rh + p).astype(F32)
+                bb = (s - rh).astype(F32)
+                err = ((rh - (s - bb)) + (p - bb)).astype(F32)
+                upd = ok[:, i, None]
+                rl = np.where(upd, (rl + (err + pe)).astype(F32), rl)
+                rh = np.where(upd, s, rh)
+            r = (rh + rl).astype(F32)
             for k in range(3):
                 v = V[:, :, k]
                 pos = lam[:, k] > 0

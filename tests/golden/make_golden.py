@@ -282,6 +282,61 @@ def run_pipeline(prims, res, technique, out_mask, t=0.0, qef_blend=1.0, max_vert
     return d
 
 
+def batch_digests(out_dir, count=256):
+    """Digests of the batched workload (scenes.batch_scenes: 256 scenes, primitive counts log-uniform in
+    [16, 2048], grids from {64, 96, 128, 192, 256}^3, half marching cubes, half dual contouring with the
+    reference's solver), each scene run alone through the reference's own CUDA path with a fresh mesh
+    object (CudaSDFMesh.cpp keeps process-wide allocation sizes, :301, :314), VBO + EBO outputs, sorted
+    active list. Per scene: primitive-record sha, active blocks, per-block vertex totals, per-cell count
+    and offset sha, VBO and EBO sha, and for dual contouring the corner-mask, cell-vertex-offset and
+    cell-vertex sha. Written to batch_c5.npz."""
+    scenes = S.batch_scenes(count)
+    cols = {k: [] for k in ("res", "technique", "nprims", "prims_sha", "active_count", "total_vertices",
+                            "counts_sha", "offsets_sha", "verts_sha", "indices_sha", "dc_mask_sha", "dc_voff_sha",
+                            "dc_vert_sha", "dc_vertices")}
+    actives, totals = [], []
+    for sc in scenes:
+        prims, res, tech = sc["primitives"], sc["resolution"], sc["technique"]
+        mesh = R.RefMesh(S.cell_size_for(res), max_vertices=24_000_000)
+        mesh.set_primitives(prims)
+        st = mesh.run(0.0, tech, 1.0, R.OUT_INDICES, sort_active=True)
+        nA, V = st["activeUsed"], st["totalVertices"]
+        counts = mesh.copy(R.RB_COUNTS, np.uint32, nA * 512)
+        offsets = mesh.copy(R.RB_OFFSETS, np.uint32, nA * 512)
+        verts = mesh.copy(R.RB_VERTS, np.float32, V * 4).reshape(V, 4)
+        indices = mesh.copy(R.RB_INDICES, np.uint32, V)
+        h = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()  # noqa: E731
+        cols["res"].append(res)
+        cols["technique"].append(tech)
+        cols["nprims"].append(len(prims))
+        cols["prims_sha"].append(h(prims))
+        cols["active_count"].append(nA)
+        cols["total_vertices"].append(V)
+        cols["counts_sha"].append(h(counts))
+        cols["offsets_sha"].append(h(offsets))
+        cols["verts_sha"].append(h(verts))
+        cols["indices_sha"].append(h(indices))
+        actives.append(mesh.copy(R.RB_ACTIVE, np.int32, nA))
+        totals.append(counts.reshape(nA, 512).sum(1).astype(np.uint32) if nA else np.zeros(0, np.uint32))
+        if tech == 1:
+            mask = mesh.copy(R.RB_DCMASK, np.uint8, nA * 512)
+            dvoff = mesh.copy(R.RB_DCVOFF, np.uint32, nA * 512)
+            nv = int(dvoff[-1] + (1 if mask[-1] not in (0, 255) else 0)) if nA else 0
+            cols["dc_mask_sha"].append(h(mask))
+            cols["dc_voff_sha"].append(h(dvoff))
+            cols["dc_vert_sha"].append(h(mesh.copy(R.RB_DCVERT, np.uint16, nv * 4)))
+            cols["dc_vertices"].append(nv)
+        else:
+            for k in ("dc_mask_sha", "dc_voff_sha", "dc_vert_sha"):
+                cols[k].append("")
+            cols["dc_vertices"].append(0)
+        mesh.close()
+    starts = np.concatenate([[0], np.cumsum([len(a) for a in actives])]).astype(np.int64)
+    np.savez_compressed(os.path.join(out_dir, "batch_c5.npz"), active=np.concatenate(actives).astype(np.int32),
+                        block_totals=np.concatenate(totals).astype(np.uint32), active_starts=starts,
+                        **{k: np.asarray(v) for k, v in cols.items()})
+
+
 def single_type_scene(t, n, seed):
     rng = np.random.default_rng(seed)
     p = S.random_scene(n, seed, size_range=(0.1, 0.35), center_range=0.6)
@@ -318,9 +373,14 @@ def main():
     ap.add_argument("--skip-full", action="store_true", help="skip the full-size digests")
     ap.add_argument("--only-odd", action="store_true", help="only the non-power-of-two grid fixtures")
     ap.add_argument("--only-types", action="store_true", help="only the per-primitive-type fixtures")
+    ap.add_argument("--only-batch", action="store_true", help="only the batched-workload digests")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     t0 = time.time()
+    if args.only_batch:
+        batch_digests(args.out)
+        print("done", time.time() - t0)
+        return
     # one marching-cubes run per primitive type: union scenes of that type only, random transforms,
     # annular / rounding shells on some primitives (pins the per-type arithmetic inside the reference's
     # 8-corner evaluation, which can contract differently than a lone map() call)

@@ -86,3 +86,85 @@ def test_batch_rejects_mixed_dc_options():
     with pytest.raises(RuntimeError):
         b.set_scenes(scenes, L.OUT_INDICES)
     b.close()
+
+
+def _sha(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def _exclusive(x):
+    out = np.zeros(len(x), np.uint64)
+    out[1:] = np.cumsum(x.astype(np.uint64))[:-1]
+    return out.astype(np.uint32)
+
+
+def test_batch_benchmark_workload_matches_reference_digests():
+    """The batched benchmark workload (256 scenes, primitive counts log-uniform in [16, 2048], grids from
+    {64, 96, 128, 192, 256}^3, half marching cubes, half dual contouring with the reference's solver),
+    extracted by the captured, autotuned graph, against digests of each scene run alone through the
+    reference's own CUDA path (tests/golden/batch_c5.npz): per scene the active blocks, per-block vertex
+    totals, VBO and EBO (as the scene's own identity indices), and for dual contouring the per-cell corner
+    masks, cell-vertex offsets, cell vertices and quad-vertex counts with their scan."""
+    import os
+
+    from conftest import GOLDEN
+    from cudasdf_b200 import _lib as L
+    from cudasdf_b200 import scenes as S
+    from cudasdf_b200.engine import Batch, MeshBuffers, make_config
+    path = os.path.join(GOLDEN, "batch_c5.npz")
+    if not os.path.exists(path):
+        pytest.skip("batch_c5.npz not generated")
+    G = np.load(path)
+    scn = S.batch_scenes(256)
+    scenes = [(sc["primitives"], make_config(S.cell_size_for(sc["resolution"]), technique=sc["technique"],
+                                             out_mask=L.OUT_INDICES)) for sc in scn]
+    for k, sc in enumerate(scn):  # the generator still draws the scenes the digests were made of
+        assert _sha(sc["primitives"]) == str(G["prims_sha"][k]) and sc["resolution"] == int(G["res"][k])
+    tot = G["total_vertices"].astype(np.int64)
+    tech = G["technique"]
+    mc = MeshBuffers(int(tot[tech == 0].sum()) + 1024, L.OUT_INDICES)
+    dc = MeshBuffers(int(tot[tech == 1].sum()) + 1024, L.OUT_INDICES)
+    b = Batch()
+    b.set_scenes(scenes, L.OUT_INDICES)
+    b.capture(mc, dc, tune=True)
+    first, count, st = b.extract(mc, dc)
+    assert st["graph"] == 1
+    lists = {t: b.read_buffer(t, 0, np.int32) for t in (0, 1)}
+    totals = {t: b.read_buffer(t, 1, np.uint32) for t in (0, 1)}
+    dcc = {"counts": b.read_buffer(1, 2, np.uint32), "mask": b.read_buffer(1, 3, np.uint8),
+           "voff": b.read_buffer(1, 4, np.uint32), "vert": b.read_buffer(1, 5, np.uint16).reshape(-1, 4)}
+    base = {0: 0, 1: 0}
+    cell_vertex_base = 0
+    bad = []
+    for k, sc in enumerate(scn):
+        t, res = int(tech[k]), sc["resolution"]
+        nblocks = ((res + 7) // 8) ** 3
+        lo, hi = base[t], base[t] + nblocks
+        base[t] = hi
+        lst = lists[t]
+        sel = np.nonzero((lst >= lo) & (lst < hi))[0]
+        a0, a1 = int(G["active_starts"][k]), int(G["active_starts"][k + 1])
+        ok = len(sel) == a1 - a0 == int(G["active_count"][k])
+        ok = ok and (sel.size == 0 or (np.diff(sel) == 1).all())  # one run of the sorted list
+        ok = ok and (lst[sel] - lo == G["active"][a0:a1]).all() and (totals[t][sel] == G["block_totals"][a0:a1]).all()
+        f, c = int(first[k]), int(count[k])
+        ok = ok and c == int(tot[k])
+        buf = dc if t else mc
+        ok = ok and _sha(buf.vertices[f:f + c].cpu().numpy()) == str(G["verts_sha"][k])
+        idx = buf.indices[f:f + c].cpu().numpy().astype(np.int64) - f
+        ok = ok and _sha(idx.astype(np.uint32)) == str(G["indices_sha"][k])
+        if t == 1 and sel.size:
+            c0, c1 = int(sel[0]) * 512, (int(sel[-1]) + 1) * 512
+            counts = dcc["counts"][c0:c1]
+            ok = ok and _sha(counts) == str(G["counts_sha"][k]) and _sha(_exclusive(counts)) == str(G["offsets_sha"][k])
+            ok = ok and _sha(dcc["mask"][c0:c1]) == str(G["dc_mask_sha"][k])
+            voff = dcc["voff"][c0:c1].astype(np.int64) - cell_vertex_base
+            ok = ok and _sha(voff.astype(np.uint32)) == str(G["dc_voff_sha"][k])
+            nv = int(G["dc_vertices"][k])
+            ok = ok and _sha(dcc["vert"][cell_vertex_base:cell_vertex_base + nv]) == str(G["dc_vert_sha"][k])
+            cell_vertex_base += nv
+        if not ok:
+            bad.append(k)
+    b.close()
+    assert not bad, f"{len(bad)} scenes differ from the reference: {bad[:20]}"
