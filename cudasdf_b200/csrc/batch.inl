@@ -196,6 +196,10 @@ struct BatchImpl {
     BatchGroup g[2];  // marching cubes, dual contouring
     int ctas[4] = {0, 0, 0, 0};
     cudaStream_t cap_stream = nullptr;
+    // the dual-contouring group runs on side_stream, concurrently with the marching-cubes group: the two
+    // groups share no data, so one group's small stages and tails overlap the other's heavy stages
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     sdf_outputs graph_out[2]{};
@@ -212,8 +216,28 @@ struct BatchImpl {
         g[0].release();
         g[1].release();
         if (cap_stream) cudaStreamDestroy(cap_stream);
+        if (side_stream) cudaStreamDestroy(side_stream);
+        if (fork_ev) cudaEventDestroy(fork_ev);
+        if (join_ev) cudaEventDestroy(join_ev);
     }
 };
+
+// both groups' kernels: marching cubes on st, dual contouring on the side stream forked from st and
+// joined back into it (in a capture this records two parallel branches of the graph)
+static void enqueue_both(BatchImpl& I, const BatchGrids& G, float time, const sdf_outputs* mc_out,
+                         const sdf_outputs* dc_out, cudaStream_t st) {
+    const bool both = I.g[0].n && I.g[1].n;
+    if (both) {
+        record(cudaEventRecord(I.fork_ev, st));
+        record(cudaStreamWaitEvent(I.side_stream, I.fork_ev, 0));
+    }
+    enqueue_group(I.g[0], G, time, mc_out, I.out_mask, st);
+    enqueue_group(I.g[1], G, time, dc_out, I.out_mask, both ? I.side_stream : st);
+    if (both) {
+        record(cudaEventRecord(I.join_ev, I.side_stream));
+        record(cudaStreamWaitEvent(st, I.join_ev, 0));
+    }
+}
 
 static bool same_outputs(const sdf_outputs* a, const sdf_outputs& b) {
     sdf_outputs z{};
@@ -334,7 +358,10 @@ sdf_status sdf_batch_create(sdf_batch** out, int device) {
     if (device >= 0 && cudaSetDevice(device) != cudaSuccess) return SDF_ERR_CUDA;
     sdf_batch* b = new sdf_batch();
     cudaGetDevice(&b->impl.device);
-    if (cudaStreamCreateWithFlags(&b->impl.cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&b->impl.cap_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->impl.side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->impl.fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->impl.join_ev, cudaEventDisableTiming) != cudaSuccess) {
         delete b;
         return SDF_ERR_CUDA;
     }
@@ -451,8 +478,7 @@ sdf_status sdf_batch_extract(sdf_batch* b, float time, const sdf_outputs* mc_out
         record(cudaGraphLaunch(I.exec, st));
     } else {
         const BatchGrids G = batch_grids(std::max(I.g[0].total_blocks, I.g[1].total_blocks), I.ctas);
-        enqueue_group(I.g[0], G, time, mc_out, I.out_mask, st);
-        enqueue_group(I.g[1], G, time, dc_out, I.out_mask, st);
+        enqueue_both(I, G, time, mc_out, dc_out, st);
     }
     const cudaError_t err = cudaStreamSynchronize(st);
     if (g_launch_failures != failures_before) return SDF_ERR_CUDA;  // a kernel was not launched
@@ -494,8 +520,7 @@ sdf_status sdf_batch_capture(sdf_batch* b, float time, const sdf_outputs* mc_out
                 float ms = 0.f;
                 for (int rep = 0; rep < 2; ++rep) {
                     cudaEventRecord(e0, st);
-                    enqueue_group(I.g[0], G, time, mc_out, I.out_mask, st);
-                    enqueue_group(I.g[1], G, time, dc_out, I.out_mask, st);
+                    enqueue_both(I, G, time, mc_out, dc_out, st);
                     cudaEventRecord(e1, st);
                     if (cudaStreamSynchronize(st) != cudaSuccess) {
                         cudaEventDestroy(e0);
@@ -516,8 +541,7 @@ sdf_status sdf_batch_capture(sdf_batch* b, float time, const sdf_outputs* mc_out
     }
     const BatchGrids G = batch_grids(blocks, I.ctas);  // attributes set before the capture
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return SDF_ERR_CUDA;
-    enqueue_group(I.g[0], G, time, mc_out, I.out_mask, st);
-    enqueue_group(I.g[1], G, time, dc_out, I.out_mask, st);
+    enqueue_both(I, G, time, mc_out, dc_out, st);
     if (cudaStreamEndCapture(st, &I.graph) != cudaSuccess || !I.graph) {
         I.graph = nullptr;
         cudaGetLastError();
