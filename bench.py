@@ -255,6 +255,20 @@ def run_ours(args, rank, world):
         times, st, out["stages"] = timed_extractions(eng, buf, args.steps, flush, world)
         out["surrogate"]["identical_mesh"] = bool(int(st["total_vertices"]) == V and
                                                   torch.equal(buf.vertices[:V], plain_verts))
+        # the method without the network: the exact map() at the coarse centres, the same reach, eps = 0
+        eng.set_coarse_cull(L.SDF_CULL_EXACT)
+        audit_x = eng.surrogate_audit(0.0)
+        for _ in range(args.warmup):
+            eng.extract(buf)
+        buf.vertices.zero_()
+        tx, stx, stages_x = timed_extractions(eng, buf, args.steps, flush, world)
+        ms_x = max_over_ranks(sum(tx) / len(tx), world)
+        out["exact_coarse"] = {"ms": ms_x, "value": job_throughput(world, voxels, ms_x), "stage_ms": stages_x,
+                               "audit": audit_x, "scouted_blocks": int(stx["scouted_blocks"]),
+                               "identical_mesh": bool(int(stx["total_vertices"]) == V and
+                                                      torch.equal(buf.vertices[:V], plain_verts))}
+        # back to the culling the timed value used
+        eng.set_coarse_cull(L.SDF_CULL_SURROGATE if audit["violations"] == 0 else L.SDF_CULL_NONE)
         del plain_verts
     else:
         out["stages"] = out["plain_stages"]
@@ -814,6 +828,13 @@ def main():
                              "train_ms": {"samples": sg["train"]["ms_samples"], "train": sg["train"]["ms_train"],
                                           "certify": sg["train"]["ms_certify"], "wall": sg["train_wall_ms"]},
                              "fallback": sg.get("fallback")}
+        if "exact_coarse" in r:
+            x = r["exact_coarse"]
+            line["surrogate"]["without_network"] = {
+                "method": "exact map() at every 32^3 coarse centre, same reach, eps = 0 (SDF_CULL_EXACT)",
+                "value": x["value"], "ms_per_step": x["ms"], "stage_ms": x["stage_ms"], "audit": x["audit"],
+                "scouted_blocks": x["scouted_blocks"], "identical_mesh": x["identical_mesh"],
+                "network_gain": r["value"] / x["value"]}
     if "e2e" in r:
         line["e2e"] = r["e2e"]
     line["roofline"] = roofline(r)

@@ -102,7 +102,8 @@ DROPIN_SYMBOLS = ["launchScoutActiveBlocks", "launchCountActiveBlockTriangles", 
                   "launchBuildBlockToActiveMap", "launchDCMarkCells", "launchDCSolveCellVertices",
                   "launchDCRecomputeNormalsAtVertices", "launchDCSmoothCellNormals", "launchDCCountQuads",
                   "launchDCGenerateQuads", "getScanStorageSize", "launchScan"]
-SURROGATE_SYMBOLS = ["sdf_surrogate_default_config", "sdf_surrogate_train", "sdf_surrogate_enable",
+SDF_CULL_NONE, SDF_CULL_SURROGATE, SDF_CULL_EXACT = 0, 1, 2
+SURROGATE_SYMBOLS = ["sdf_engine_set_coarse_cull", "sdf_surrogate_default_config", "sdf_surrogate_train", "sdf_surrogate_enable",
                      "sdf_surrogate_audit", "sdf_surrogate_num_params", "sdf_surrogate_set_params",
                      "sdf_surrogate_get_params", "sdf_surrogate_forward", "sdf_surrogate_gradient"]
 BATCH_SYMBOLS = ["sdf_batch_create", "sdf_batch_destroy", "sdf_batch_set_scenes", "sdf_batch_extract",
@@ -189,6 +190,8 @@ def lib():
     L.sdf_surrogate_train.restype = i
     L.sdf_surrogate_enable.argtypes = [vp, i]
     L.sdf_surrogate_enable.restype = i
+    L.sdf_engine_set_coarse_cull.argtypes = [vp, i]
+    L.sdf_engine_set_coarse_cull.restype = i
     i64p = ctypes.POINTER(ctypes.c_int64)
     L.sdf_surrogate_audit.argtypes = [vp, f, i64p, i64p, i64p]
     L.sdf_surrogate_audit.restype = i

@@ -40,6 +40,7 @@ struct SurrogateState {
     bool has_params = false;
     bool certified = false;
     bool enabled = false;
+    bool exact_coarse = false;      // cull by the exact map() at the coarse centres, not by f_net
     float eps = 0.f;
     float slack_cells = 2.f;
 
@@ -225,7 +226,11 @@ static float surrogate_reach(const EngineImpl& E, float slack_cells) {
     return 0.5f * (float)SUR_SPAN_CELLS * 1.7320508f * cell + r_scout + slack_cells * cell;
 }
 
-static float surrogate_margin(const EngineImpl& E) { return E.sur->eps + surrogate_reach(E, E.sur->slack_cells); }
+// the cull threshold on |f| at a coarse centre: the certified error plus the reach, or the reach alone
+// when the coarse field is the exact map()
+static float surrogate_margin(const EngineImpl& E) {
+    return (E.sur->exact_coarse ? 0.f : E.sur->eps) + surrogate_reach(E, E.sur->slack_cells);
+}
 
 // the block field with shared halos (plan -> evaluation -> gather, see mc_kernels.cuh) and the block totals
 template <bool COUNT>
@@ -263,8 +268,35 @@ static void coarse_dims(const EngineImpl& E, int& cx, int& cy, int& cz) {
     cz = (E.gv.bz + SUR_SPAN_BLOCKS - 1) / SUR_SPAN_BLOCKS;
 }
 
-// f_net at the coarse block centres into E.sur->coarse_f
-static sdf_status surrogate_coarse_eval(EngineImpl& E, cudaStream_t st) {
+static sdfb::SceneView engine_scene_view(EngineImpl& E) {
+    sdfb::SceneView sv;
+    sv.prims = reinterpret_cast<const float4*>(E.d_prims);
+    sv.nodes = reinterpret_cast<const float4*>(E.d_nodes);
+    sv.nprims = E.nprims;
+    sv.nbvh = E.nbvh;
+    sv.nnodes = E.nnodes;
+    return sv;
+}
+
+// the exact map() at the coarse block centres (the culling without the network)
+__global__ void __launch_bounds__(sdfb::BLK_THREADS) k_coarse_exact(sdfb::SceneView sc, sur::CoarseCentres cc,
+                                                                     float time, float* __restrict__ out,
+                                                                     sdfb::Diag* diag) {
+    using namespace sdfb;
+    const int warps_total = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < cc.n; base += warps_total * 32) {
+        const int i = base + lane;
+        const bool valid = i < cc.n;
+        const float3 p = valid ? cc(i) : f3(0.f, 0.f, 0.f);
+        MapState<false> st;
+        map_warp<false>(sc, p, valid, time, st, diag);
+        if (valid) out[i] = st.d;
+    }
+}
+
+// f_net (or, in the exact mode, map()) at the coarse block centres into E.sur->coarse_f
+static sdf_status surrogate_coarse_eval(EngineImpl& E, cudaStream_t st, float time = 0.f) {
     using namespace sdfb;
     SurrogateState& S = *E.sur;
     int cx, cy, cz;
@@ -278,6 +310,13 @@ static sdf_status surrogate_coarse_eval(EngineImpl& E, cudaStream_t st) {
     cc.ox = E.gv.ox; cc.oy = E.gv.oy; cc.oz = E.gv.oz; cc.cell = E.gv.cell;
     cc.cx = cx; cc.cy = cy; cc.cz = cz; cc.span = SUR_SPAN_CELLS;
     cc.n = (int)nc;
+    if (S.exact_coarse) {
+        const int warps = (int)((nc + 31) / 32);
+        k_coarse_exact<<<std::max(1, std::min((warps + 7) / 8, num_sms() * 8)), BLK_THREADS, 0, st>>>(
+            engine_scene_view(E), cc, time, S.coarse_f, &reinterpret_cast<Ctrl*>(E.ctrl_region)->diag);
+        check_launch();
+        return SDF_OK;
+    }
     const size_t smem = sizeof(sur::InferSmem);
     const int tiles = (int)((nc + sur::TILE - 1) / sur::TILE);
     sur::k_sur_infer<sur::CoarseCentres><<<persistent_grid(sur::k_sur_infer<sur::CoarseCentres>, sur::TILE, tiles, smem),
@@ -291,7 +330,7 @@ static void run_culled_scout_compact(EngineImpl& E, const sdfb::SceneView& sv, f
                                      sdfb::Ctrl* ctrl, cudaStream_t st) {
     using namespace sdfb;
     const GridView& gv = E.gv;
-    surrogate_coarse_eval(E, st);
+    surrogate_coarse_eval(E, st, time);
     const int nbricks = ((gv.bx + 3) / 4) * ((gv.by + 3) / 4) * ((gv.bz + 1) / 2);
     const int warps_per_cta = BLK_THREADS / 32;
     k_scout_t<true><<<(nbricks + warps_per_cta - 1) / warps_per_cta, BLK_THREADS, 0, st>>>(
@@ -396,7 +435,10 @@ static sdf_status scene_prepare(EngineImpl& E, const sdf_primitive* prims, int c
                       memcmp(E.scene.data(), prims, (size_t)count * sizeof(sdf_primitive)) == 0;
     if (!same) {
         E.scene.assign(prims, prims + count);
-        if (E.sur) E.sur->certified = E.sur->enabled = false;  // a new scene needs a new surrogate
+        if (E.sur) {  // a new scene needs a new surrogate; the exact coarse culling stays valid
+            E.sur->certified = false;
+            if (!E.sur->exact_coarse) E.sur->enabled = false;
+        }
         E.nbvh = sdfb::prepare_scene(prims, count, E.sorted, E.nodes);
         E.depth = sdfb::bvh_depth(E.nodes);
         ++E.scene_gen;
@@ -491,7 +533,10 @@ sdf_status sdf_engine_set_scene_device(sdf_engine* e, const sdf_primitive* prims
     E.scene.clear();
     E.sorted.clear();
     E.nodes.clear();
-    if (E.sur) E.sur->certified = E.sur->enabled = false;
+    if (E.sur) {
+        E.sur->certified = false;
+        if (!E.sur->exact_coarse) E.sur->enabled = false;
+    }
     E.nprims = E.nbvh = E.nnodes = E.depth = 0;
     E.device_scene = true;
     if (count == 0) return SDF_OK;
@@ -877,16 +922,6 @@ const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes) {
     }
     if (bytes) *bytes = b;
     return p;
-}
-
-static sdfb::SceneView engine_scene_view(EngineImpl& E) {
-    sdfb::SceneView sv;
-    sv.prims = reinterpret_cast<const float4*>(E.d_prims);
-    sv.nodes = reinterpret_cast<const float4*>(E.d_nodes);
-    sv.nprims = E.nprims;
-    sv.nbvh = E.nbvh;
-    sv.nnodes = E.nnodes;
-    return sv;
 }
 
 sdf_status sdf_engine_eval_normals(sdf_engine* e, const float* d_points, int n, float time, float cell,

@@ -402,7 +402,27 @@ sdf_status sdf_surrogate_enable(sdf_engine* e, int enabled) {
     if (!e) return SDF_ERR_INVALID;
     EngineImpl& E = e->impl;
     if (enabled && (!E.sur || !E.sur->certified)) return SDF_ERR_INVALID;
-    if (E.sur) E.sur->enabled = enabled != 0;
+    if (E.sur) {
+        E.sur->enabled = enabled != 0;
+        E.sur->exact_coarse = false;
+    }
+    return SDF_OK;
+}
+
+sdf_status sdf_engine_set_coarse_cull(sdf_engine* e, int mode) {
+    using namespace sdfb;
+    if (!e || mode < SDF_CULL_NONE || mode > SDF_CULL_EXACT) return SDF_ERR_INVALID;
+    EngineImpl& E = e->impl;
+    if (mode == SDF_CULL_SURROGATE) return sdf_surrogate_enable(e, 1);
+    if (mode == SDF_CULL_NONE) {
+        if (E.sur) E.sur->enabled = E.sur->exact_coarse = false;
+        return SDF_OK;
+    }
+    cudaSetDevice(E.device);
+    const sdf_status s = surrogate_state(E);  // the coarse-field buffer and the audit counters
+    if (s != SDF_OK) return s;
+    E.sur->exact_coarse = true;
+    E.sur->enabled = true;
     return SDF_OK;
 }
 
@@ -410,7 +430,7 @@ sdf_status sdf_surrogate_audit(sdf_engine* e, float time, int64_t* violations, i
     using namespace sdfb;
     if (!e) return SDF_ERR_INVALID;
     EngineImpl& E = e->impl;
-    if (!E.configured || !E.sur || !E.sur->certified) return SDF_ERR_INVALID;
+    if (!E.configured || !E.sur || !(E.sur->certified || E.sur->exact_coarse)) return SDF_ERR_INVALID;
     cudaSetDevice(E.device);
     SurrogateState& S = *E.sur;
     Ctrl* ctrl = reinterpret_cast<Ctrl*>(E.ctrl_region);
@@ -420,7 +440,7 @@ sdf_status sdf_surrogate_audit(sdf_engine* e, float time, int64_t* violations, i
     const int nbricks = ((gv.bx + 3) / 4) * ((gv.by + 3) / 4) * ((gv.bz + 1) / 2);
     k_scout_t<false><<<(nbricks + BLK_THREADS / 32 - 1) / (BLK_THREADS / 32), BLK_THREADS>>>(gv, sv, time, E.flags,
                                                                                             &ctrl->diag, nullptr, 0.f);
-    sdf_status s = surrogate_coarse_eval(E, 0);
+    sdf_status s = surrogate_coarse_eval(E, 0, time);
     if (s != SDF_OK) return s;
     int cx, cy, cz;
     coarse_dims(E, cx, cy, cz);

@@ -371,9 +371,19 @@ void sdf_surrogate_default_config(sdf_surrogate_config* cfg);
 sdf_status sdf_surrogate_train(sdf_engine* e, const sdf_surrogate_config* cfg, sdf_surrogate_stats* stats);
 /* Turns surrogate culling in sdf_engine_extract on or off (SDF_ERR_INVALID if not trained). */
 sdf_status sdf_surrogate_enable(sdf_engine* e, int enabled);
-/* Exact audit: a full exact scout at `time`; *violations = exact-active blocks inside culled coarse
- * blocks (0 means the culled extraction equals the plain one), *culled = culled coarse blocks,
- * *coarse = all coarse blocks. Synchronous. */
+/* Coarse-block culling of sdf_engine_extract: SDF_CULL_NONE, SDF_CULL_SURROGATE (f_net with the
+ * certified margin eps + K; as sdf_surrogate_enable(e, 1)) or SDF_CULL_EXACT, the method without the
+ * network: the exact map() at each coarse centre, one evaluation per 32^3 cells, culled when
+ * |f| > K (the reach above with eps = 0; the field of smooth-blended, pruned primitives is not
+ * 1-Lipschitz, so the audit below is the judge here too). The exact mode needs no training and stays
+ * on across scene changes. */
+#define SDF_CULL_NONE 0
+#define SDF_CULL_SURROGATE 1
+#define SDF_CULL_EXACT 2
+sdf_status sdf_engine_set_coarse_cull(sdf_engine* e, int mode);
+/* Exact audit of the current culling (surrogate or exact coarse field): a full exact scout at `time`;
+ * *violations = exact-active blocks inside culled coarse blocks (0 means the culled extraction equals
+ * the plain one), *culled = culled coarse blocks, *coarse = all coarse blocks. Synchronous. */
 sdf_status sdf_surrogate_audit(sdf_engine* e, float time, int64_t* violations, int64_t* culled, int64_t* coarse);
 /* Number of trainable parameters (hidden W[4][64][64] out x in, b[4][64], w5[64], b5). */
 int sdf_surrogate_num_params(void);

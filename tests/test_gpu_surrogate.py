@@ -96,3 +96,43 @@ def test_training_culls_and_keeps_the_mesh():
     with pytest.raises(RuntimeError):
         eng.surrogate_enable(True)
     eng.close()
+
+
+def test_network_against_the_method_without_it():
+    """What the trained network gains over culling without it. The method without the network evaluates
+    the exact map() at every 32^3 coarse centre and culls with the same reach and eps = 0
+    (SDF_CULL_EXACT); the surrogate evaluates f_net on tensor cores and culls with eps_cert + reach. Both
+    must keep the plain mesh (audit 0, identical vertices); the test reports the coarse blocks each culls
+    and the blocks each leaves to the exact scout (the time is in the bench line)."""
+    from cudasdf_b200 import _lib as L
+    from cudasdf_b200 import scenes as S
+    from cudasdf_b200.engine import Engine, MeshBuffers, make_config
+    eng = Engine()
+    eng.configure(make_config(S.cell_size_for(1024), out_mask=L.OUT_INDICES))
+    eng.set_scene(S.config_scene(4))
+    buf = MeshBuffers(8_000_000, L.OUT_INDICES)
+    plain = eng.extract(buf, 0.0)
+    V = plain["total_vertices"]
+    h_plain = hashlib.sha256(buf.vertices[:V].cpu().numpy().tobytes()).hexdigest()
+    res = {}
+    eng.set_coarse_cull(L.SDF_CULL_EXACT)  # no training needed
+    res["exact"] = eng.surrogate_audit(0.0)
+    buf.vertices.zero_()
+    st = eng.extract(buf, 0.0)
+    res["exact"]["scouted_blocks"] = st["scouted_blocks"]
+    assert res["exact"]["violations"] == 0 and st["total_vertices"] == V
+    assert hashlib.sha256(buf.vertices[:V].cpu().numpy().tobytes()).hexdigest() == h_plain
+    eng.surrogate_train()
+    eng.set_coarse_cull(L.SDF_CULL_SURROGATE)
+    res["surrogate"] = eng.surrogate_audit(0.0)
+    buf.vertices.zero_()
+    st = eng.extract(buf, 0.0)
+    res["surrogate"]["scouted_blocks"] = st["scouted_blocks"]
+    assert res["surrogate"]["violations"] == 0 and st["total_vertices"] == V
+    assert hashlib.sha256(buf.vertices[:V].cpu().numpy().tobytes()).hexdigest() == h_plain
+    # the exact coarse field is the sharper cull (eps = 0 against eps_cert > 0)
+    assert res["exact"]["culled_coarse"] >= res["surrogate"]["culled_coarse"]
+    eng.set_coarse_cull(L.SDF_CULL_NONE)
+    assert eng.extract(buf, 0.0)["scouted_blocks"] == plain["scouted_blocks"]
+    print("coarse culling at 1024^3:", res, "plain scouted", plain["scouted_blocks"])
+    eng.close()
