@@ -190,7 +190,7 @@ def lib():
     L.sdf_surrogate_train.restype = i
     L.sdf_surrogate_enable.argtypes = [vp, i]
     L.sdf_surrogate_enable.restype = i
-    L.sdf_engine_set_coarse_cull.argtypes = [vp, i]
+    L.sdf_engine_set_coarse_cull.argtypes = [vp, i, f]
     L.sdf_engine_set_coarse_cull.restype = i
     i64p = ctypes.POINTER(ctypes.c_int64)
     L.sdf_surrogate_audit.argtypes = [vp, f, i64p, i64p, i64p]

@@ -138,7 +138,7 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
         k_field_gather<<<G.gather, BLK_THREADS, 0, st>>>(g0, av, B.fields, B.b2a, B.flags, B.block_totals, nullptr,
                                                          flat ? B.cell_words : nullptr);
         k_exclusive_scan<<<std::max(1u, scan_tiles(nb)), SCAN_THREADS, 0, st>>>(
-            B.block_totals, B.block_offsets, 0, &ctrl->active_count, 1, scan_state(B.scan(B.scanB_off)),
+            B.block_totals, B.block_offsets, nb, &ctrl->active_count, 1, scan_state(B.scan(B.scanB_off)),
             &ctrl->total_vertices, diag);
         if (flat)
             k_mc_emit_cells<<<G.emit_cells, EMIT_WARPS * 32, 0, st>>>(g0, av, B.fields, B.cell_words, B.block_offsets,
@@ -167,7 +167,7 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
         k_field_gather<<<G.gather, BLK_THREADS, 0, st>>>(g0, av, B.fields, B.b2a, B.flags, nullptr, nullptr, nullptr);
         k_dc_mark<<<G.mark, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, D, &ctrl->tickets[0], diag, true);
         k_exclusive_scan<<<std::max(1u, scan_tiles(nb * 512u)), SCAN_THREADS, 0, st>>>(
-            B.packet_counts, B.dc_voff, 0, &ctrl->active_count, 512, scan_state(B.scan(B.scanC_off)),
+            B.packet_counts, B.dc_voff, nb, &ctrl->active_count, 512, scan_state(B.scan(B.scanC_off)),
             &ctrl->dc_vertices, diag);
         DcSolveParams sp = B.sp;
         sp.max_cell_vertices = (unsigned)B.dc_cap;
@@ -175,7 +175,7 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
                                                                     &ctrl->tickets[1], diag);
         k_dc_count_quads<<<G.count_quads, 512, 0, st>>>(g0, av, D, B.packet_counts, B.block_totals);
         k_exclusive_scan<<<std::max(1u, scan_tiles(nb)), SCAN_THREADS, 0, st>>>(
-            B.block_totals, B.block_offsets, 0, &ctrl->active_count, 1, scan_state(B.scan(B.scanB_off)),
+            B.block_totals, B.block_offsets, nb, &ctrl->active_count, 1, scan_state(B.scan(B.scanB_off)),
             &ctrl->total_vertices, diag);
         k_dc_quads<<<G.quads, BLK_THREADS, sizeof(QuadSmem), st>>>(g0, sc0, time, av, D, nullptr, B.packet_counts,
                                                                    B.block_offsets, mo, m, B.qp, &ctrl->tickets[2],

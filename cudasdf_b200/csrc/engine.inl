@@ -41,6 +41,7 @@ struct SurrogateState {
     bool certified = false;
     bool enabled = false;
     bool exact_coarse = false;      // cull by the exact map() at the coarse centres, not by f_net
+    float exact_extra = 0.f;        // the exact mode's margin beyond the reach
     float eps = 0.f;
     float slack_cells = 2.f;
 
@@ -118,10 +119,15 @@ struct EngineImpl {
         uint64_t ticket = 0;
         cudaEvent_t done = nullptr;
         int nb = 0;
+        int rows_cap = 0;                  // active blocks the per-block buffers held
         bool dc = false, welded = false, culled = false;
         uint32_t max_vertices = 0;
         size_t dc_cap = 0;
         std::chrono::high_resolution_clock::time_point t0;
+        // what to run again when the extraction finds more active blocks than rows_cap
+        sdf_outputs out{};
+        float time = 0.f;
+        cudaStream_t stream = nullptr;
     };
     static constexpr int ASYNC_SLOTS = 4;
     Pending pend[ASYNC_SLOTS];
@@ -137,6 +143,9 @@ struct EngineImpl {
     uint64_t image_gen = ~0ull;            // the build the pinned image holds
     bool timing = false;
     int debug = 0;
+    // active blocks the per-active-block buffers hold (block-field rows, halo-miss list, cell words,
+    // per-cell DC arrays, weld bitmaps); grown after an extraction that found more (engine_grow_rows)
+    int rows_cap = 0;
     cudaEvent_t ev[8] = {};
     size_t packet_cap = 0;
     unsigned* miss = nullptr;          // listed halo samples, capacity nblocks * HALO_N
@@ -229,7 +238,7 @@ static float surrogate_reach(const EngineImpl& E, float slack_cells) {
 // the cull threshold on |f| at a coarse centre: the certified error plus the reach, or the reach alone
 // when the coarse field is the exact map()
 static float surrogate_margin(const EngineImpl& E) {
-    return (E.sur->exact_coarse ? 0.f : E.sur->eps) + surrogate_reach(E, E.sur->slack_cells);
+    return (E.sur->exact_coarse ? E.sur->exact_extra : E.sur->eps) + surrogate_reach(E, E.sur->slack_cells);
 }
 
 // the block field with shared halos (plan -> evaluation -> gather, see mc_kernels.cuh) and the block totals
@@ -238,7 +247,7 @@ static sdf_status run_block_field(EngineImpl& E, const sdfb::SceneView& sv, floa
                                   sdfb::Ctrl* ctrl, unsigned* packet_counts, cudaStream_t st,
                                   unsigned* cell_words = nullptr, bool counts = true) {
     using namespace sdfb;
-    const size_t need = (size_t)E.nblocks * HALO_N;
+    const size_t need = (size_t)E.rows_cap * HALO_N;
     if (E.miss_cap < need) {
         if (dev_alloc(E.miss, need) != SDF_OK) {
             E.miss_cap = 0;
@@ -248,13 +257,13 @@ static sdf_status run_block_field(EngineImpl& E, const sdfb::SceneView& sv, floa
     }
     k_field_plan<<<num_sms() * 8, 256, 0, st>>>(E.gv, av, E.flags, E.fields, E.b2a, E.miss, &ctrl->halo_misses);
     check_launch();
-    k_field_own<COUNT><<<persistent_grid(k_field_own<COUNT>, BLK_THREADS, E.nblocks), BLK_THREADS, 0, st>>>(
+    k_field_own<COUNT><<<persistent_grid(k_field_own<COUNT>, BLK_THREADS, E.rows_cap), BLK_THREADS, 0, st>>>(
         E.gv, sv, time, av, E.fields, &ctrl->tickets[0], &ctrl->diag);
     check_launch();
     k_field_miss<COUNT><<<persistent_grid(k_field_miss<COUNT>, BLK_THREADS, 1 << 30), BLK_THREADS, 0, st>>>(
         E.gv, sv, time, av, E.fields, E.miss, &ctrl->halo_misses, &ctrl->tickets[4], &ctrl->diag);
     check_launch();
-    k_field_gather<<<persistent_grid(k_field_gather, BLK_THREADS, (E.nblocks + GATHER_WARPS - 1) / GATHER_WARPS),
+    k_field_gather<<<persistent_grid(k_field_gather, BLK_THREADS, (E.rows_cap + GATHER_WARPS - 1) / GATHER_WARPS),
                      BLK_THREADS, 0, st>>>(E.gv, av, E.fields, E.b2a, E.flags,
                                            (COUNT || !counts) ? nullptr : E.block_totals, packet_counts, cell_words);
     check_launch();
@@ -412,8 +421,13 @@ sdf_status sdf_engine_configure(sdf_engine* e, const sdf_config* cfg) {
     if (s == SDF_OK) s = sdfb::dev_alloc(E.block_totals, nb);
     if (s == SDF_OK) s = sdfb::dev_alloc(E.block_offsets, nb);
     if (s == SDF_OK) s = sdfb::dev_alloc(E.b2a, nb);
-    if (s == SDF_OK) s = sdfb::dev_alloc(E.fields, (size_t)nb * sdfb::FIELD_STRIDE);
+    // the per-active-block buffers start at a sixteenth of the blocks (a surface touches a few percent
+    // of them) and grow when an extraction finds more active blocks
+    E.rows_cap = (int)std::min<long long>(nb, std::max<long long>(4096, nb / 16));
+    if (s == SDF_OK) s = sdfb::dev_alloc(E.fields, (size_t)E.rows_cap * sdfb::FIELD_STRIDE);
     if (s != SDF_OK) return s;
+    // a block's map entry is read only where its scout flag is set; blocks past rows_cap keep -1
+    cudaMemset(E.b2a, 0xFF, (size_t)nb * sizeof(int));
     // control block + scan regions (word 0 of a region is its ticket)
     const size_t tA = sdfb::scan_tiles((unsigned)nb) + 1;
     const size_t tC = sdfb::scan_tiles((unsigned)(nb * 512)) + 1;
@@ -637,12 +651,13 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
     const unsigned failures_before = g_launch_failures;
     const sdf_config& C = E.cfg;
     const bool dc = C.technique == SDF_TECH_DUAL_CONTOURING;
+    const int cap = E.rows_cap;  // active blocks the per-block buffers hold
     if (dc || (E.debug & 1)) {
-        const sdf_status s = engine_ensure_packets(E, (size_t)E.nblocks * 512);
+        const sdf_status s = engine_ensure_packets(E, (size_t)cap * 512);
         if (s != SDF_OK) return s;
     }
     if (dc) {
-        const size_t want = std::min<size_t>((size_t)E.nblocks * 512, (size_t)1 << 28);
+        const size_t want = std::min<size_t>((size_t)cap * 512, (size_t)1 << 28);
         if (E.dc_cap < want) {
             if (dev_alloc(E.dc_verts, want) != SDF_OK || dev_alloc(E.dc_norms, want) != SDF_OK) return SDF_ERR_NOMEM;
             E.dc_cap = want;
@@ -678,7 +693,7 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
     else if (run_scout_compact(gv, sv, time, E.flags, scanA, E.list, &ctrl->active_count, diag, st) != cudaSuccess)
         return SDF_ERR_CUDA;
     if (E.timing) cudaEventRecord(E.ev[1], st);
-    ActiveView av{E.list, &ctrl->active_count, nb};
+    ActiveView av{E.list, &ctrl->active_count, cap};  // the kernels take at most cap active blocks
     MeshOut mo;
     mo.verts = reinterpret_cast<float4*>(out->vertices);
     mo.colors = reinterpret_cast<float4*>(out->colors);
@@ -700,27 +715,28 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
     if (!dc) {
         // positions and indices only (no per-cell debug layout): the flat per-cell emission
         const bool flat = !(mask & (OUT_COLORS | OUT_UVS | OUT_PRIMIDS | OUT_NORMALS)) && (!(E.debug & 1) || welded);
-        if (welded && E.weld_cap < (size_t)nb) {
+        if (welded && E.weld_cap < (size_t)cap) {
             E.weld_cap = 0;
-            if (dev_alloc(E.weld_bits, (size_t)nb * WELD_STRIDE) != SDF_OK ||
-                dev_alloc(E.weld_prefix, (size_t)nb * WELD_STRIDE) != SDF_OK ||
-                dev_alloc(E.weld_totals, (size_t)nb) != SDF_OK || dev_alloc(E.weld_base, (size_t)nb) != SDF_OK)
+            if (dev_alloc(E.weld_bits, (size_t)cap * WELD_STRIDE) != SDF_OK ||
+                dev_alloc(E.weld_prefix, (size_t)cap * WELD_STRIDE) != SDF_OK ||
+                dev_alloc(E.weld_totals, (size_t)cap) != SDF_OK || dev_alloc(E.weld_base, (size_t)cap) != SDF_OK)
                 return SDF_ERR_NOMEM;
-            E.weld_cap = (size_t)nb;
+            E.weld_cap = (size_t)cap;
         }
-        if (flat && E.cell_words_cap < (size_t)nb * 512) {
-            if (dev_alloc(E.cell_words, (size_t)nb * 512) != SDF_OK) {
+        if (flat && E.cell_words_cap < (size_t)cap * 512) {
+            if (dev_alloc(E.cell_words, (size_t)cap * 512) != SDF_OK) {
                 E.cell_words_cap = 0;
                 return SDF_ERR_NOMEM;
             }
-            E.cell_words_cap = (size_t)nb * 512;
+            E.cell_words_cap = (size_t)cap * 512;
         }
         if (run_block_field<false>(E, sv, time, av, ctrl, (E.debug & 1) ? E.packet_counts : nullptr, st,
                                    flat ? E.cell_words : nullptr) != SDF_OK)
             return SDF_ERR_NOMEM;
         if (E.timing) cudaEventRecord(E.ev[2], st);
-        k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)nb)), SCAN_THREADS, 0, st>>>(
-            E.block_totals, E.block_offsets, 0, &ctrl->active_count, 1, scan_state(scanB), &ctrl->total_vertices, diag);
+        k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)cap)), SCAN_THREADS, 0, st>>>(
+            E.block_totals, E.block_offsets, (unsigned)cap, &ctrl->active_count, 1, scan_state(scanB),
+            &ctrl->total_vertices, diag);
         check_launch();
         if (E.timing) cudaEventRecord(E.ev[3], st);
         if (welded) {
@@ -731,13 +747,14 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
             wb.base = E.weld_base;
             wb.flags = E.flags;
             wb.block_to_active = E.b2a;
-            const int wblocks = (nb + WELD_WARPS - 1) / WELD_WARPS;
+            const int wblocks = (cap + WELD_WARPS - 1) / WELD_WARPS;
             k_weld_mark<<<persistent_grid(k_weld_mark, WELD_WARPS * 32, wblocks), WELD_WARPS * 32, 0, st>>>(gv, av,
                                                                                                      E.fields, wb);
             check_launch();
             unsigned long long* scanD = reinterpret_cast<unsigned long long*>(E.ctrl_region + E.scanD_off);
-            k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)nb)), SCAN_THREADS, 0, st>>>(
-                E.weld_totals, E.weld_base, 0, &ctrl->active_count, 1, scan_state(scanD), &ctrl->welded_vertices, diag);
+            k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)cap)), SCAN_THREADS, 0, st>>>(
+                E.weld_totals, E.weld_base, (unsigned)cap, &ctrl->active_count, 1, scan_state(scanD),
+                &ctrl->welded_vertices, diag);
             check_launch();
             k_weld_vertices<<<persistent_grid(k_weld_vertices, WELD_WARPS * 32, wblocks), WELD_WARPS * 32, 0, st>>>(
                 gv, av, E.fields, wb, mo.verts, mo.maxV);
@@ -745,11 +762,11 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
             k_weld_indices<<<persistent_grid(k_weld_indices, WELD_WARPS * 32, wblocks), WELD_WARPS * 32, 0, st>>>(
                 gv, av, E.cell_words, E.block_offsets, wb, mo.indices, mo.maxV);
         } else if (flat) {
-            k_mc_emit_cells<<<persistent_grid(k_mc_emit_cells, EMIT_WARPS * 32, (nb + EMIT_WARPS - 1) / EMIT_WARPS),
+            k_mc_emit_cells<<<persistent_grid(k_mc_emit_cells, EMIT_WARPS * 32, (cap + EMIT_WARPS - 1) / EMIT_WARPS),
                               EMIT_WARPS * 32, 0, st>>>(
                 gv, av, E.fields, E.cell_words, E.block_offsets, mo, mask);
         } else {
-            k_mc_emit<<<persistent_grid(k_mc_emit, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(
+            k_mc_emit<<<persistent_grid(k_mc_emit, BLK_THREADS, cap), BLK_THREADS, 0, st>>>(
                 gv, sv, time, av, E.fields, E.block_offsets, nullptr, (E.debug & 1) ? E.packet_offsets : nullptr, mo,
                 mask, &ctrl->tickets[1], diag);
         }
@@ -767,17 +784,18 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
         B.offsets = E.packet_offsets;
         B.qef_debug = (E.debug & 2) ? E.dc_qef : nullptr;
         record(cudaMemsetAsync(E.b2a, 0xFF, (size_t)nb * sizeof(int), st));
-        k_dc_block_map<<<(nb + 255) / 256, 256, 0, st>>>(E.list, &ctrl->active_count, nb, nb, E.b2a);
+        k_dc_block_map<<<(cap + 255) / 256, 256, 0, st>>>(E.list, &ctrl->active_count, cap, nb, E.b2a);
         check_launch();
         // the block rows by the shared-halo block field (own samples two per lane, halos copied from
         // active neighbours), then the cells classified from the finished rows
         if (run_block_field<false>(E, sv, time, av, ctrl, nullptr, st, nullptr, false) != SDF_OK) return SDF_ERR_NOMEM;
-        k_dc_mark<<<persistent_grid(k_dc_mark, BLK_THREADS, nb), BLK_THREADS, 0, st>>>(gv, sv, time, av, E.fields, B,
+        k_dc_mark<<<persistent_grid(k_dc_mark, BLK_THREADS, cap), BLK_THREADS, 0, st>>>(gv, sv, time, av, E.fields, B,
                                                                                       &ctrl->tickets[5], diag, true);
         check_launch();
-        const unsigned ncells_max = (unsigned)nb * 512u;
+        const unsigned ncells_max = (unsigned)cap * 512u;
         k_exclusive_scan<<<std::max(1u, scan_tiles(ncells_max)), SCAN_THREADS, 0, st>>>(
-            E.packet_counts, E.dc_voff, 0, &ctrl->active_count, 512, scan_state(scanC), &ctrl->dc_vertices, diag);
+            E.packet_counts, E.dc_voff, (unsigned)cap, &ctrl->active_count, 512, scan_state(scanC),
+            &ctrl->dc_vertices, diag);
         check_launch();
         if (E.timing) cudaEventRecord(E.ev[2], st);
         DcSolveParams sp;
@@ -787,23 +805,24 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
         sp.projection_iters = C.dc_solver == SDF_DC_SOLVER_MASSPOINT ? C.projection_iters : 0;
         sp.cond_threshold = C.cond_threshold > 0.f ? C.cond_threshold : 1e4f;
         const size_t solve_smem = sizeof(SolveSmem);
-        k_dc_solve<<<persistent_grid(k_dc_solve, SOLVE_THREADS, nb, solve_smem), SOLVE_THREADS, solve_smem, st>>>(
+        k_dc_solve<<<persistent_grid(k_dc_solve, SOLVE_THREADS, cap, solve_smem), SOLVE_THREADS, solve_smem, st>>>(
             gv, sv, time, av, E.fields, B, sp, &ctrl->tickets[1], diag);
         check_launch();
         if (E.timing) cudaEventRecord(E.ev[3], st);
-        k_dc_count_quads<<<std::min(nb, num_sms() * 4), 512, 0, st>>>(gv, av, B, E.packet_counts, E.block_totals);
+        k_dc_count_quads<<<std::min(cap, num_sms() * 4), 512, 0, st>>>(gv, av, B, E.packet_counts, E.block_totals);
         check_launch();
-        k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)nb)), SCAN_THREADS, 0, st>>>(
-            E.block_totals, E.block_offsets, 0, &ctrl->active_count, 1, scan_state(scanB), &ctrl->total_vertices, diag);
+        k_exclusive_scan<<<std::max(1u, scan_tiles((unsigned)cap)), SCAN_THREADS, 0, st>>>(
+            E.block_totals, E.block_offsets, (unsigned)cap, &ctrl->active_count, 1, scan_state(scanB),
+            &ctrl->total_vertices, diag);
         check_launch();
         DcQuadParams qp;
         qp.adaptive_diagonal = (C.dc_solver == SDF_DC_SOLVER_MASSPOINT) ? C.adaptive_diagonal : 0;
         const size_t quad_smem = sizeof(QuadSmem);
-        k_dc_quads<<<persistent_grid(k_dc_quads, BLK_THREADS, nb, quad_smem), BLK_THREADS, quad_smem, st>>>(
+        k_dc_quads<<<persistent_grid(k_dc_quads, BLK_THREADS, cap, quad_smem), BLK_THREADS, quad_smem, st>>>(
             gv, sv, time, av, B, nullptr, E.packet_counts, E.block_offsets, mo, mask, qp, &ctrl->tickets[2], diag);
         check_launch();
         if (welded) {  // indexed output: the cell vertices themselves
-            k_dc_weld_vertices<<<persistent_grid(k_dc_weld_vertices, 256, nb * 2), 256, 0, st>>>(
+            k_dc_weld_vertices<<<persistent_grid(k_dc_weld_vertices, 256, cap * 2), 256, 0, st>>>(
                 gv, av, B, (unsigned)E.dc_cap, mo.verts, mo.maxV);
             check_launch();
         }
@@ -814,6 +833,10 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
     record(cudaMemcpyAsync(h_slot, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
     if (cudaEventRecord(P.done, st) != cudaSuccess) return SDF_ERR_CUDA;
     P.nb = nb;
+    P.rows_cap = cap;
+    P.out = *out;
+    P.time = time;
+    P.stream = st;
     P.dc = dc;
     P.welded = welded;
     P.culled = culled;
@@ -823,9 +846,32 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
     return SDF_OK;
 }
 
+// Grows the per-active-block buffers to hold `need` active blocks (a quarter more, at most every block)
+// after an extraction found more active blocks than they held. Waits for the device first: other
+// extractions in flight may still use the buffers the next enqueue reallocates.
+static sdf_status engine_grow_rows(EngineImpl& E, long long need) {
+    using namespace sdfb;
+    const long long cap = std::min<long long>(E.nblocks, need + need / 4 + 1024);
+    if (cap <= E.rows_cap) return SDF_OK;
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        record(e);
+        return SDF_ERR_CUDA;
+    }
+    if (dev_alloc(E.fields, (size_t)cap * FIELD_STRIDE) != SDF_OK) {
+        E.rows_cap = 0;
+        return SDF_ERR_NOMEM;
+    }
+    E.rows_cap = (int)cap;  // the miss list, cell words, weld and DC arrays follow on their next use
+    return SDF_OK;
+}
+
 // Waits for the extraction of a slot and turns its read-back into stats and a status. The stage
-// times are the engine's timing events, valid for the most recent extraction only.
-static sdf_status engine_collect(EngineImpl& E, int slot, sdf_stats* stats, bool stage_times) {
+// times are the engine's timing events, valid for the most recent extraction only. *rows_need > 0:
+// the extraction found more active blocks than its per-block buffers held (its outputs are not
+// valid; engine_grow_rows and a second run follow).
+static sdf_status engine_collect(EngineImpl& E, int slot, sdf_stats* stats, bool stage_times,
+                                 long long* rows_need = nullptr) {
     using namespace sdfb;
     EngineImpl::Pending& P = E.pend[slot];
     const cudaError_t err = cudaEventSynchronize(P.done);
@@ -836,6 +882,7 @@ static sdf_status engine_collect(EngineImpl& E, int slot, sdf_stats* stats, bool
         return SDF_ERR_CUDA;
     }
     const Ctrl& h = E.h_ctrl[slot];
+    if (rows_need) *rows_need = h.active_count > P.rows_cap ? (long long)h.active_count : 0;
     if (stats) {
         memset(stats, 0, sizeof(*stats));
         stats->total_blocks = P.nb;
@@ -889,7 +936,20 @@ sdf_status sdf_engine_extract_wait(sdf_engine* e, uint64_t ticket, sdf_stats* st
     cudaSetDevice(E.device);
     const int slot = (int)(ticket % EngineImpl::ASYNC_SLOTS);
     if (!E.pend[slot].used || E.pend[slot].ticket != ticket) return SDF_ERR_INVALID;  // unknown or collected
-    return engine_collect(E, slot, stats, ticket + 1 == E.next_ticket);
+    const bool last = ticket + 1 == E.next_ticket;
+    long long need = 0;
+    sdf_status s = engine_collect(E, slot, stats, last, &need);
+    if (need == 0) return s;
+    // more active blocks than the per-block buffers held: grow them and run this extraction again
+    // (synchronously, on its stream; the same scene and time cannot need more the second time)
+    s = engine_grow_rows(E, need);
+    if (s != SDF_OK) return s;
+    EngineImpl::Pending& P = E.pend[slot];
+    const sdf_outputs out = P.out;
+    s = engine_enqueue(E, P.time, &out, P.stream, P, &E.h_ctrl[slot]);
+    if (s != SDF_OK) return s;
+    P.used = true;
+    return engine_collect(E, slot, stats, last, &need);
 }
 
 sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out, void* stream, sdf_stats* stats) {
@@ -902,7 +962,7 @@ sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out,
 const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes) {
     if (!e) return nullptr;
     EngineImpl& E = e->impl;
-    const size_t cells = (size_t)E.nblocks * 512;
+    const size_t cells = (size_t)E.rows_cap * 512;
     const void* p = nullptr;
     size_t b = 0;
     switch (which) {
@@ -914,7 +974,7 @@ const void* sdf_engine_buffer(sdf_engine* e, int which, size_t* bytes) {
         case 5: p = E.dc_verts; b = E.dc_cap * 8; break;
         case 6: p = E.dc_norms; b = E.dc_cap * 8; break;
         case 7: p = E.block_totals; b = (size_t)E.nblocks * 4; break;
-        case 8: p = E.fields; b = (size_t)E.nblocks * sdfb::FIELD_STRIDE * 4; break;
+        case 8: p = E.fields; b = (size_t)E.rows_cap * sdfb::FIELD_STRIDE * 4; break;
         case 9: p = E.d_prims; b = (size_t)E.nprims * sizeof(sdf_primitive); break;
         case 10: p = E.d_nodes; b = (size_t)E.nnodes * sizeof(sdf_bvh_node); break;
         case 11: p = E.dc_qef; b = E.dc_qef_cap * 16; break;
@@ -994,8 +1054,11 @@ sdf_status sdf_engine_count_work(sdf_engine* e, unsigned long long out[8]) {
     sv.nnodes = E.nnodes;
     if (run_scout_compact(E.gv, sv, 0.f, E.flags, scanA, E.list, &ctrl->active_count, &ctrl->diag, 0) != cudaSuccess)
         return SDF_ERR_CUDA;
+    int count = 0;
+    if (cudaMemcpy(&count, &ctrl->active_count, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return SDF_ERR_CUDA;
+    if (count > E.rows_cap && engine_grow_rows(E, count) != SDF_OK) return SDF_ERR_NOMEM;
     record(cudaMemsetAsync(&ctrl->diag, 0, sizeof(Diag), 0));
-    ActiveView av{E.list, &ctrl->active_count, E.nblocks};
+    ActiveView av{E.list, &ctrl->active_count, E.rows_cap};
     // the engine's block-field stage (own samples, then the halos no active block owns) with counters on
     if (run_block_field<true>(E, sv, 0.f, av, ctrl, nullptr, 0) != SDF_OK) return SDF_ERR_NOMEM;
     Ctrl h;

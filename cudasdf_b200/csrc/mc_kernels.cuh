@@ -611,6 +611,12 @@ __global__ void __launch_bounds__(BLK_THREADS, 4) k_field_gather(GridView g0, Ac
             int hx, hy, hz;
             halo_coord(lane + 32 * k, hx, hy, hz);
             const int b = block_to_active[bbase + src[k]];
+            // an owner past the rows the buffers hold (the engine then grows them and runs again) has no
+            // row this extraction: the entry is left as it is
+            if (b < 0 || b >= n) {
+                src[k] = -1;
+                continue;
+            }
             hv[k] = fields[(size_t)b * FIELD_STRIDE + ((hz & 7) * 9 + (hy & 7)) * 9 + (hx & 7)];
         }
         __syncwarp();  // the row is in place before the copied halo entries overwrite their slots

@@ -119,8 +119,8 @@ __device__ __forceinline__ unsigned tile_lookback(const ScanState& st, int tile,
     return r;
 }
 
-// out[i] = sum(in[0..i)), i < n. n is (*n_dev) * n_mult when n_dev != nullptr (a device-side count),
-// else n_host. If `total` is set, the grand total is written there by the last tile.
+// out[i] = sum(in[0..i)), i < n. n is min(*n_dev, n_host) * n_mult when n_dev != nullptr (a device-side
+// count, bounded by the rows the arrays hold), else n_host. If `total` is set, the grand total is written there by the last tile.
 __global__ void __launch_bounds__(SCAN_THREADS) k_exclusive_scan(const unsigned* __restrict__ in,
                                                                  unsigned* __restrict__ out, unsigned n_host,
                                                                  const int* __restrict__ n_dev, unsigned n_mult,
@@ -128,7 +128,8 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_exclusive_scan(const unsigned*
     __shared__ unsigned s_warp[SCAN_THREADS / 32];
     __shared__ unsigned s_pfx;
     __shared__ int s_tile;
-    const unsigned n = n_dev ? (unsigned)max(*n_dev, 0) * n_mult : n_host;
+    // with a device count, n_host bounds it (the rows the caller's arrays hold)
+    const unsigned n = n_dev ? (unsigned)min(max(*n_dev, 0), (int)n_host) * n_mult : n_host;
     if (threadIdx.x == 0) s_tile = (int)atomicAdd(st.ticket, 1u);
     __syncthreads();
     const int tile = s_tile;

@@ -409,9 +409,9 @@ sdf_status sdf_surrogate_enable(sdf_engine* e, int enabled) {
     return SDF_OK;
 }
 
-sdf_status sdf_engine_set_coarse_cull(sdf_engine* e, int mode) {
+sdf_status sdf_engine_set_coarse_cull(sdf_engine* e, int mode, float extra_margin) {
     using namespace sdfb;
-    if (!e || mode < SDF_CULL_NONE || mode > SDF_CULL_EXACT) return SDF_ERR_INVALID;
+    if (!e || mode < SDF_CULL_NONE || mode > SDF_CULL_EXACT || !(extra_margin >= 0.f)) return SDF_ERR_INVALID;
     EngineImpl& E = e->impl;
     if (mode == SDF_CULL_SURROGATE) return sdf_surrogate_enable(e, 1);
     if (mode == SDF_CULL_NONE) {
@@ -422,6 +422,7 @@ sdf_status sdf_engine_set_coarse_cull(sdf_engine* e, int mode) {
     const sdf_status s = surrogate_state(E);  // the coarse-field buffer and the audit counters
     if (s != SDF_OK) return s;
     E.sur->exact_coarse = true;
+    E.sur->exact_extra = extra_margin;
     E.sur->enabled = true;
     return SDF_OK;
 }

@@ -258,7 +258,9 @@ __global__ void __launch_bounds__(WELD_WARPS * 32) k_weld_indices(GridView g, Ac
                         block_coord(g, olin, obx, oby, obz);
                         slot = weld_slot(X - 8 * obx, Y - 8 * oby, Z - 8 * obz, axis);
                     }
-                    indices[v + j] = wb.base[oa] + weld_rank(wb, oa, slot);
+                    // an owner past the rows the buffers hold has no bitmap this extraction (the engine
+                    // grows them and runs again)
+                    indices[v + j] = (oa >= 0 && oa < n) ? wb.base[oa] + weld_rank(wb, oa, slot) : 0u;
                 }
                 v += 3;
             }

@@ -195,9 +195,11 @@ class Engine:
     def surrogate_enable(self, on: bool):
         L.check(self._lib.sdf_surrogate_enable(self.h, 1 if on else 0), "sdf_surrogate_enable")
 
-    def set_coarse_cull(self, mode: int):
-        """L.SDF_CULL_NONE, L.SDF_CULL_SURROGATE or L.SDF_CULL_EXACT (the exact map() at the coarse centres)."""
-        L.check(self._lib.sdf_engine_set_coarse_cull(self.h, int(mode)), "sdf_engine_set_coarse_cull")
+    def set_coarse_cull(self, mode: int, extra_margin: float = 0.0):
+        """L.SDF_CULL_NONE, L.SDF_CULL_SURROGATE or L.SDF_CULL_EXACT (the exact map() at the coarse centres,
+        culled beyond the reach plus extra_margin)."""
+        L.check(self._lib.sdf_engine_set_coarse_cull(self.h, int(mode), float(extra_margin)),
+                "sdf_engine_set_coarse_cull")
 
     def surrogate_audit(self, time: float = 0.0) -> dict:
         v, c, n = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()

@@ -374,13 +374,14 @@ sdf_status sdf_surrogate_enable(sdf_engine* e, int enabled);
 /* Coarse-block culling of sdf_engine_extract: SDF_CULL_NONE, SDF_CULL_SURROGATE (f_net with the
  * certified margin eps + K; as sdf_surrogate_enable(e, 1)) or SDF_CULL_EXACT, the method without the
  * network: the exact map() at each coarse centre, one evaluation per 32^3 cells, culled when
- * |f| > K (the reach above with eps = 0; the field of smooth-blended, pruned primitives is not
- * 1-Lipschitz, so the audit below is the judge here too). The exact mode needs no training and stays
- * on across scene changes. */
+ * |f| > K + extra_margin (extra_margin >= 0 is ignored by the other modes). The capped, pruned field
+ * of smooth-blended primitives is not 1-Lipschitz (a coarse centre whose search hits the 256-step cap
+ * can read far too large a distance), so extra_margin = 0 is not safe in general; the audit below is
+ * the judge. The exact mode needs no training and stays on across scene changes. */
 #define SDF_CULL_NONE 0
 #define SDF_CULL_SURROGATE 1
 #define SDF_CULL_EXACT 2
-sdf_status sdf_engine_set_coarse_cull(sdf_engine* e, int mode);
+sdf_status sdf_engine_set_coarse_cull(sdf_engine* e, int mode, float extra_margin);
 /* Exact audit of the current culling (surrogate or exact coarse field): a full exact scout at `time`;
  * *violations = exact-active blocks inside culled coarse blocks (0 means the culled extraction equals
  * the plain one), *culled = culled coarse blocks, *coarse = all coarse blocks. Synchronous. */

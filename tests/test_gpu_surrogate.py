@@ -100,10 +100,13 @@ def test_training_culls_and_keeps_the_mesh():
 
 def test_network_against_the_method_without_it():
     """What the trained network gains over culling without it. The method without the network evaluates
-    the exact map() at every 32^3 coarse centre and culls with the same reach and eps = 0
-    (SDF_CULL_EXACT); the surrogate evaluates f_net on tensor cores and culls with eps_cert + reach. Both
-    must keep the plain mesh (audit 0, identical vertices); the test reports the coarse blocks each culls
-    and the blocks each leaves to the exact scout (the time is in the bench line)."""
+    the exact map() at every 32^3 coarse centre and culls beyond a margin (SDF_CULL_EXACT); the
+    surrogate evaluates f_net on tensor cores and culls beyond its certified margin eps_cert + reach.
+    With the reach alone (no extra margin) the exact field culls coarse blocks that hold active blocks:
+    the capped, pruned field of blended primitives is not 1-Lipschitz, and a coarse centre whose search
+    hits the 256-step cap reads too large a distance. Given the surrogate's certified eps as its extra
+    margin it keeps the plain mesh; the test reports the coarse blocks each mode culls and the blocks
+    each leaves to the exact scout (the time of each is in the bench line)."""
     from cudasdf_b200 import _lib as L
     from cudasdf_b200 import scenes as S
     from cudasdf_b200.engine import Engine, MeshBuffers, make_config
@@ -115,23 +118,20 @@ def test_network_against_the_method_without_it():
     V = plain["total_vertices"]
     h_plain = hashlib.sha256(buf.vertices[:V].cpu().numpy().tobytes()).hexdigest()
     res = {}
-    eng.set_coarse_cull(L.SDF_CULL_EXACT)  # no training needed
-    res["exact"] = eng.surrogate_audit(0.0)
-    buf.vertices.zero_()
-    st = eng.extract(buf, 0.0)
-    res["exact"]["scouted_blocks"] = st["scouted_blocks"]
-    assert res["exact"]["violations"] == 0 and st["total_vertices"] == V
-    assert hashlib.sha256(buf.vertices[:V].cpu().numpy().tobytes()).hexdigest() == h_plain
-    eng.surrogate_train()
-    eng.set_coarse_cull(L.SDF_CULL_SURROGATE)
-    res["surrogate"] = eng.surrogate_audit(0.0)
-    buf.vertices.zero_()
-    st = eng.extract(buf, 0.0)
-    res["surrogate"]["scouted_blocks"] = st["scouted_blocks"]
-    assert res["surrogate"]["violations"] == 0 and st["total_vertices"] == V
-    assert hashlib.sha256(buf.vertices[:V].cpu().numpy().tobytes()).hexdigest() == h_plain
-    # the exact coarse field is the sharper cull (eps = 0 against eps_cert > 0)
-    assert res["exact"]["culled_coarse"] >= res["surrogate"]["culled_coarse"]
+    eng.set_coarse_cull(L.SDF_CULL_EXACT, 0.0)  # no training needed
+    res["exact_reach_only"] = eng.surrogate_audit(0.0)
+    st = eng.surrogate_train()
+    res["eps_cert"] = st["eps_cert"]
+    for name, mode, extra in (("surrogate", L.SDF_CULL_SURROGATE, 0.0),
+                              ("exact_same_margin", L.SDF_CULL_EXACT, st["eps_cert"])):
+        eng.set_coarse_cull(mode, extra)
+        res[name] = eng.surrogate_audit(0.0)
+        buf.vertices.zero_()
+        out = eng.extract(buf, 0.0)
+        res[name]["scouted_blocks"] = out["scouted_blocks"]
+        assert res[name]["violations"] == 0, (name, res)
+        assert out["total_vertices"] == V
+        assert hashlib.sha256(buf.vertices[:V].cpu().numpy().tobytes()).hexdigest() == h_plain
     eng.set_coarse_cull(L.SDF_CULL_NONE)
     assert eng.extract(buf, 0.0)["scouted_blocks"] == plain["scouted_blocks"]
     print("coarse culling at 1024^3:", res, "plain scouted", plain["scouted_blocks"])
