@@ -142,7 +142,7 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
             &ctrl->total_vertices, diag);
         if (flat)
             k_mc_emit_cells<<<G.emit_cells, EMIT_WARPS * 32, 0, st>>>(g0, av, B.fields, B.cell_words, B.block_offsets,
-                                                                      mo, m);
+                                                                      mo, m, diag);
         else
             k_mc_emit<<<G.emit, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.fields, B.block_offsets, nullptr, nullptr, mo,
                                                       m, &ctrl->tickets[1], diag);

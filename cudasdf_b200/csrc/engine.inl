@@ -764,7 +764,7 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
         } else if (flat) {
             k_mc_emit_cells<<<persistent_grid(k_mc_emit_cells, EMIT_WARPS * 32, (cap + EMIT_WARPS - 1) / EMIT_WARPS),
                               EMIT_WARPS * 32, 0, st>>>(
-                gv, av, E.fields, E.cell_words, E.block_offsets, mo, mask);
+                gv, av, E.fields, E.cell_words, E.block_offsets, mo, mask, diag);
         } else {
             k_mc_emit<<<persistent_grid(k_mc_emit, BLK_THREADS, cap), BLK_THREADS, 0, st>>>(
                 gv, sv, time, av, E.fields, E.block_offsets, nullptr, (E.debug & 1) ? E.packet_offsets : nullptr, mo,

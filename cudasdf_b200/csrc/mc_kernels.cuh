@@ -13,6 +13,7 @@
 #pragma once
 
 #include "mc_cases.inc"
+#include "bulk.cuh"
 #include "scan.cuh"
 #include "sdf_device.cuh"
 #include "uv.cuh"
@@ -728,27 +729,51 @@ __global__ void __launch_bounds__(256) k_fma_peak(float* out, int iters, float a
 // ------------------------------------------------------------------------------------------------
 constexpr int EMIT_WARPS = 8;
 
+// A warp's staging: the 512 cell words of two blocks (the one it emits and the next one it will emit,
+// filled by a bulk copy while the current one is processed), the emitting cells, the copies' barriers.
 struct EmitWarpSmem {
-    unsigned words[512];
+    unsigned words[2][512];
     unsigned short list[512];
+    uint64_t bar[2];
 };
 
 __global__ void __launch_bounds__(EMIT_WARPS * 32, 5) k_mc_emit_cells(GridView g0, ActiveView av,
                                                                   const float* __restrict__ fields,
                                                                   const unsigned* __restrict__ cell_words,
                                                                   const unsigned* __restrict__ block_offsets,
-                                                                  MeshOut out, unsigned mask) {
+                                                                  MeshOut out, unsigned mask, Diag* diag) {
     __shared__ unsigned long long s_cases[256];
     __shared__ __align__(16) EmitWarpSmem s_warp[EMIT_WARPS];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) s_cases[i] = c_mcCases[i];
-    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     EmitWarpSmem& W = s_warp[warp];
+    if (lane == 0) {
+        bar_init(&W.bar[0], 1);
+        bar_init(&W.bar[1], 1);
+    }
+    __syncthreads();
     const int n = active_count(av);
-    for (int a = blockIdx.x * EMIT_WARPS + warp; a < n; a += gridDim.x * EMIT_WARPS) {
-        const uint4* src = reinterpret_cast<const uint4*>(cell_words + (size_t)a * 512);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) reinterpret_cast<uint4*>(W.words)[lane + 32 * q] = __ldcs(src + lane + 32 * q);
+    const int stride = gridDim.x * EMIT_WARPS;
+    // the cell words of block a into staging buffer b (lane 0; 2 KB, 16-byte aligned rows)
+    auto stage = [&](int a, int b) {
+        bar_expect_tx(&W.bar[b], 512 * sizeof(unsigned));
+        bulk_g2s(W.words[b], cell_words + (size_t)a * 512, 512 * sizeof(unsigned), &W.bar[b]);
+    };
+    int a = blockIdx.x * EMIT_WARPS + warp;
+    if (a < n && lane == 0) stage(a, 0);
+    unsigned parity[2] = {0u, 0u};
+    int buf = 0;
+    bool pending_other = false;  // a copy into the other buffer is in flight
+    for (; a < n; a += stride) {
+        const int next = a + stride;
+        if (next < n && lane == 0) stage(next, buf ^ 1);  // that buffer was released at the end of the last block
+        pending_other = next < n;
+        if (!__all_sync(0xffffffffu, bar_wait(&W.bar[buf], parity[buf]))) {
+            if (lane == 0 && diag) atomicExch(&diag->timeout, 1);
+            break;
+        }
+        parity[buf] ^= 1u;
+        const unsigned* words = W.words[buf];
         GridView g = g0;
         SceneView unused;
         int lin;
@@ -758,7 +783,7 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32, 5) k_mc_emit_cells(GridView g
         int nlist = 0;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const uint4 w4 = reinterpret_cast<const uint4*>(W.words)[lane + 32 * q];
+            const uint4 w4 = reinterpret_cast<const uint4*>(words)[lane + 32 * q];
             const unsigned wq[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
@@ -775,7 +800,7 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32, 5) k_mc_emit_cells(GridView g
         const float* f = fields + (size_t)a * FIELD_STRIDE;
         for (int i = lane; i < nlist; i += 32) {
             const int tid = W.list[i];
-            const unsigned w = W.words[tid];
+            const unsigned w = words[tid];
             const unsigned vm = (w >> 8) & 31u;
             const CellInfo c = cell_info(g, bx, by, bz, tid);
             float cv[8];
@@ -800,8 +825,13 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32, 5) k_mc_emit_cells(GridView g
                 v += 3;
             }
         }
-        __syncwarp();  // the warp's shared memory is free for the next block
+        __syncwarp();  // the buffer and the list are free for the next block
+        buf ^= 1;
+        pending_other = false;
     }
+    // after a timeout, the copy already issued into the other buffer is waited for (bounded) before
+    // the CTA's shared memory goes away
+    if (pending_other) (void)bar_wait(&W.bar[buf ^ 1], parity[buf ^ 1]);
 }
 
 // ------------------------------------------------------------------------------------------------
