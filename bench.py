@@ -860,8 +860,9 @@ def main():
 # 3 products, 3 cross terms, 3 x (2 FMA + 1 mul), 3 divisions), the primitive's distance (about 12)
 # and the smooth-union blend (about 12).
 FLOP_PER_NODE = 12
-# DRAM bytes per active block of the block-field stage, from an ncu capture (see roofline())
-TRAFFIC_PER_ACTIVE_BLOCK = (14.046208e6 + 13.871616e6) / 12524
+# DRAM bytes per active block of the block-field stage (k_field_own + k_field_miss), from a one-pass ncu
+# capture of the 1024^3 workload: 85.60 + 85.64 MB and 23.63 + 15.04 MB for its 44,270 active blocks
+TRAFFIC_PER_ACTIVE_BLOCK = (85.60e6 + 85.64e6 + 23.63e6 + 15.04e6) / 44270
 FLOP_PER_LEAF = 44 + 12 + 12 + 1
 
 
@@ -879,9 +880,9 @@ def roofline(r):
             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": "measured by the library's FMA loop on this GPU (no FP32 figure in MEASURED_PEAKS.json)",
             "traffic": TRAFFIC_PER_ACTIVE_BLOCK * active,
-            "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of k_field_own on "
-                              "the 256^3, 256-primitive workload, 2.23 KB per active block, scaled by this run's "
-                              "active blocks",
+            "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of k_field_own + k_field_miss in one "
+                              "ncu capture of the 1024^3, 16,384-primitive workload, 4.74 KB per active block, "
+                              "scaled by this run's active blocks",
             "work": c}
 
 
