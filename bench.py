@@ -172,7 +172,7 @@ def fp32_peak_tflops():
     return v.value if rc == 0 else None
 
 
-STAGES = ("ms_scout", "ms_field", "ms_scan", "ms_emit")
+STAGES = ("ms_scout", "ms_field", "ms_scan", "ms_emit", "ms_classify")
 
 
 def timed_extractions(eng, buf, steps, flush, world):
@@ -863,6 +863,8 @@ FLOP_PER_NODE = 12
 # DRAM bytes per active block of the block-field stage (k_field_own + k_field_miss), from a one-pass ncu
 # capture of the 1024^3 workload: 85.60 + 85.64 MB and 23.63 + 15.04 MB for its 44,270 active blocks
 TRAFFIC_PER_ACTIVE_BLOCK = (85.60e6 + 85.64e6 + 23.63e6 + 15.04e6) / 44270
+# the same capture's DRAM bytes per active block of the gather (classification and counts) and the emission
+DRAM_PER_ACTIVE_BLOCK = {"gather": (133.37e6 + 134.72e6) / 44270, "emission": (133.75e6 + 86.49e6) / 44270}
 FLOP_PER_LEAF = 44 + 12 + 12 + 1
 
 
@@ -904,19 +906,27 @@ def hbm_peak():
 
 def stage_roofline(r):
     """Achieved HBM fraction of the memory-bound stages by their algorithmic bytes, A active blocks and
-    V vertices (one index per vertex): scan 8 B x A; emission reads the 4-byte cell word of each of the
-    512 A cells and writes 16 B (float4 position) + 4 B (index) per vertex. Classification and counting
-    run inside the block-field stage (the gather kernel, fused with the halo copy), so their time is
-    not separate here; an ncu launch list of the same command gives the gather kernel's own time."""
+    V vertices (one index per vertex): classification and counting (the gather kernel, timed by its own
+    events inside the block-field stage) read the 4-byte samples of the 512 A cells and write 4 B per
+    block; scan 8 B x A; emission reads the 4-byte cell word of each of the 512 A cells and writes 16 B
+    (float4 position) + 4 B (index) per vertex. Beside each, the DRAM bytes ncu measured."""
     st, stages = r["stats"], r["stages"]
     a, v = st["active_blocks"], st["total_vertices"]
     peak, source = hbm_peak()
-    out = {"peak": peak, "unit": "GB/s", "peak_source": source}
-    for name, ms, nbytes in (("scan", stages.get("ms_scan"), 8 * a),
-                             ("emission", stages.get("ms_emit"), 4 * 512 * a + 20 * v)):
+    out = {"peak": peak, "unit": "GB/s", "peak_source": source,
+           "dram_source": "dram__bytes_read.sum + dram__bytes_write.sum per active block from a one-pass ncu "
+                          "capture of the 1024^3 workload, scaled by this run's active blocks"}
+    for name, ms, nbytes, dram in (("classify_count", stages.get("ms_classify"), 4 * 512 * a + 4 * a,
+                                    DRAM_PER_ACTIVE_BLOCK["gather"] * a),
+                                   ("scan", stages.get("ms_scan"), 8 * a, None),
+                                   ("emission", stages.get("ms_emit"), 4 * 512 * a + 20 * v,
+                                    DRAM_PER_ACTIVE_BLOCK["emission"] * a)):
         if ms:
             gbs = nbytes / (ms * 1e-3) / 1e9
             out[name] = {"bytes": nbytes, "ms": ms, "achieved": gbs, "frac": gbs / peak}
+            if dram:
+                out[name]["dram_bytes"] = dram
+                out[name]["dram_gbs"] = dram / (ms * 1e-3) / 1e9
     return out
 
 

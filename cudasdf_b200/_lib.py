@@ -38,7 +38,8 @@ class SdfStats(ctypes.Structure):
                 ("dc_cell_vertices", ctypes.c_int64), ("bvh_cap_hits", ctypes.c_int64),
                 ("ms_scout", ctypes.c_float), ("ms_field", ctypes.c_float), ("ms_scan", ctypes.c_float),
                 ("ms_emit", ctypes.c_float), ("ms_total", ctypes.c_float), ("scouted_blocks", ctypes.c_int64),
-                ("dc_fp64_cells", ctypes.c_int64), ("welded_vertices", ctypes.c_int64)]
+                ("dc_fp64_cells", ctypes.c_int64), ("welded_vertices", ctypes.c_int64),
+                ("ms_classify", ctypes.c_float), ("reserved", ctypes.c_float)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -263,6 +263,7 @@ static sdf_status run_block_field(EngineImpl& E, const sdfb::SceneView& sv, floa
     k_field_miss<COUNT><<<persistent_grid(k_field_miss<COUNT>, BLK_THREADS, 1 << 30), BLK_THREADS, 0, st>>>(
         E.gv, sv, time, av, E.fields, E.miss, &ctrl->halo_misses, &ctrl->tickets[4], &ctrl->diag);
     check_launch();
+    if (E.timing) cudaEventRecord(E.ev[5], st);  // the gather: halos, case codes, counts
     k_field_gather<<<persistent_grid(k_field_gather, BLK_THREADS, (E.rows_cap + GATHER_WARPS - 1) / GATHER_WARPS),
                      BLK_THREADS, 0, st>>>(E.gv, av, E.fields, E.b2a, E.flags,
                                            (COUNT || !counts) ? nullptr : E.block_totals, packet_counts, cell_words);
@@ -900,6 +901,7 @@ static sdf_status engine_collect(EngineImpl& E, int slot, sdf_stats* stats, bool
             cudaEventElapsedTime(&stats->ms_field, E.ev[1], E.ev[2]);
             cudaEventElapsedTime(&stats->ms_scan, E.ev[2], E.ev[3]);
             cudaEventElapsedTime(&stats->ms_emit, E.ev[3], E.ev[4]);
+            if (!P.dc) cudaEventElapsedTime(&stats->ms_classify, E.ev[5], E.ev[2]);
         }
     }
     if (h.diag.timeout) return SDF_ERR_TIMEOUT;

@@ -229,6 +229,9 @@ typedef struct sdf_stats {
     int64_t scouted_blocks;     /* blocks whose centre the exact scout evaluated (all, unless culled) */
     int64_t dc_fp64_cells;      /* mass-point DC: cells whose QEF was solved in FP64 (condition number) */
     int64_t welded_vertices;    /* SDF_OUT_WELDED: vertices of the indexed mesh (total_vertices = indices) */
+    float ms_classify;          /* marching cubes, timing enabled: the part of ms_field that completes the
+                                   rows' halos, classifies the cells and counts their triangles */
+    float reserved;
 } sdf_stats;
 
 typedef struct sdf_engine sdf_engine;
