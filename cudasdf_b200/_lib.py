@@ -112,6 +112,59 @@ BATCH_SYMBOLS = ["sdf_batch_create", "sdf_batch_destroy", "sdf_batch_set_scenes"
 STATIC_SCOUT_SYMBOLS = ["sdf_scout_active_blocks_static"]
 SCOUT_STATIC_MAX_BLOCKS = 1 << 20  # SDF_SCOUT_STATIC_MAX_BLOCKS of the header
 EXPORT_SYMBOLS = ["sdf_write_obj"]
+UVPACK_SYMBOLS = ["sdf_uv_pack_default_config", "sdf_uv_atlas_create", "sdf_uv_atlas_destroy",
+                  "sdf_uv_atlas_extract_charts", "sdf_uv_atlas_create_islands", "sdf_uv_atlas_pack",
+                  "sdf_uv_atlas_remap", "sdf_uv_atlas_run", "sdf_uv_atlas_read", "sdf_uv_pack_random_draws"]
+
+
+class UvPackConfig(ctypes.Structure):
+    """sdf_uv_pack_config (the reference's PackingConfig)."""
+    _fields_ = [(n, ctypes.c_int32) for n in (
+        "grid_size", "grid_resolution", "max_iterations", "margin_cells", "enable_rotation", "x_alignment",
+        "max_candidates_per_island", "max_drop_steps", "shuffle_order_per_attempt", "random_seed")]
+
+    def as_list(self):
+        return [getattr(self, n) for n, _ in self._fields_]
+
+
+class UvChart(ctypes.Structure):
+    _fields_ = [("primitive_id", ctypes.c_int32), ("num_triangles", ctypes.c_int32),
+                ("uv_min", ctypes.c_float * 2), ("uv_max", ctypes.c_float * 2)]
+
+
+class UvGrid(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("stride", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("word_offset", ctypes.c_int64)]
+
+
+class UvIsland(ctypes.Structure):
+    _fields_ = [("island_index", ctypes.c_int32), ("primitive_id", ctypes.c_int32), ("num_triangles", ctypes.c_int32),
+                ("min_cell_x", ctypes.c_int32), ("min_cell_y", ctypes.c_int32), ("width", ctypes.c_int32),
+                ("height", ctypes.c_int32), ("pad", ctypes.c_int32), ("mask", UvGrid), ("collision", UvGrid),
+                ("mask90", UvGrid), ("collision90", UvGrid), ("row_bounds", ctypes.c_int64),
+                ("row_bounds90", ctypes.c_int64), ("profile", ctypes.c_int64), ("profile90", ctypes.c_int64)]
+
+
+class UvPlacement(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ("island_index", "grid_x", "grid_y", "rotation")]
+
+
+class UvSolution(ctypes.Structure):
+    _fields_ = [("num_placed", ctypes.c_int32), ("utilized_width", ctypes.c_int32),
+                ("utilized_height", ctypes.c_int32), ("flags", ctypes.c_int32), ("fitness", ctypes.c_float),
+                ("seed", ctypes.c_int32)]
+
+
+class UvAtlasInfo(ctypes.Structure):
+    _fields_ = [("success", ctypes.c_int32), ("atlas_width", ctypes.c_int32), ("atlas_height", ctypes.c_int32),
+                ("num_placed", ctypes.c_int32), ("fitness", ctypes.c_float), ("scaling_factor", ctypes.c_float),
+                ("num_charts", ctypes.c_int32), ("num_islands", ctypes.c_int32), ("num_solutions", ctypes.c_int32),
+                ("best_solution", ctypes.c_int32), ("shelf_width", ctypes.c_int32),
+                ("candidate_loop_open", ctypes.c_int32), ("ms_pack", ctypes.c_float),
+                ("reserved", ctypes.c_float * 3)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
 ENGINE_SYMBOLS = ["sdf_engine_create", "sdf_engine_destroy", "sdf_engine_configure", "sdf_engine_set_scene",
                   "sdf_engine_set_scene_device",
                   "sdf_engine_set_scene_async", "sdf_engine_extract_async", "sdf_engine_extract_wait",
@@ -222,6 +275,27 @@ def lib():
     L.sdf_scout_active_blocks_static.restype = i
     L.sdf_write_obj.argtypes = [ctypes.c_char_p, vp, ctypes.c_uint64, vp, ctypes.c_uint64, vp]
     L.sdf_write_obj.restype = i
+    L.sdf_uv_pack_default_config.argtypes = [ctypes.POINTER(UvPackConfig)]
+    L.sdf_uv_pack_default_config.restype = None
+    L.sdf_uv_atlas_create.argtypes = [ctypes.POINTER(vp)]
+    L.sdf_uv_atlas_create.restype = i
+    L.sdf_uv_atlas_destroy.argtypes = [vp]
+    L.sdf_uv_atlas_destroy.restype = None
+    L.sdf_uv_atlas_extract_charts.argtypes = [vp, vp, vp, ctypes.c_int64, vp, ctypes.POINTER(ctypes.c_int32)]
+    L.sdf_uv_atlas_extract_charts.restype = i
+    L.sdf_uv_atlas_create_islands.argtypes = [vp, vp, i, i, vp]
+    L.sdf_uv_atlas_create_islands.restype = i
+    L.sdf_uv_atlas_pack.argtypes = [vp, ctypes.POINTER(UvPackConfig), vp, ctypes.POINTER(UvAtlasInfo)]
+    L.sdf_uv_atlas_pack.restype = i
+    L.sdf_uv_atlas_remap.argtypes = [vp, vp, vp, ctypes.c_int64, i, vp]
+    L.sdf_uv_atlas_remap.restype = i
+    L.sdf_uv_atlas_run.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.POINTER(UvPackConfig), vp,
+                                   ctypes.POINTER(UvAtlasInfo)]
+    L.sdf_uv_atlas_run.restype = i
+    L.sdf_uv_atlas_read.argtypes = [vp, i, vp, ctypes.POINTER(ctypes.c_size_t)]
+    L.sdf_uv_atlas_read.restype = i
+    L.sdf_uv_pack_random_draws.argtypes = [vp, i, i, vp]
+    L.sdf_uv_pack_random_draws.restype = i
     L.sdf_last_error.restype = i
     L.sdf_version.restype = ctypes.c_char_p
     _lib = L

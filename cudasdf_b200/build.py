@@ -10,7 +10,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libsdfmesh_b200.so")
 SOURCES = ["sdfmesh.cu", "engine.inl", "mc_kernels.cuh", "dc_kernels.cuh", "sdf_device.cuh", "scan.cuh", "uv.cuh",
            "qef_masspoint.cuh", "bvh_host.h", "mc_cases.inc", "surrogate.cuh", "surrogate.inl", "noalloc.inl", "batch.inl",
-           "bvh_device.cuh", "weld.cuh", "obj_export.inl"]
+           "bvh_device.cuh", "weld.cuh", "obj_export.inl", "uvpack.cuh", "uvpack.inl"]
 
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",

@@ -10,6 +10,10 @@
 #include <string.h>
 
 #include <algorithm>
+#include <climits>
+#include <cmath>
+#include <ctime>
+#include <new>
 #include <mutex>
 #include <vector>
 
@@ -20,6 +24,7 @@
 #include "bvh_device.cuh"
 #include "weld.cuh"
 #include "surrogate.cuh"
+#include "uvpack.cuh"
 
 namespace sdfb {
 
@@ -489,3 +494,4 @@ const char* sdf_version(void) { return "sdfmesh_b200 0.1 (sm_100a)"; }
 #include "batch.inl"
 #include "noalloc.inl"
 #include "obj_export.inl"
+#include "uvpack.inl"

@@ -470,6 +470,118 @@ sdf_status sdf_batch_read_buffer(sdf_batch* b, int technique, int which, void* h
 sdf_status sdf_write_obj(const char* path, const sdf_float4* vertices, uint64_t num_vertices, const uint32_t* indices,
                          uint64_t num_indices, const sdf_float2* uvs);
 
+/* ------------------------------------------------------------------------------------------------
+ * UV atlas packing: the reference's GridUVPacker (src/SDFMesh/GridUVPacker.{cuh,cu}), which packs the
+ * per-primitive UV charts of a mesh (the SDF_OUT_UVS and SDF_OUT_PRIMIDS streams) into one atlas and
+ * remaps the UVs into it. The four steps are the reference's ExtractCharts, CreateIslands,
+ * PackIslands and RemapUVsToAtlas (GridUVPacker.cuh:186-219, called in that order by main.cpp:1429-1442),
+ * with the same results; sdf_uv_atlas_run does all four.
+ * ---------------------------------------------------------------------------------------------- */
+/* PackingConfig (GridUVPacker.cuh:121-146): the same fields, in the same order, with the same defaults. */
+typedef struct sdf_uv_pack_config {
+    int32_t grid_size;                 /* board side in cells (square board); at most 16384 */
+    int32_t grid_resolution;           /* cells per UV unit */
+    int32_t max_iterations;            /* packing attempts; at most 256 run */
+    int32_t margin_cells;              /* gutter around each island, in cells (0..1024) */
+    int32_t enable_rotation;           /* also try each island rotated by 90 degrees */
+    int32_t x_alignment;               /* placement x is a multiple of this */
+    int32_t max_candidates_per_island; /* candidate columns per island and rotation (4..64) */
+    int32_t max_drop_steps;            /* cap on the downward search (0 = none) */
+    int32_t shuffle_order_per_attempt; /* random island order per attempt */
+    int32_t random_seed;               /* seed of the attempts' seeds (0 = time()) */
+} sdf_uv_pack_config;
+
+/* UVChart (GridUVPacker.cuh:149-157) without its triangle list (sdf_uv_atlas_read 1 has each
+ * triangle's chart). */
+typedef struct sdf_uv_chart {
+    int32_t primitive_id;
+    int32_t num_triangles;
+    sdf_float2 uv_min, uv_max;
+} sdf_uv_chart;
+
+/* A bit grid in the island word arena: 32 cells per word, rows of `stride` words from word_offset. */
+typedef struct sdf_uv_grid {
+    int32_t width, height, stride, pad;
+    int64_t word_offset;
+} sdf_uv_grid;
+
+/* Island (GridUVPacker.cuh:68-100), in packing order (the reference's sort by area). */
+typedef struct sdf_uv_island {
+    int32_t island_index;      /* its chart's index */
+    int32_t primitive_id;
+    int32_t num_triangles;
+    int32_t min_cell_x, min_cell_y;
+    int32_t width, height;     /* mask dimensions */
+    int32_t pad;
+    sdf_uv_grid mask, collision, mask90, collision90;
+    int64_t row_bounds, row_bounds90;  /* uint16 arena offsets: first, then last nonzero word of each row */
+    int64_t profile, profile90;        /* int32 arena offsets: lowest, then highest set row of each column */
+} sdf_uv_island;
+
+/* IslandPlacement (GridUVPacker.cuh:104-111) */
+typedef struct sdf_uv_placement {
+    int32_t island_index, grid_x, grid_y, rotation;
+} sdf_uv_placement;
+
+/* One packing attempt (Solution, GridUVPacker.cuh:114-119). flags bit 0: a candidate loop had fewer
+ * aligned columns than its budget and stopped when all were listed (the reference's loop does not end
+ * there, GridUVPacker.cu:660-665). */
+typedef struct sdf_uv_solution {
+    int32_t num_placed, utilized_width, utilized_height, flags;
+    float fitness;
+    int32_t seed;
+} sdf_uv_solution;
+
+/* PackedAtlas (GridUVPacker.cuh:160-170) and the run's counts. */
+typedef struct sdf_uv_atlas_info {
+    int32_t success;           /* every island placed */
+    int32_t atlas_width, atlas_height;  /* squared: both max(utilized width, height) */
+    int32_t num_placed;
+    float fitness, scaling_factor;
+    int32_t num_charts, num_islands, num_solutions;
+    int32_t best_solution;     /* -1 when no attempt placed an island */
+    int32_t shelf_width;
+    int32_t candidate_loop_open;  /* some attempt had a candidate loop the reference could not end */
+    float ms_pack;             /* device time of the packing attempts */
+    float reserved[3];
+} sdf_uv_atlas_info;
+
+typedef struct sdf_uv_atlas sdf_uv_atlas;
+
+void sdf_uv_pack_default_config(sdf_uv_pack_config* c);
+sdf_status sdf_uv_atlas_create(sdf_uv_atlas** out);
+void sdf_uv_atlas_destroy(sdf_uv_atlas* a);
+/* ExtractCharts (GridUVPacker.cu:833-896): one chart per primitive id (the first vertex's float id + 0.5,
+ * truncated), in ascending id; d_uvs and d_primitive_ids are num_vertices device entries (the mesh's
+ * triangle soup; a partial last triangle is ignored). Synchronises `stream` (the chart table is read
+ * back). SDF_ERR_INVALID for ids of 2^24 or more. */
+sdf_status sdf_uv_atlas_extract_charts(sdf_uv_atlas* a, const sdf_float2* d_uvs, const float* d_primitive_ids,
+                                       int64_t num_vertices, void* stream, int32_t* num_charts);
+/* CreateIslands (GridUVPacker.cu:898-1061) for the charts of the last extraction; d_uvs as given to it.
+ * Islands wider or taller than 65536 cells (or above 2^30 cells) give SDF_ERR_INVALID. */
+sdf_status sdf_uv_atlas_create_islands(sdf_uv_atlas* a, const sdf_float2* d_uvs, int32_t grid_resolution,
+                                       int32_t margin_cells, void* stream);
+/* PackIslands (GridUVPacker.cu:1063-1439). Synchronises `stream`. info->success as the reference's
+ * PackedAtlas.success; SDF_OK also when the atlas is not a success. */
+sdf_status sdf_uv_atlas_pack(sdf_uv_atlas* a, const sdf_uv_pack_config* c, void* stream, sdf_uv_atlas_info* info);
+/* RemapUVsToAtlas (GridUVPacker.cu:1441-1547): UVs of placed charts into [0, 1] of the atlas; nothing
+ * changes when the last packing is not a success. */
+sdf_status sdf_uv_atlas_remap(sdf_uv_atlas* a, sdf_float2* d_uvs, const float* d_primitive_ids, int64_t num_vertices,
+                              int32_t grid_resolution, void* stream);
+/* The four steps in main.cpp's order (main.cpp:1429-1442). */
+sdf_status sdf_uv_atlas_run(sdf_uv_atlas* a, sdf_float2* d_uvs, const float* d_primitive_ids, int64_t num_vertices,
+                            const sdf_uv_pack_config* c, void* stream, sdf_uv_atlas_info* info);
+/* Copies internal arrays to host memory (after the step that makes them): 0 charts (sdf_uv_chart),
+ * 1 chart per triangle (int32, -1 none), 2 islands (sdf_uv_island, packing order), 3 the mask word
+ * arena (uint32), 4 row bounds (uint16), 5 column profiles (int32), 6 attempt seeds (int32),
+ * 7 attempts (sdf_uv_solution), 8 every attempt's placements (sdf_uv_placement, min(islands, 256) per
+ * attempt), 9 the chosen placements. *bytes: in, the capacity of host_dst; out, the bytes the array
+ * holds (host_dst may be NULL to ask). Synchronous. */
+sdf_status sdf_uv_atlas_read(sdf_uv_atlas* a, int which, void* host_dst, size_t* bytes);
+/* For tests: the first `per_seed` values of curand(curand_init(seed, 0, 0)) for each seed, the
+ * stream a packing attempt draws from; host arrays. */
+sdf_status sdf_uv_pack_random_draws(const int32_t* seeds, int32_t num_seeds, int32_t per_seed, uint32_t* host_out);
+
 /* First CUDA error recorded by a drop-in launcher since the last call (cleared on read). */
 int sdf_last_error(void);
 /* Library version string. */

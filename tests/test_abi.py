@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in declared_functions() if not hasattr(L, n)]
     assert not missing, missing
     assert set(_lib.DROPIN_SYMBOLS + _lib.ENGINE_SYMBOLS + _lib.SURROGATE_SYMBOLS + _lib.BATCH_SYMBOLS +
-               _lib.STATIC_SCOUT_SYMBOLS + _lib.EXPORT_SYMBOLS) <= set(declared_functions())
+               _lib.STATIC_SCOUT_SYMBOLS + _lib.EXPORT_SYMBOLS + _lib.UVPACK_SYMBOLS) <= set(declared_functions())
     assert L.sdf_version().startswith(b"sdfmesh_b200")
 
 
@@ -55,7 +55,10 @@ def test_header_compiles_as_c():
     from cudasdf_b200 import _lib
     structs = {"sdf_config": _lib.SdfConfig, "sdf_outputs": _lib.SdfOutputs, "sdf_stats": _lib.SdfStats,
                "sdf_surrogate_config": _lib.SurrogateConfig, "sdf_surrogate_stats": _lib.SurrogateStats,
-               "sdf_grid": _lib.SdfGrid, "sdf_batch_scene": _lib.BatchScene, "sdf_batch_stats": _lib.BatchStats}
+               "sdf_grid": _lib.SdfGrid, "sdf_batch_scene": _lib.BatchScene, "sdf_batch_stats": _lib.BatchStats,
+               "sdf_uv_pack_config": _lib.UvPackConfig, "sdf_uv_chart": _lib.UvChart, "sdf_uv_grid": _lib.UvGrid,
+               "sdf_uv_island": _lib.UvIsland, "sdf_uv_placement": _lib.UvPlacement,
+               "sdf_uv_solution": _lib.UvSolution, "sdf_uv_atlas_info": _lib.UvAtlasInfo}
     body = "".join(f'printf("%zu\\n", sizeof({n}));' for n in structs)
     src = ('#include <stdio.h>\n#include "sdfmesh_b200.h"\n'
            'int main(void){ if (sizeof(sdf_primitive) != 160) return 1; ' + body + ' return 0; }\n')
