@@ -317,6 +317,7 @@ def run_ours(args, rank, world):
         eng.configure(make_config(cell, technique=tech, out_mask=mask))  # same grid: buffers and surrogate stay
     if tech == L.TECH_MC and rank == 0:
         out["dropin"] = dropin_host_timing(args, prims, res, voxels)
+        out["uv_atlas"] = uv_atlas_timing(args)
     out["fp32_peak"] = fp32_peak_tflops()
     out["counters"] = count_work(eng, buf, res) if rank == 0 else None
     eng.close()
@@ -327,6 +328,111 @@ def run_ours(args, rank, world):
 
 
 DROPIN_HOST = os.path.join(ROOT, "cudasdf_b200", "dropin_host", "_build", "dropin_host")
+
+# UV atlas packing (the reference's GridUVPacker): the mesh of the reference's own scene at 128^3 with
+# UVs and primitive ids, packed with the configuration of its only caller (main.cpp:1417-1427)
+UV_ATLAS_RES = 128
+UV_ATLAS_WORKLOAD = ("uv atlas of the 128^3 showcase mesh, main.cpp:1417-1427 configuration "
+                     "(2048^2 board, 256 attempts, margin 4, 16 candidates, drop cap 256, seed 1337)")
+
+
+def uv_atlas_config():
+    from cudasdf_b200.uvpack import PackingConfig
+    return PackingConfig.app()
+
+
+def uv_atlas_timing(args):
+    """sdf_uv_atlas_run (charts, islands, the 256 packing attempts, remap) on this library's mesh of the
+    scene, host wall time per atlas with the UVs restored between runs (outside the timed region)."""
+    import torch
+
+    from cudasdf_b200 import _lib as L
+    from cudasdf_b200 import scenes as S
+    from cudasdf_b200.engine import Engine, MeshBuffers, make_config
+    from cudasdf_b200.uvpack import UVAtlas
+    mask = L.OUT_UVS | L.OUT_PRIMIDS
+    eng = Engine()
+    eng.configure(make_config(S.cell_size_for(UV_ATLAS_RES), out_mask=mask))
+    eng.set_scene(S.showcase_scene(0.0, animate=False))
+    buf = MeshBuffers(4_000_000, mask)
+    V = int(eng.extract(buf, 0.0)["total_vertices"])
+    eng.close()
+    uvs0 = buf.uvs[:V].clone()
+    uvs = buf.uvs[:V].clone()
+    prim = buf.primitive_ids[:V].view(torch.float32).clone()
+    cfg = uv_atlas_config()
+    a = UVAtlas()
+    times, info = [], None
+    for i in range(args.warmup + args.steps):
+        uvs.copy_(uvs0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        info = a.run(uvs, prim, cfg)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            times.append((time.perf_counter() - t0) * 1e3)
+    a.close()
+    ms = sorted(times)[len(times) // 2]
+    return {"workload": UV_ATLAS_WORKLOAD, "ms_per_atlas": ms, "unit": "ms (host wall, median)",
+            "ms_pack_kernel": info["ms_pack"], "vertices": V, "charts": info["num_charts"],
+            "attempts": info["num_solutions"], "success": info["success"], "atlas": info["atlas_width"],
+            "fitness": info["fitness"], "launches_per_atlas": 14}
+
+
+def uv_atlas_reference(args):
+    """The reference's GridUVPacker (oracle/_ref/libuvpackref.so, its own sources) on the reference's own
+    mesh of the scene (its marching cubes, oracle/_ref/libsdfref.so), through its host API in main.cpp's
+    order; the wall time of its four calls, which synchronise internally."""
+    from cudasdf_b200 import scenes as S
+    from oracle import reflib as R
+    from oracle import uvpack_oracle as O
+    import numpy as np
+    m = R.RefMesh(S.cell_size_for(UV_ATLAS_RES))
+    m.set_primitives(S.showcase_scene(0.0, animate=False))
+    V = int(m.run(technique=0)["totalVertices"])
+    uvs = m.copy(R.RB_UVS, np.float32, V * 2).reshape(V, 2)
+    prim = m.copy(R.RB_PRIMIDS, np.float32, V)
+    m.close()
+    cfg = uv_atlas_config().as_dict()
+    runs = []
+    for _ in range(max(1, min(args.steps, 3))):
+        r = O.reference_run(uvs, prim, cfg)
+        if not r["loops_end"]:
+            return {"workload": UV_ATLAS_WORKLOAD, "unavailable": "the reference's candidate loop would not end"}
+        runs.append(r["ms_charts"] + r["ms_islands"] + r["ms_pack"] + r["ms_remap"])
+    return {"workload": UV_ATLAS_WORKLOAD, "ms_per_atlas": sorted(runs)[len(runs) // 2],
+            "unit": "ms (host wall, median)", "ms_pack": r["ms_pack"], "ms_islands": r["ms_islands"],
+            "ms_charts": r["ms_charts"], "vertices": V, "success": r["atlas"]["success"],
+            "atlas": r["atlas"]["width"], "runs": len(runs)}
+
+
+def uv_atlas_cpu():
+    """The CPU oracle of the packer (oracle/uvpack_oracle.cpp, the reference's loops, OpenMP over the
+    attempts) on this library's mesh, fed with the attempts' curand draws."""
+    import torch
+
+    from cudasdf_b200 import _lib as L
+    from cudasdf_b200 import scenes as S
+    from cudasdf_b200.engine import Engine, MeshBuffers, make_config
+    from cudasdf_b200.uvpack import random_draws
+    from oracle import uvpack_oracle as O
+    mask = L.OUT_UVS | L.OUT_PRIMIDS
+    eng = Engine()
+    eng.configure(make_config(S.cell_size_for(UV_ATLAS_RES), out_mask=mask))
+    eng.set_scene(S.showcase_scene(0.0, animate=False))
+    buf = MeshBuffers(4_000_000, mask)
+    V = int(eng.extract(buf, 0.0)["total_vertices"])
+    eng.close()
+    uvs = buf.uvs[:V].cpu().numpy()
+    prim = buf.primitive_ids[:V].view(torch.float32).cpu().numpy()
+    cfg = uv_atlas_config().as_dict()
+    draws = random_draws(O.seeds(cfg["random_seed"], cfg["max_iterations"]), 1 << 14)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    r = O.run(uvs, prim, cfg, lambda s: draws, nthreads=cores)
+    secs = time.perf_counter() - t0
+    return {"workload": UV_ATLAS_WORKLOAD, "ms_per_atlas": secs * 1e3, "cores": cores, "kind": "port",
+            "success": r["atlas"]["success"], "atlas": r["atlas"]["width"]}
 
 
 def dropin_host_timing(args, prims, res, voxels):
@@ -652,8 +758,12 @@ def cpu_baseline(args):
     t0 = time.perf_counter()
     O.mc_blocks(sc, g, sample, 0.0, 1)
     t1_mc = (time.perf_counter() - t0) / max(len(sample), 1) * nact
+    try:
+        uv = uv_atlas_cpu()
+    except Exception as ex:  # reported, never required
+        uv = {"error": str(ex)}
     return {"value": float(res) ** 3 / secs / 1e9, "unit": "Gvoxels/s", "cores": cores, "kind": "port",
-            "seconds": secs, "vertices": nverts,
+            "seconds": secs, "vertices": nverts, "uv_atlas": uv,
             "value_1thread": float(res) ** 3 / (t1_scout + t1_mc) / 1e9,
             "sample": f"one whole {res}^3 extraction ({nblocks} blocks scouted, {nact} active blocks meshed, "
                       f"{nverts} vertices) in {secs:.1f} s on {cores} threads; value_1thread: a scout slice of "
@@ -726,8 +836,11 @@ def run_reference(args, rank, world):
     clk = clocks.stop()
     m.close()
     ms = sum(walls) / len(walls)
-    return {"ms": ms, "ms_kernels": sum(kern) / len(kern), "value": float(res) ** 3 / (ms * 1e-3) / 1e9,
-            "stats": st, "clocks": clk, "res": res}
+    out = {"ms": ms, "ms_kernels": sum(kern) / len(kern), "value": float(res) ** 3 / (ms * 1e-3) / 1e9,
+           "stats": st, "clocks": clk, "res": res}
+    if tech == 0:
+        out["uv_atlas"] = uv_atlas_reference(args)
+    return out
 
 
 METRIC = "Gvoxels/s SDF\u2192mesh at 1024\u00b3, surrogate-culled vs plain, identical topology"
@@ -775,6 +888,7 @@ def main():
                                 "path": "the reference's plain exact path (it has no surrogate)",
                                 "l2": "per-stage host syncs of the reference (CudaSDFMesh.cpp:83-88)"},
                      "reference_kernel_ms": r["ms_kernels"], "reference_stats": r["stats"], "clocks": r["clocks"],
+                     "uv_atlas": r.get("uv_atlas"),
                      "reference_cuda_path": {"value": r["value"], "unit": "Gvoxels/s",
                                              "sample": "the reference's own CUDA sources (oracle/_ref) on this GPU: "
                                                        "its per-stage launches, host syncs and count read-backs"},
@@ -823,6 +937,7 @@ def main():
                  "triangles_per_s": (st["total_vertices"] // 3) / (r["ms"] * 1e-3),
                  "bvh_cap_hits": st["bvh_cap_hits"], "clocks": r["clocks"],
                  "dynamic_scene": r.get("dynamic_scene"), "welded": r.get("welded"), "dropin": r.get("dropin"),
+                 "uv_atlas": r.get("uv_atlas"),
                  "gpu_launches": r["launches_per_step"] * args.steps})
     if "surrogate" in r:
         sg = r["surrogate"]

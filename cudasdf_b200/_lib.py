@@ -114,7 +114,8 @@ SCOUT_STATIC_MAX_BLOCKS = 1 << 20  # SDF_SCOUT_STATIC_MAX_BLOCKS of the header
 EXPORT_SYMBOLS = ["sdf_write_obj"]
 UVPACK_SYMBOLS = ["sdf_uv_pack_default_config", "sdf_uv_atlas_create", "sdf_uv_atlas_destroy",
                   "sdf_uv_atlas_extract_charts", "sdf_uv_atlas_create_islands", "sdf_uv_atlas_pack",
-                  "sdf_uv_atlas_remap", "sdf_uv_atlas_run", "sdf_uv_atlas_read", "sdf_uv_pack_random_draws"]
+                  "sdf_uv_atlas_remap", "sdf_uv_atlas_remap_placements", "sdf_uv_atlas_run", "sdf_uv_atlas_read",
+                  "sdf_uv_pack_random_draws"]
 
 
 class UvPackConfig(ctypes.Structure):
@@ -289,6 +290,8 @@ def lib():
     L.sdf_uv_atlas_pack.restype = i
     L.sdf_uv_atlas_remap.argtypes = [vp, vp, vp, ctypes.c_int64, i, vp]
     L.sdf_uv_atlas_remap.restype = i
+    L.sdf_uv_atlas_remap_placements.argtypes = [vp, vp, vp, ctypes.c_int64, i, vp, i, i, i, i, vp]
+    L.sdf_uv_atlas_remap_placements.restype = i
     L.sdf_uv_atlas_run.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.POINTER(UvPackConfig), vp,
                                    ctypes.POINTER(UvAtlasInfo)]
     L.sdf_uv_atlas_run.restype = i

@@ -224,33 +224,65 @@ __device__ bool triangle_overlaps_cell(F2 v0, F2 v1, F2 v2, int cx, int cy) {
     return in_cell(ctr, x0, y0, x1, y1);
 }
 
-// rasterizeIslandKernel (GridUVPacker.cu:171-225) for every triangle of every chart in one launch
+// rasterizeIslandKernel (GridUVPacker.cu:171-225) for every triangle of every chart in one launch. A lane
+// tests the cells of its own triangle when its box has at most 32 cells; a larger box (UV triangles can
+// span hundreds of cells) is tested by the whole warp, one cell per lane. Cells are set with atomicOr,
+// so the order of the tests changes nothing.
 __global__ void k_uv_raster(const sdf_float2* __restrict__ uvs, int64_t T, const int* __restrict__ tri_chart,
                             const int* __restrict__ slot_of_chart, const sdf_uv_island* __restrict__ isl,
                             uint32_t* __restrict__ words, int res) {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x) {
-        const int c = tri_chart[t];
-        if (c < 0) continue;
-        const sdf_uv_island& I = isl[slot_of_chart[c]];
-        const float fr = (float)res, mx0 = (float)I.min_cell_x, my0 = (float)I.min_cell_y;
-        F2 p[3];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * blockDim.x / 32;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x + threadIdx.x - lane; base < T; base += warps * 32) {
+        const int64_t t = base + lane;
+        const int c = t < T ? tri_chart[t] : -1;
+        F2 p[3] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+        int xMin = 0, xMax = 0, yMin = 0, yMax = 0, stride = 0;
+        int64_t off = 0;
+        if (c >= 0) {
+            const sdf_uv_island& I = isl[slot_of_chart[c]];
+            const float fr = (float)res, mx0 = (float)I.min_cell_x, my0 = (float)I.min_cell_y;
 #pragma unroll
-        for (int v = 0; v < 3; v++) {
-            const sdf_float2 uv = uvs[3 * t + v];
-            p[v] = F2{__fmaf_rn(uv.x, fr, -mx0), __fmaf_rn(uv.y, fr, -my0)};
+            for (int v = 0; v < 3; v++) {
+                const sdf_float2 uv = uvs[3 * t + v];
+                p[v] = F2{__fmaf_rn(uv.x, fr, -mx0), __fmaf_rn(uv.y, fr, -my0)};
+            }
+            const float minU = fminf(fminf(p[0].x, p[1].x), p[2].x), maxU = fmaxf(fmaxf(p[0].x, p[1].x), p[2].x);
+            const float minV = fminf(fminf(p[0].y, p[1].y), p[2].y), maxV = fmaxf(fmaxf(p[0].y, p[1].y), p[2].y);
+            const int W = I.width, H = I.height;
+            xMin = max(0, min(__float2int_rz(floorf(minU)), W - 1));
+            xMax = max(0, min(__float2int_rz(ceilf(maxU)), W));
+            yMin = max(0, min(__float2int_rz(floorf(minV)), H - 1));
+            yMax = max(0, min(__float2int_rz(ceilf(maxV)), H));
+            stride = I.mask.stride;
+            off = I.mask.word_offset;
         }
-        const float minU = fminf(fminf(p[0].x, p[1].x), p[2].x), maxU = fmaxf(fmaxf(p[0].x, p[1].x), p[2].x);
-        const float minV = fminf(fminf(p[0].y, p[1].y), p[2].y), maxV = fmaxf(fmaxf(p[0].y, p[1].y), p[2].y);
-        const int W = I.width, H = I.height;
-        const int xMin = max(0, min(__float2int_rz(floorf(minU)), W - 1));
-        const int xMax = max(0, min(__float2int_rz(ceilf(maxU)), W));
-        const int yMin = max(0, min(__float2int_rz(floorf(minV)), H - 1));
-        const int yMax = max(0, min(__float2int_rz(ceilf(maxV)), H));
-        uint32_t* m = words + I.mask.word_offset;
-        for (int y = yMin; y < yMax; y++)
-            for (int x = xMin; x < xMax; x++)
-                if (triangle_overlaps_cell(p[0], p[1], p[2], x, y))
-                    atomicOr(&m[(int64_t)y * I.mask.stride + (x >> 5)], 1u << (x & 31));
+        const int wx = max(xMax - xMin, 0), ncell = wx * max(yMax - yMin, 0);
+        const bool big = ncell > 32;
+        if (c >= 0 && !big) {
+            uint32_t* m = words + off;
+            for (int y = yMin; y < yMax; y++)
+                for (int x = xMin; x < xMax; x++)
+                    if (triangle_overlaps_cell(p[0], p[1], p[2], x, y))
+                        atomicOr(&m[(int64_t)y * stride + (x >> 5)], 1u << (x & 31));
+        }
+        unsigned todo = __ballot_sync(kFull, c >= 0 && big);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            F2 q[3];
+#pragma unroll
+            for (int v = 0; v < 3; v++) q[v] = F2{__shfl_sync(kFull, p[v].x, src), __shfl_sync(kFull, p[v].y, src)};
+            const int qx = __shfl_sync(kFull, xMin, src), qy = __shfl_sync(kFull, yMin, src);
+            const int qw = __shfl_sync(kFull, wx, src), qn = __shfl_sync(kFull, ncell, src);
+            const int qs = __shfl_sync(kFull, stride, src);
+            uint32_t* m = words + __shfl_sync(kFull, off, src);
+            for (int k = lane; k < qn; k += 32) {
+                const int x = qx + k % qw, y = qy + k / qw;
+                if (triangle_overlaps_cell(q[0], q[1], q[2], x, y))
+                    atomicOr(&m[(int64_t)y * qs + (x >> 5)], 1u << (x & 31));
+            }
+        }
     }
 }
 
@@ -664,45 +696,53 @@ __global__ void __launch_bounds__(kPackThreads) k_uv_pack(const sdf_uv_island* _
     }
 }
 
-// the choice of PackIslands (GridUVPacker.cu:1188-1214, 1403-1420); one warp
+// the atlas PackIslands returns (GridUVPacker.cu:1188-1214, 1403-1420)
 struct AtlasResult {
     int32_t success, width, height, placed, best, open;
     float fitness, scaling;
 };
 
+// The choice of the attempt, one warp. The reference's loop keeps the first attempt with the most islands placed and replaces it
+// only by a later one with as many and a strictly higher fitness: the maximum of
+// (placed, fitness, -index), which the warp reduces in one 64-bit key (fitness >= 0, so its bits order).
 __global__ void k_uv_select(const sdf_uv_solution* __restrict__ sols, int nsol, int num_islands, int G,
                             const sdf_uv_placement* __restrict__ placements, int n,
                             sdf_uv_placement* __restrict__ best_pl, AtlasResult* __restrict__ out) {
-    __shared__ int s_best;
-    if (threadIdx.x == 0) {
-        int best = -1, most = 0, open = 0;
-        float bestFit = 0.0f;
-        for (int i = 0; i < nsol; i++) {
-            const int p = sols[i].num_placed;
-            open |= sols[i].flags & UVP_CANDIDATE_LOOP_OPEN;
-            if (p > most) { most = p; best = i; bestFit = sols[i].fitness; }
-            else if (p == most && sols[i].fitness > bestFit) { best = i; bestFit = sols[i].fitness; }
+    const int lane = threadIdx.x;
+    unsigned long long key = 0ull;
+    unsigned open = 0u;
+    for (int i = lane; i < nsol; i += 32) {
+        const sdf_uv_solution s = sols[i];
+        open |= (unsigned)(s.flags & UVP_CANDIDATE_LOOP_OPEN);
+        if (s.num_placed > 0) {
+            const unsigned long long k = ((unsigned long long)s.num_placed << 40) |
+                                         ((unsigned long long)__float_as_uint(s.fitness) << 8) |
+                                         (unsigned long long)(255 - i);
+            key = max(key, k);
         }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) key = max(key, __shfl_xor_sync(kFull, key, o));
+    open = __reduce_or_sync(kFull, open);
+    const int best = key ? 255 - (int)(key & 255ull) : -1;
+    if (lane == 0) {
         AtlasResult r;
-        r.success = 0; r.width = 0; r.height = 0; r.placed = 0; r.best = -1; r.open = open;
+        r.success = 0; r.width = 0; r.height = 0; r.placed = 0; r.best = best; r.open = open ? 1 : 0;
         r.fitness = 0.0f; r.scaling = 1.0f;
-        if (best >= 0 && most > 0) {
-            const int m = max(sols[best].utilized_width, sols[best].utilized_height);
-            r.success = sols[best].num_placed == num_islands;
+        if (best >= 0) {
+            const sdf_uv_solution s = sols[best];
+            const int m = max(s.utilized_width, s.utilized_height);
+            r.success = s.num_placed == num_islands;
             r.width = m;
             r.height = m;
-            r.placed = sols[best].num_placed;
-            r.best = best;
-            r.fitness = sols[best].fitness;
+            r.placed = s.num_placed;
+            r.fitness = s.fitness;
             r.scaling = m > 0 ? __fdiv_rn((float)G, (float)m) : 1.0f;
         }
         *out = r;
-        s_best = r.best;
     }
-    __syncthreads();
-    if (s_best >= 0)
-        for (int i = threadIdx.x; i < sols[s_best].num_placed && i < n; i += blockDim.x)
-            best_pl[i] = placements[(size_t)s_best * n + i];
+    if (best >= 0)
+        for (int i = lane; i < sols[best].num_placed && i < n; i += 32) best_pl[i] = placements[(size_t)best * n + i];
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -322,7 +322,7 @@ sdf_status sdf_uv_atlas_pack(sdf_uv_atlas* a, const sdf_uv_pack_config* c, void*
     uvp::k_uv_pack<<<nsol, uvp::kPackThreads, sizeof(unsigned short) * (size_t)G, s>>>(
         a->d_isl, pa, a->d_seeds, a->d_words, a->d_rb, a->d_prof, a->d_boards, a->d_sols, a->d_pl);
     cudaEventRecord(a->ev1, s);
-    uvp::k_uv_select<<<1, 256, 0, s>>>(a->d_sols, nsol, nisl, G, a->d_pl, pa.n, a->d_best, a->d_res);
+    uvp::k_uv_select<<<1, 32, 0, s>>>(a->d_sols, nsol, nisl, G, a->d_pl, pa.n, a->d_best, a->d_res);
     if (check_launch() != cudaSuccess) return SDF_ERR_CUDA;
     uvp::AtlasResult res;
     cudaMemcpyAsync(&res, a->d_res, sizeof(res), cudaMemcpyDeviceToHost, s);
@@ -350,22 +350,43 @@ sdf_status sdf_uv_atlas_pack(sdf_uv_atlas* a, const sdf_uv_pack_config* c, void*
     return SDF_OK;
 }
 
+namespace {
+sdf_status uv_remap(sdf_uv_atlas* a, sdf_float2* d_uvs, const float* d_prim, int64_t nv, int res,
+                    const sdf_uv_placement* d_pl, int np, int atlas_w, int atlas_h, cudaStream_t s) {
+    const int nc = (int)a->charts.size();
+    if (!ensure_buffer(a->d_cp, a->cp_cap, (size_t)std::max(nc, 1))) return SDF_ERR_NOMEM;
+    const int nisl = (int)a->islands.size();
+    uvp::k_uv_remap_init<<<uv_grid(nisl), 256, 0, s>>>(a->d_isl, nisl, a->d_cp);
+    uvp::k_uv_remap_place<<<uv_grid(np), 256, 0, s>>>(d_pl, np, nc, a->d_cp);
+    const float denom = (float)std::max(atlas_w, atlas_h);
+    if (nv > 0)
+        uvp::k_uv_remap<<<uv_grid(nv), 256, 0, s>>>(d_uvs, d_prim, nv, a->d_chart_of_id, a->R, a->d_cp, res, denom);
+    return check_launch() == cudaSuccess ? SDF_OK : SDF_ERR_CUDA;
+}
+}  // namespace
+
 sdf_status sdf_uv_atlas_remap(sdf_uv_atlas* a, sdf_float2* d_uvs, const float* d_primitive_ids, int64_t num_vertices,
                               int32_t grid_resolution, void* stream) {
     if (!a || num_vertices < 0 || (num_vertices > 0 && (!d_uvs || !d_primitive_ids))) return SDF_ERR_INVALID;
     // "Cannot remap UVs - invalid atlas" (GridUVPacker.cu:1450-1453): the UVs stay as they are
     if (!a->have_pack || !a->info.success || a->best.empty()) return SDF_OK;
+    return uv_remap(a, d_uvs, d_primitive_ids, num_vertices, grid_resolution, a->d_best, (int)a->best.size(),
+                    a->info.atlas_width, a->info.atlas_height, (cudaStream_t)stream);
+}
+
+sdf_status sdf_uv_atlas_remap_placements(sdf_uv_atlas* a, sdf_float2* d_uvs, const float* d_primitive_ids,
+                                         int64_t num_vertices, int32_t grid_resolution,
+                                         const sdf_uv_placement* placements, int32_t num_placements,
+                                         int32_t success, int32_t atlas_width, int32_t atlas_height, void* stream) {
+    if (!a || num_vertices < 0 || num_placements < 0 || (num_vertices > 0 && (!d_uvs || !d_primitive_ids)) ||
+        (num_placements > 0 && !placements) || !a->have_islands)
+        return SDF_ERR_INVALID;
+    if (!success || num_placements == 0) return SDF_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    const int nc = (int)a->charts.size();
-    if (!ensure_buffer(a->d_cp, a->cp_cap, (size_t)std::max(nc, 1))) return SDF_ERR_NOMEM;
-    const int nisl = (int)a->islands.size(), np = (int)a->best.size();
-    uvp::k_uv_remap_init<<<uv_grid(nisl), 256, 0, s>>>(a->d_isl, nisl, a->d_cp);
-    uvp::k_uv_remap_place<<<uv_grid(np), 256, 0, s>>>(a->d_best, np, nc, a->d_cp);
-    const float denom = (float)std::max(a->info.atlas_width, a->info.atlas_height);
-    if (num_vertices > 0)
-        uvp::k_uv_remap<<<uv_grid(num_vertices), 256, 0, s>>>(d_uvs, d_primitive_ids, num_vertices, a->d_chart_of_id,
-                                                              a->R, a->d_cp, grid_resolution, denom);
-    return check_launch() == cudaSuccess ? SDF_OK : SDF_ERR_CUDA;
+    if (!ensure_buffer(a->d_best, a->best_cap, (size_t)num_placements)) return SDF_ERR_NOMEM;
+    cudaMemcpyAsync(a->d_best, placements, sizeof(sdf_uv_placement) * (size_t)num_placements, cudaMemcpyHostToDevice, s);
+    return uv_remap(a, d_uvs, d_primitive_ids, num_vertices, grid_resolution, a->d_best, num_placements, atlas_width,
+                    atlas_height, s);
 }
 
 sdf_status sdf_uv_atlas_run(sdf_uv_atlas* a, sdf_float2* d_uvs, const float* d_primitive_ids, int64_t num_vertices,

@@ -568,6 +568,13 @@ sdf_status sdf_uv_atlas_pack(sdf_uv_atlas* a, const sdf_uv_pack_config* c, void*
  * changes when the last packing is not a success. */
 sdf_status sdf_uv_atlas_remap(sdf_uv_atlas* a, sdf_float2* d_uvs, const float* d_primitive_ids, int64_t num_vertices,
                               int32_t grid_resolution, void* stream);
+/* RemapUVsToAtlas with the atlas given explicitly (the reference's PackedAtlas argument): its
+ * placements (host array), squared width and height; the islands of the last sdf_uv_atlas_create_islands.
+ * The UVs stay as they are when success is 0 or num_placements is 0. */
+sdf_status sdf_uv_atlas_remap_placements(sdf_uv_atlas* a, sdf_float2* d_uvs, const float* d_primitive_ids,
+                                         int64_t num_vertices, int32_t grid_resolution,
+                                         const sdf_uv_placement* placements, int32_t num_placements,
+                                         int32_t success, int32_t atlas_width, int32_t atlas_height, void* stream);
 /* The four steps in main.cpp's order (main.cpp:1429-1442). */
 sdf_status sdf_uv_atlas_run(sdf_uv_atlas* a, sdf_float2* d_uvs, const float* d_primitive_ids, int64_t num_vertices,
                             const sdf_uv_pack_config* c, void* stream, sdf_uv_atlas_info* info);

@@ -213,3 +213,33 @@ def test_atlas_has_no_overlap():
         assert sub.shape == bits.shape and not (sub & bits).any()
         sub |= bits
     assert g["info"]["atlas_width"] >= max(int(p["grid_x"]) for p in g["best"])
+
+
+UVPACK_HOST = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "cudasdf_b200", "dropin_host",
+                           "_build", "uvpack_host")
+
+
+@pytest.mark.skipif(not os.path.exists(UVPACK_HOST), reason="uvpack_host not built")
+def test_cpp_api_host_matches(tmp_path):
+    """The reference's call sequence (main.cpp:1417-1442) written against include/grid_uv_packer_b200.hpp
+    (cudasdf_b200/dropin_host/uvpack_host.cpp) gives the atlas and UVs of the C entry points and of the
+    oracle, with the app's full configuration (256 attempts)."""
+    import json
+    import subprocess
+    uvs, prim = scene("showcase")
+    cfg = dict(O.APP_CONFIG)
+    fu, fp, fo = tmp_path / "uvs.bin", tmp_path / "prim.bin", tmp_path / "out.bin"
+    uvs.tofile(fu)
+    prim.tofile(fp)
+    r = subprocess.run([UVPACK_HOST, str(fu), str(fp), str(len(prim)), str(fo), "2"], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    host = json.loads(r.stdout.strip().splitlines()[-1])
+    g = ours(uvs, prim, cfg)
+    assert host["success"] == g["info"]["success"] == 1
+    assert (host["atlas_width"], host["atlas_height"]) == (g["info"]["atlas_width"], g["info"]["atlas_height"])
+    assert np.array_equal(np.array(host["placements"], np.int32).reshape(-1, 4), g["best"].view(np.int32).reshape(-1, 4))
+    out = np.fromfile(fo, np.float32).reshape(-1, 2)
+    assert np.array_equal(out.view(np.uint32), g["uvs"].view(np.uint32))
+    o = O.run(uvs, prim, cfg, draws_for)
+    assert np.array_equal(out.view(np.uint32), o["uvs"].view(np.uint32))
