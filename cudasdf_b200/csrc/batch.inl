@@ -157,6 +157,9 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
         D.counts = B.packet_counts;
         D.offsets = B.packet_offsets;
         D.qef_debug = nullptr;
+        D.proj = nullptr;  // the projection steps stay in k_dc_solve
+        D.proj_nsum = nullptr;
+        D.proj_cap = 0;
         record(cudaMemsetAsync(B.b2a, 0xFF, (size_t)nb * sizeof(int), st));
         k_dc_block_map<<<(nb + 255) / 256, 256, 0, st>>>(B.list, &ctrl->active_count, (int)nb, (int)nb, B.b2a);
         // block rows by the shared-halo block field, then the cells classified from the rows

@@ -21,6 +21,12 @@ struct DcBuffers {
     unsigned* counts;         // per packed cell: has-vertex (mark) / quad vertex count (count quads)
     unsigned* offsets;        // per packed cell: scanned counts
     float4* qef_debug;        // optional, per DC vertex: mass-point QEF vertex before projection, w = 1 if FP64
+    // optional, mass-point projection: per DC vertex below proj_cap, two float4 (start point in cell-local
+    // coordinates, active block; mean Hermite normal, cell | has-direction << 16) for k_dc_project, and
+    // the raw Hermite normal sum when cell normals are written
+    float4* proj;
+    float4* proj_nsum;
+    unsigned proj_cap;
 };
 
 struct DcSolveParams {
@@ -504,6 +510,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
             // evaluates map() at the float point corner + y. A fixed direction per cell keeps the step
             // independent of finite differences of the field at the vertex, and every operation is
             // rounded on its own, so a float32 restatement on the host reproduces the steps.
+            // The steps of a block's few cells leave most warps of the CTA idle at the next barrier, so
+            // every cell whose vertex slot has a projection record is handed to k_dc_project (32 cells
+            // per warp over all blocks) with its start point and direction; the others finish here.
+            const bool handoff = P.solver == SDF_DC_SOLVER_MASSPOINT && P.projection_iters > 0 && B.proj;
             if (P.solver == SDF_DC_SOLVER_MASSPOINT && P.projection_iters > 0) {
                 const float margin = MUL(0.10f, g.cell), hi = ADD(g.cell, margin);
                 for (int i = threadIdx.x; i < (int)ncells; i += blockDim.x) {
@@ -512,10 +522,31 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
                     S.cell_x[i] = f3(CLAMP(y.x, -margin, hi), CLAMP(y.y, -margin, hi), CLAMP(y.z, -margin, hi));
                 }
                 __syncthreads();
-                // each cell stays with one lane of one warp for all steps
+                if (handoff)
+                    for (int i = threadIdx.x; i < (int)ncells; i += blockDim.x) {
+                        const unsigned v = S.cell_vidx[i];
+                        if (v >= B.proj_cap) continue;
+                        float3 nsum = f3(0.f, 0.f, 0.f), nbar = f3(0.f, 0.f, 0.f);
+                        const int h0 = S.cell_h0[i], m = S.cell_m[i];
+                        for (int q = 0; q < m; ++q) {
+                            float3 nq;
+                            if (unit_normal_rn(S.h_n[h0 + q], nq)) nsum = add3(nsum, nq);
+                        }
+                        const bool has_dir = unit_normal_rn(nsum, nbar);
+                        const float3 y = S.cell_x[i];
+                        B.proj[2 * (size_t)v] = make_float4(y.x, y.y, y.z, __int_as_float(a));
+                        B.proj[2 * (size_t)v + 1] =
+                            make_float4(nbar.x, nbar.y, nbar.z, __uint_as_float(S.cell_tid[i] | (has_dir ? 0x10000u : 0u)));
+                        if (B.cell_normals && B.proj_nsum) {
+                            float3 raw = f3(0.f, 0.f, 0.f);
+                            for (int q = 0; q < m; ++q) raw = add3(raw, S.h_n[h0 + q]);
+                            B.proj_nsum[v] = make_float4(raw.x, raw.y, raw.z, 0.f);
+                        }
+                    }
+                // each remaining cell stays with one lane of one warp for all steps
                 for (int base = warp * 32; base < (int)ncells; base += nwarps * 32) {
                     const int i = base + lane;
-                    const bool valid = i < (int)ncells;
+                    const bool valid = i < (int)ncells && !(handoff && S.cell_vidx[i] < B.proj_cap);
                     float3 cm = f3(0.f, 0.f, 0.f), nbar = f3(0.f, 0.f, 0.f), y = f3(0.f, 0.f, 0.f);
                     bool has_dir = false;
                     if (valid) {
@@ -544,6 +575,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
             }
             // soft clamp, hard clamp to the cell, blend towards the cell centre (:1556-1577)
             for (int i = threadIdx.x; i < (int)ncells; i += blockDim.x) {
+                if (handoff && S.cell_vidx[i] < B.proj_cap) continue;  // k_dc_project finishes it
                 const CellInfo c = cell_info(g, bx, by, bz, S.cell_tid[i]);
                 float3 x = S.cell_x[i];
                 const float3 cmin = grid_loc(g, c.x, c.y, c.z);
@@ -563,7 +595,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
             if (B.cell_normals) {
                 for (int base = warp * 32; base < (int)ncells; base += nwarps * 32) {
                     const int i = base + lane;
-                    const bool valid = i < (int)ncells;
+                    const bool valid = i < (int)ncells && !(handoff && S.cell_vidx[i] < B.proj_cap);
                     const float3 x = valid ? S.cell_x[i] : f3(0.f, 0.f, 0.f);
                     const float3 nref = normal_warp(sc, x, valid, time, g.cell, diag);
                     if (valid) {
@@ -579,6 +611,96 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
             }
             __syncthreads();
             cursor = next > cursor ? next : 512;
+        }
+    }
+}
+
+// The mass-point projection steps and the finishing of the DC vertices handed off by k_dc_solve: 32
+// vertices per warp task in vertex order (so a warp's cells are neighbours from one or two blocks),
+// each lane taking x <- x - f(x) n along its cell's mean Hermite normal, in cell-local coordinates kept
+// in the cell widened by 0.1 cell, then the clamps, the blend and the encoding of k_dc_solve. The same
+// operations as there, so the vertices are the same; a warp walks one scene's BVH at a time.
+__global__ void __launch_bounds__(BLK_THREADS) k_dc_project(GridView g0, SceneView sc0, float time, ActiveView av,
+                                                           DcBuffers B, DcSolveParams P,
+                                                           const unsigned* __restrict__ nverts, unsigned* ticket,
+                                                           Diag* diag) {
+    const unsigned n = min(min(*nverts, B.proj_cap), P.max_cell_vertices);
+    const int nact = active_count(av);
+    const int tasks = nact > 0 ? (int)((n + 31u) / 32u) : 0;
+    const int lane = threadIdx.x & 31;
+    const unsigned FULL = 0xffffffffu;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = (int)atomicAdd(ticket, 1u);
+        t = __shfl_sync(FULL, t, 0);
+        if (t >= tasks) break;
+        const unsigned v = (unsigned)t * 32u + (unsigned)lane;
+        const unsigned vv = v < n ? v : (unsigned)t * 32u;  // lanes past the end read the task's first record
+        const float4 r0 = B.proj[2 * (size_t)vv], r1 = B.proj[2 * (size_t)vv + 1];
+        const int ra = __float_as_int(r0.w);
+        const unsigned cw = __float_as_uint(r1.w);
+        // every vertex below n has a record from k_dc_solve; a record that names no active block or cell
+        // is skipped rather than followed
+        const bool ok = ra >= 0 && ra < nact && (cw & 0xFFFFu) < 512u;
+        const bool live = v < n && ok;
+        const int a = ok ? ra : 0;
+        const bool has_dir = live && ((cw >> 16) & 1u);
+        GridView g = g0;
+        SceneView sc = sc0;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[a], g, sc, lin, bbase);
+        int bx, by, bz;
+        block_coord(g, lin, bx, by, bz);
+        const CellInfo c = cell_info(g, bx, by, bz, ok ? (int)(cw & 0xFFFFu) : 0);
+        const float3 cm = grid_loc(g, c.x, c.y, c.z);
+        const float3 nbar = f3(r1.x, r1.y, r1.z);
+        float3 y = f3(r0.x, r0.y, r0.z);
+        const float margin = MUL(0.10f, g.cell), hi = ADD(g.cell, margin);
+        for (int it = 0; it < P.projection_iters; ++it) {
+            unsigned pending = __ballot_sync(FULL, live);
+            while (pending) {
+                const unsigned lead = __shfl_sync(FULL, bbase, __ffs(pending) - 1);
+                const bool mine = live && bbase == lead && ((pending >> lane) & 1u);
+                SceneView scw = sc;
+                if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead)].sc;
+                MapState<false> st;
+                map_warp<false>(scw, add3(cm, y), mine && has_dir, time, st, diag);
+                if (mine && has_dir && isfinite(st.d)) {
+                    const float3 yn = sub3(y, scl3(nbar, st.d));
+                    y = f3(CLAMP(yn.x, -margin, hi), CLAMP(yn.y, -margin, hi), CLAMP(yn.z, -margin, hi));
+                }
+                pending &= ~__ballot_sync(FULL, mine);
+            }
+        }
+        // soft clamp, hard clamp to the cell, blend towards the cell centre (:1556-1577)
+        float3 x = add3(cm, y);
+        const float3 cmax = f3(ADD(cm.x, g.cell), ADD(cm.y, g.cell), ADD(cm.z, g.cell));
+        x = f3(CLAMP(x.x, SUB(cm.x, margin), ADD(cmax.x, margin)), CLAMP(x.y, SUB(cm.y, margin), ADD(cmax.y, margin)),
+               CLAMP(x.z, SUB(cm.z, margin), ADD(cmax.z, margin)));
+        x = f3(CLAMP(x.x, cm.x, cmax.x), CLAMP(x.y, cm.y, cmax.y), CLAMP(x.z, cm.z, cmax.z));
+        const float3 ctr = f3(FMA(0.5f, g.cell, cm.x), FMA(0.5f, g.cell, cm.y), FMA(0.5f, g.cell, cm.z));
+        x = lerp3(ctr, x, P.qef_blend);
+        if (live) B.cell_verts[v] = encode_vertex(x, cm, g.cell);
+        // vertex normal: averaged Hermite normals, oriented by the SDF gradient at the vertex
+        if (B.cell_normals && B.proj_nsum) {
+            unsigned pending = __ballot_sync(FULL, live);
+            while (pending) {
+                const unsigned lead = __shfl_sync(FULL, bbase, __ffs(pending) - 1);
+                const bool mine = live && bbase == lead && ((pending >> lane) & 1u);
+                SceneView scw = sc;
+                if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead)].sc;
+                const float3 nref = normal_warp(scw, x, mine, time, g.cell, diag);
+                if (mine) {
+                    const float4 r = B.proj_nsum[v];
+                    const float3 nsum = f3(r.x, r.y, r.z);
+                    const float len = SQRT(dot3(nsum, nsum));
+                    float3 nout = (len > 1e-6f) ? f3(DIV(nsum.x, len), DIV(nsum.y, len), DIV(nsum.z, len)) : nref;
+                    if (dot3(nout, nref) < 0.f) nout = f3(-nout.x, -nout.y, -nout.z);
+                    B.cell_normals[v] = encode_normal(nout);
+                }
+                pending &= ~__ballot_sync(FULL, mine);
+            }
         }
     }
 }

@@ -103,6 +103,10 @@ struct EngineImpl {
     size_t dc_cap = 0;
     float4* dc_qef = nullptr;              // debug bit 1: mass-point QEF vertices before projection
     size_t dc_qef_cap = 0;
+    float4* dc_proj = nullptr;             // mass-point projection records (k_dc_project), 2 per vertex
+    float4* dc_proj_nsum = nullptr;        //   and the Hermite normal sums when cell normals are kept
+    size_t dc_proj_cap = 0, dc_proj_nsum_cap = 0;
+    unsigned last_dc_vertices = 0;         // DC vertices of the last collected extraction
     unsigned char* ctrl_region = nullptr;  // Ctrl, then the three scan regions
     size_t ctrl_bytes = 0;
     size_t scanA_off = 0, scanB_off = 0, scanD_off = 0, scanC_off = 0;
@@ -161,7 +165,8 @@ struct EngineImpl {
     void release() {
         void* ptrs[] = {d_prims, d_nodes, flags, list, fields, block_totals, block_offsets, packet_counts,
                         packet_offsets, b2a, masks, dc_voff, dc_verts, dc_norms, ctrl_region, eval_diag, miss,
-                        cell_words, bvh_work, weld_bits, weld_prefix, weld_totals, weld_base, dc_qef};
+                        cell_words, bvh_work, weld_bits, weld_prefix, weld_totals, weld_base, dc_qef,
+                        dc_proj, dc_proj_nsum};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         d_prims = nullptr; d_nodes = nullptr; flags = nullptr; list = nullptr; fields = nullptr;
@@ -176,6 +181,8 @@ struct EngineImpl {
         weld_cap = 0;
         dc_qef = nullptr;
         dc_qef_cap = 0;
+        dc_proj = dc_proj_nsum = nullptr;
+        dc_proj_cap = dc_proj_nsum_cap = 0;
         prims_cap = nodes_cap = dc_cap = packet_cap = miss_cap = cell_words_cap = bvh_work_cap = 0;
         if (h_bvh_ctl) cudaFreeHost(h_bvh_ctl);
         h_bvh_ctl = nullptr;
@@ -667,6 +674,26 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
             if (dev_alloc(E.dc_qef, E.dc_cap) != SDF_OK) return SDF_ERR_NOMEM;
             E.dc_qef_cap = E.dc_cap;
         }
+        // projection records for k_dc_project: sized by the last extraction's vertices (an eighth of the
+        // cells at first); vertices beyond them are projected inside k_dc_solve, so no size is wrong
+        if (C.dc_solver == SDF_DC_SOLVER_MASSPOINT && C.projection_iters > 0) {
+            const size_t pw = std::min<size_t>(E.dc_cap, std::max<size_t>(E.dc_cap / 8, (size_t)E.last_dc_vertices +
+                                                                                          E.last_dc_vertices / 4));
+            if (E.dc_proj_cap < pw) {
+                if (E.dc_proj) cudaFree(E.dc_proj);
+                E.dc_proj = nullptr;
+                E.dc_proj_cap = 0;
+                if (dev_alloc(E.dc_proj, 2 * pw) == SDF_OK) E.dc_proj_cap = pw;
+                cudaGetLastError();  // without records every vertex is projected in k_dc_solve
+            }
+            if ((E.debug & 1) && E.dc_proj_nsum_cap < E.dc_proj_cap) {
+                if (E.dc_proj_nsum) cudaFree(E.dc_proj_nsum);
+                E.dc_proj_nsum = nullptr;
+                E.dc_proj_nsum_cap = 0;
+                if (dev_alloc(E.dc_proj_nsum, E.dc_proj_cap) == SDF_OK) E.dc_proj_nsum_cap = E.dc_proj_cap;
+                cudaGetLastError();
+            }
+        }
     }
     cudaGetLastError();
     auto t0 = std::chrono::high_resolution_clock::now();
@@ -784,6 +811,11 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
         B.counts = E.packet_counts;
         B.offsets = E.packet_offsets;
         B.qef_debug = (E.debug & 2) ? E.dc_qef : nullptr;
+        const bool project = C.dc_solver == SDF_DC_SOLVER_MASSPOINT && C.projection_iters > 0 && E.dc_proj &&
+                             (!B.cell_normals || E.dc_proj_nsum_cap >= E.dc_proj_cap);
+        B.proj = project ? E.dc_proj : nullptr;
+        B.proj_nsum = project && B.cell_normals ? E.dc_proj_nsum : nullptr;
+        B.proj_cap = project ? (unsigned)std::min<size_t>(E.dc_proj_cap, 0xFFFFFFFFu) : 0u;
         record(cudaMemsetAsync(E.b2a, 0xFF, (size_t)nb * sizeof(int), st));
         k_dc_block_map<<<(cap + 255) / 256, 256, 0, st>>>(E.list, &ctrl->active_count, cap, nb, E.b2a);
         check_launch();
@@ -809,6 +841,11 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
         k_dc_solve<<<persistent_grid(k_dc_solve, SOLVE_THREADS, cap, solve_smem), SOLVE_THREADS, solve_smem, st>>>(
             gv, sv, time, av, E.fields, B, sp, &ctrl->tickets[1], diag);
         check_launch();
+        if (project) {
+            k_dc_project<<<persistent_grid(k_dc_project, BLK_THREADS, std::max(1, (int)(B.proj_cap / 256))), BLK_THREADS,
+                           0, st>>>(gv, sv, time, av, B, sp, &ctrl->dc_vertices, &ctrl->tickets[6], diag);
+            check_launch();
+        }
         if (E.timing) cudaEventRecord(E.ev[3], st);
         k_dc_count_quads<<<std::min(cap, num_sms() * 4), 512, 0, st>>>(gv, av, B, E.packet_counts, E.block_totals);
         check_launch();
@@ -891,6 +928,7 @@ static sdf_status engine_collect(EngineImpl& E, int slot, sdf_stats* stats, bool
         stats->total_vertices = h.total_vertices;
         stats->written_vertices = std::min<int64_t>(h.total_vertices, P.max_vertices);
         stats->dc_cell_vertices = h.dc_vertices;
+        if (P.dc) E.last_dc_vertices = h.dc_vertices;
         stats->bvh_cap_hits = (int64_t)h.diag.cap_hits;
         stats->scouted_blocks = P.culled ? (int64_t)h.diag.scouted : (int64_t)P.nb;
         stats->dc_fp64_cells = (int64_t)h.diag.fp64_cells;

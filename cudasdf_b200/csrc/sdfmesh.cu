@@ -389,6 +389,9 @@ static DcBuffers dc_buffers_of(const sdf_grid& g) {
     b.counts = g.d_packetVertexCounts;
     b.offsets = g.d_packetVertexOffsets;
     b.qef_debug = nullptr;
+    b.proj = nullptr;
+    b.proj_nsum = nullptr;
+    b.proj_cap = 0;
     return b;
 }
 
