@@ -243,3 +243,76 @@ def test_cpp_api_host_matches(tmp_path):
     assert np.array_equal(out.view(np.uint32), g["uvs"].view(np.uint32))
     o = O.run(uvs, prim, cfg, draws_for)
     assert np.array_equal(out.view(np.uint32), o["uvs"].view(np.uint32))
+
+
+def synthetic_soup(seed, nchart=24, tris=150, nan_frac=0.01):
+    """UV triangles in random patches, one primitive id per patch, with the inputs a mesh can hold and
+    the reference reads in its own way: fractional ids (rounded by + 0.5 and truncation), -1 (which
+    rounds to chart 0), -2 (no chart), NaN UVs in a few vertices (fminf skips them), triangles with a
+    vertex on a cell boundary, degenerate (zero-area) triangles and triangles spanning tens of cells."""
+    rng = np.random.default_rng(seed)
+    uvs, ids = [], []
+    for c in range(nchart):
+        su, sv = rng.uniform(0.3, 1.2, 2)
+        o = rng.uniform(-0.2, 0.6, 2)
+        base = rng.uniform(0, 1, (tris, 1, 2)) * [su, sv] + o
+        t = base + rng.normal(0, 0.04, (tris, 3, 2))
+        t[: tris // 10] = base[: tris // 10] + rng.uniform(-0.4, 0.4, (tris // 10, 3, 2))  # large triangles
+        t[tris // 10: tris // 10 + 5, 1] = t[tris // 10: tris // 10 + 5, 0]                 # degenerate
+        k = slice(tris // 10 + 5, tris // 10 + 15)
+        t[k] = np.round(t[k] * 64) / 64                                                    # on cell corners
+        uvs.append(t.reshape(-1, 2))
+        pid = float(c) + rng.choice([0.0, 0.3, -0.4])
+        ids.append(np.full(tris * 3, pid, np.float32))
+    uv = np.concatenate(uvs).astype(np.float32)
+    pid = np.concatenate(ids)
+    T = len(pid) // 3
+    tri_ids = pid.reshape(T, 3)
+    pick = rng.choice(T, T // 50, replace=False)
+    tri_ids[pick[: len(pick) // 2], 0] = -1.0
+    tri_ids[pick[len(pick) // 2:], 0] = -2.0
+    nanv = rng.choice(len(uv), int(len(uv) * nan_frac), replace=False)
+    uv[nanv, rng.integers(0, 2, len(nanv))] = np.nan
+    order = rng.permutation(T)
+    return uv.reshape(T, 3, 2)[order].reshape(-1, 2).copy(), tri_ids[order].reshape(-1).copy()
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_adversarial_soup_matches_oracle_and_reference(seed):
+    uvs, prim = synthetic_soup(seed)
+    cfg = dict(O.APP_CONFIG, max_iterations=16)
+    g = ours(uvs, prim, cfg)
+    o = O.run(uvs, prim, cfg, draws_for)
+    check_charts(g, o["charts"])
+    check_islands(g, o["islands"])
+    assert np.array_equal(g["best"].view(np.int32).reshape(-1, 4), o["atlas"]["placements"])
+    # NaN UVs stay NaN (the GPU writes its canonical NaN, the host keeps the input's bits); every other
+    # value bit for bit
+    nan = np.isnan(g["uvs"])
+    assert np.array_equal(nan, np.isnan(o["uvs"])) and nan.any()
+    assert np.array_equal(g["uvs"][~nan].view(np.uint32), o["uvs"][~nan].view(np.uint32))
+    if HAVE_REF and o["loops_end"]:
+        ref = O.reference_run(uvs, prim, cfg)
+        assert np.array_equal(g["charts"]["primitive_id"], ref["charts"]["prim"])
+        for slot, rg in enumerate(O.reference_grids(ref)):
+            for name, v in rg.items():
+                assert np.array_equal(g["grids"][slot][name], v), (slot, name)
+        assert np.array_equal(g["best"].view(np.int32).reshape(-1, 4), ref["atlas"]["placements"])
+        assert np.array_equal(g["uvs"].view(np.uint32), ref["uvs"].view(np.uint32))
+
+
+def test_partial_triangle_and_limits():
+    """A partial last triangle is not read; ids of 2^24 and more are refused (SDF_ERR_INVALID)."""
+    import torch
+    from cudasdf_b200 import _lib as L
+    from cudasdf_b200.uvpack import UVAtlas
+    uvs, prim = synthetic_soup(3, nchart=6, tris=40)
+    a = UVAtlas()
+    du, dp = torch.from_numpy(uvs[:-1].copy()).cuda(), torch.from_numpy(prim[:-1].copy()).cuda()
+    assert a.extract_charts(du, dp) == len(O.extract_charts(uvs[:-3], prim[:-3])["prim"])
+    big = prim.copy()
+    big[0] = float(1 << 24)
+    with pytest.raises(RuntimeError, match="SDF_ERR_INVALID"):
+        a.extract_charts(torch.from_numpy(uvs).cuda(), torch.from_numpy(big).cuda())
+    a.close()
+    assert L.SDF_ERR_INVALID == 1
