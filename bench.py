@@ -913,7 +913,7 @@ def main():
                                          "value": r["voxels"] / (r["solo_ms"] * 1e-3) / 1e9},
                      "setup_ms": r["setup_ms"], "autotune_and_capture_ms": r["tune_ms"],
                      "tuned_ctas_per_sm": st["tuned_ctas"], "clocks": r["clocks"],
-                     "gpu_launches": 19 * args.steps})
+                     "gpu_launches": 27 * args.steps})
         if "e2e" in r:
             line["e2e"] = r["e2e"]
         line["roofline"] = None

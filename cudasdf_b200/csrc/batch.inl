@@ -40,13 +40,27 @@ struct BatchGroup {
     size_t dc_cap = 0;
     DcSolveParams sp{};
     DcQuadParams qp{};
+    // dual contouring, the lists of the cross-block kernels (sized by the last run's counts; blocks and
+    // quads past them are handled inside k_dc_solve / k_dc_quads): Hermite samples and representatives,
+    // quads, projection records
+    unsigned* hsamp = nullptr;
+    float4* hreps = nullptr;
+    float4* hnorm = nullptr;
+    int4* hbase = nullptr;
+    uint2* qrec = nullptr;
+    float4* qnorm = nullptr;
+    float4* proj = nullptr;
+    size_t hsamp_cap = 0, hrep_cap = 0, q_cap = 0, proj_cap = 0;
+    unsigned last_herm[2] = {0u, 0u};
+    unsigned last_total = 0, last_dc = 0;
     // pinned read-back
     Ctrl* h_ctrl = nullptr;
     unsigned* h_first = nullptr;
 
     void release() {
         void* ptrs[] = {desc, prims, nodes, flags, list, fields, block_totals, block_offsets, b2a, miss, cell_words, first,
-                        ctrl_region, packet_counts, packet_offsets, masks, dc_voff, dc_verts};
+                        ctrl_region, packet_counts, packet_offsets, masks, dc_voff, dc_verts, hsamp, hreps, hnorm,
+                        hbase, qrec, qnorm, proj};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         if (h_ctrl) cudaFreeHost(h_ctrl);
@@ -71,7 +85,7 @@ static int capped_grid(K kernel, int threads, long long items, size_t smem, int 
 
 // launch shapes of one extraction, fixed before any capture
 struct BatchGrids {
-    int own, miss, gather, emit, mark, solve, quads, count_quads, emit_cells;
+    int own, miss, gather, emit, mark, solve, quads, count_quads, emit_cells, herm_reps, flat;
 };
 
 static BatchGrids batch_grids(long long blocks, const int ctas[4]) {
@@ -85,6 +99,9 @@ static BatchGrids batch_grids(long long blocks, const int ctas[4]) {
     G.quads = capped_grid(k_dc_quads, BLK_THREADS, blocks, sizeof(QuadSmem), ctas[3]);
     G.count_quads = (int)std::min<long long>(std::max(1LL, blocks), (long long)num_sms() * 4);
     G.emit_cells = capped_grid(k_mc_emit_cells, EMIT_WARPS * 32, (blocks + EMIT_WARPS - 1) / EMIT_WARPS, 0, 0);
+    G.herm_reps = capped_grid(k_dc_hermite_reps, SOLVE_THREADS, blocks, sizeof(HermSmem), 0);
+    // the flat DC kernels (Hermite normals, projection, quad normals) claim 32-item tasks: one full wave
+    G.flat = capped_grid(k_dc_quad_normals, BLK_THREADS, 1LL << 30, 0, 0);
     return G;
 }
 
@@ -157,9 +174,17 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
         D.counts = B.packet_counts;
         D.offsets = B.packet_offsets;
         D.qef_debug = nullptr;
-        D.proj = nullptr;  // the projection steps stay in k_dc_solve
-        D.proj_nsum = nullptr;
-        D.proj_cap = 0;
+        const bool project = B.sp.solver == SDF_DC_SOLVER_MASSPOINT && B.sp.projection_iters > 0 && B.proj_cap > 0;
+        D.proj = project ? B.proj : nullptr;
+        D.proj_nsum = nullptr;  // no cell normals
+        D.proj_cap = project ? (unsigned)std::min<size_t>(B.proj_cap, 0xFFFFFFFFu) : 0u;
+        const bool herm = B.hsamp_cap > 0 && B.hrep_cap > 0 && B.hbase;
+        D.hbase = herm ? B.hbase : nullptr;
+        D.hsample_rep = herm ? B.hsamp : nullptr;
+        D.hnormals = herm ? B.hnorm : nullptr;
+        const bool qlist = B.q_cap > 0;
+        D.qnormals = qlist ? B.qnorm : nullptr;
+        D.qcap = qlist ? (unsigned)std::min<size_t>(B.q_cap, 0xFFFFFFFFu) : 0u;
         record(cudaMemsetAsync(B.b2a, 0xFF, (size_t)nb * sizeof(int), st));
         k_dc_block_map<<<(nb + 255) / 256, 256, 0, st>>>(B.list, &ctrl->active_count, (int)nb, (int)nb, B.b2a);
         // block rows by the shared-halo block field, then the cells classified from the rows
@@ -174,12 +199,29 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
             &ctrl->dc_vertices, diag);
         DcSolveParams sp = B.sp;
         sp.max_cell_vertices = (unsigned)B.dc_cap;
+        if (herm) {
+            k_dc_hermite_reps<<<G.herm_reps, SOLVE_THREADS, sizeof(HermSmem), st>>>(
+                g0, av, B.fields, D, sp, ctrl->herm, B.hsamp, B.hreps, (unsigned)std::min<size_t>(B.hsamp_cap, 0xFFFFFFFFu),
+                (unsigned)std::min<size_t>(B.hrep_cap, 0xFFFFFFFFu), &ctrl->tickets[7]);
+            k_dc_hermite_normals<<<G.flat, BLK_THREADS, 0, st>>>(g0, sc0, time, av, B.hreps, ctrl->herm,
+                                                                 (unsigned)std::min<size_t>(B.hrep_cap, 0xFFFFFFFFu),
+                                                                 B.hnorm, &ctrl->tickets[8], diag);
+        }
         k_dc_solve<<<G.solve, SOLVE_THREADS, sizeof(SolveSmem), st>>>(g0, sc0, time, av, B.fields, D, sp,
                                                                     &ctrl->tickets[1], diag);
+        if (project)
+            k_dc_project<<<G.flat, BLK_THREADS, 0, st>>>(g0, sc0, time, av, D, sp, &ctrl->dc_vertices,
+                                                         &ctrl->tickets[6], diag);
         k_dc_count_quads<<<G.count_quads, 512, 0, st>>>(g0, av, D, B.packet_counts, B.block_totals);
         k_exclusive_scan<<<std::max(1u, scan_tiles(nb)), SCAN_THREADS, 0, st>>>(
             B.block_totals, B.block_offsets, nb, &ctrl->active_count, 1, scan_state(B.scan(B.scanB_off)),
             &ctrl->total_vertices, diag);
+        if (qlist) {
+            k_dc_quad_list<<<G.count_quads, BLK_THREADS, 0, st>>>(g0, av, D, B.packet_counts, B.block_offsets, B.qrec,
+                                                                 D.qcap);
+            k_dc_quad_normals<<<G.flat, BLK_THREADS, 0, st>>>(g0, sc0, time, av, D, B.qrec, &ctrl->total_vertices,
+                                                              D.qcap, mo.maxV, B.qnorm, &ctrl->tickets[9], diag);
+        }
         k_dc_quads<<<G.quads, BLK_THREADS, sizeof(QuadSmem), st>>>(g0, sc0, time, av, D, nullptr, B.packet_counts,
                                                                    B.block_offsets, mo, m, B.qp, &ctrl->tickets[2],
                                                                    diag);
@@ -429,6 +471,69 @@ sdf_status sdf_batch_set_scenes(sdf_batch* b, const sdf_batch_scene* scenes, int
     return SDF_OK;
 }
 
+// Grows the dual-contouring group's lists to the last run's counts plus a quarter (fractions of the cells
+// before any run); true when a buffer moved. Called outside any capture.
+static bool batch_size_lists(sdfb::BatchGroup& B) {
+    using namespace sdfb;
+    if (B.technique != SDF_TECH_DUAL_CONTOURING || B.n == 0) return false;
+    bool moved = false;
+    auto grow = [&](auto*& p, size_t& cap, size_t want) {
+        if (cap >= want) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        moved = true;
+        if (dev_alloc(p, want) == SDF_OK) cap = want;
+        cudaGetLastError();  // without a list the kernels fall back to their in-block paths
+    };
+    auto want = [&](unsigned last, size_t div) {
+        return std::min<size_t>(B.dc_cap, std::max<size_t>(B.dc_cap / div, (size_t)last + last / 4));
+    };
+    size_t hb = B.hbase ? (size_t)B.total_blocks : 0;
+    grow(B.hbase, hb, (size_t)B.total_blocks);
+    if (!B.hbase) B.hsamp_cap = B.hrep_cap = 0;
+    grow(B.hsamp, B.hsamp_cap, want(B.last_herm[0], 4));
+    {
+        const size_t w = want(B.last_herm[1], 8);
+        size_t c1 = B.hrep_cap, c2 = B.hrep_cap;
+        if (c1 < w) {
+            grow(B.hreps, c1, w);
+            grow(B.hnorm, c2, w);
+            B.hrep_cap = std::min(c1, c2);
+        }
+    }
+    {
+        const size_t w = want(B.last_total / 6, 16);
+        size_t c1 = B.q_cap, c2 = B.q_cap;
+        if (c1 < w) {
+            grow(B.qrec, c1, w);
+            grow(B.qnorm, c2, w);
+            B.q_cap = std::min(c1, c2);
+        }
+    }
+    if (B.sp.solver == SDF_DC_SOLVER_MASSPOINT && B.sp.projection_iters > 0) {
+        const size_t w = want(B.last_dc, 8);
+        if (B.proj_cap < w) {
+            if (B.proj) cudaFree(B.proj);
+            B.proj = nullptr;
+            B.proj_cap = 0;
+            moved = true;
+            if (dev_alloc(B.proj, 2 * w) == SDF_OK) B.proj_cap = w;
+            cudaGetLastError();
+        }
+    }
+    return moved;
+}
+
+// the counts the lists are sized by, from the last read-back of the group's control block
+static void batch_note_counts(sdfb::BatchGroup& B) {
+    if (B.n == 0 || !B.h_ctrl) return;
+    B.last_herm[0] = B.h_ctrl->herm[0];
+    B.last_herm[1] = B.h_ctrl->herm[1];
+    B.last_total = B.h_ctrl->total_vertices;
+    B.last_dc = B.h_ctrl->dc_vertices;
+}
+
 static sdf_status batch_finish(sdfb::BatchImpl& I, const sdf_outputs* out[2], int64_t* first_vertex,
                                int64_t* vertex_count, sdf_batch_stats* stats, float ms, int graph) {
     using namespace sdfb;
@@ -444,7 +549,9 @@ static sdf_status batch_finish(sdfb::BatchImpl& I, const sdf_outputs* out[2], in
         BatchGroup& B = I.g[k];
         if (B.n == 0) continue;
         const Ctrl& h = *B.h_ctrl;
+        batch_note_counts(B);
         if (h.diag.timeout) status = SDF_ERR_TIMEOUT;
+        if (h.diag.inconsistent && status == SDF_OK) status = SDF_ERR_CUDA;
         if (h.diag.stack_overflow && status == SDF_OK) status = SDF_ERR_STACK;
         const unsigned cap = out[k] ? out[k]->max_vertices : 0u;
         if (status == SDF_OK && (h.total_vertices > cap || (k == 1 && h.dc_vertices > B.dc_cap)))
@@ -480,6 +587,7 @@ sdf_status sdf_batch_extract(sdf_batch* b, float time, const sdf_outputs* mc_out
     if (replay) {
         record(cudaGraphLaunch(I.exec, st));
     } else {
+        if (batch_size_lists(I.g[1])) I.drop_graph();  // the graph holds the old lists
         const BatchGrids G = batch_grids(std::max(I.g[0].total_blocks, I.g[1].total_blocks), I.ctas);
         enqueue_both(I, G, time, mc_out, dc_out, st);
     }
@@ -506,6 +614,7 @@ sdf_status sdf_batch_capture(sdf_batch* b, float time, const sdf_outputs* mc_out
     cudaStream_t st = I.cap_stream;
     I.drop_graph();
     const long long blocks = std::max(I.g[0].total_blocks, I.g[1].total_blocks);
+    batch_size_lists(I.g[1]);
     if (tune) {
         // coordinate descent over the CTAs per SM of the block field, the emission, the DC solve and
         // the DC quads: each candidate is timed on one direct extraction after a warm-up run
@@ -531,6 +640,7 @@ sdf_status sdf_batch_capture(sdf_batch* b, float time, const sdf_outputs* mc_out
                         return SDF_ERR_CUDA;
                     }
                     cudaEventElapsedTime(&ms, e0, e1);
+                    batch_note_counts(I.g[1]);
                 }
                 if (ms < best) {
                     best = ms;
@@ -543,6 +653,12 @@ sdf_status sdf_batch_capture(sdf_batch* b, float time, const sdf_outputs* mc_out
         cudaEventDestroy(e1);
     }
     const BatchGrids G = batch_grids(blocks, I.ctas);  // attributes set before the capture
+    if (!tune) {  // one direct run gives the counts the lists are sized by
+        enqueue_both(I, G, time, mc_out, dc_out, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) return SDF_ERR_CUDA;
+        batch_note_counts(I.g[1]);
+    }
+    batch_size_lists(I.g[1]);
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return SDF_ERR_CUDA;
     enqueue_both(I, G, time, mc_out, dc_out, st);
     if (cudaStreamEndCapture(st, &I.graph) != cudaSuccess || !I.graph) {

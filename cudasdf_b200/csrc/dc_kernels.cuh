@@ -27,6 +27,16 @@ struct DcBuffers {
     float4* proj;
     float4* proj_nsum;
     unsigned proj_cap;
+    // optional, Hermite normals evaluated across blocks (k_dc_hermite_reps / k_dc_hermite_normals): per
+    // active block its first sample, first representative and their counts (x < 0: not listed, k_dc_solve
+    // evaluates its normals itself), per sample its representative, per representative the normal
+    int4* hbase;
+    const unsigned* hsample_rep;
+    const float4* hnormals;
+    // optional, the quads' winding normals evaluated across blocks (k_dc_quad_list / k_dc_quad_normals),
+    // per counted quad in emission order (quad q = its first vertex / 6), q < qcap
+    const float4* qnormals;
+    unsigned qcap;
 };
 
 struct DcSolveParams {
@@ -346,6 +356,189 @@ __device__ float3 solve_reference(const GridView& g, const CellInfo& c, const fl
     return xsol;
 }
 
+// the (edge, direction) key of Hermite sample (cell tid, edge e) in the block's 9^3 lattice: the cells
+// around an edge that name it with the same direction share the key, the edge point and the normal
+__device__ __forceinline__ int hermite_key(int tid, int e) {
+    const int c0 = edge_c0(e), c1 = edge_c1(e);
+    const int d0 = corner_dx(c0) + 2 * corner_dy(c0) + 4 * corner_dz(c0);
+    const int d1 = corner_dx(c1) + 2 * corner_dy(c1) + 4 * corner_dz(c1);
+    const int lo = d0 < d1 ? c0 : c1;  // the edge's lower corner
+    const int axis = (d0 ^ d1) == 1 ? 0 : ((d0 ^ d1) == 2 ? 1 : 2);
+    const int sx = (tid & 7) + corner_dx(lo), sy = ((tid >> 3) & 7) + corner_dy(lo), sz = (tid >> 6) + corner_dz(lo);
+    return ((sz * 9 + sy) * 9 + sx) * 6 + axis * 2 + (d0 < d1 ? 0 : 1);
+}
+
+// the edge mask of a solved cell (sign-changing edges), 0 for a cell k_dc_solve does not solve
+__device__ __forceinline__ unsigned solved_cell_edges(const GridView& g, const DcBuffers& B, const DcSolveParams& P,
+                                                      const float* field, int a, int bx, int by, int bz, int tid,
+                                                      CellInfo& c, float (&cv)[8]) {
+    const size_t pk = (size_t)a * 512 + tid;
+    if (B.counts[pk] == 0) return 0u;
+    c = cell_info(g, bx, by, bz, tid);
+    if (c.oob) return 0u;
+    if (B.vert_offsets[pk] >= P.max_cell_vertices) return 0u;
+    const int mask = cell_case(field, c.lx, c.ly, c.lz, cv);
+    unsigned em = 0;
+    for (int e = 0; e < 12; ++e)
+        if (((mask >> edge_c0(e)) & 1) != ((mask >> edge_c1(e)) & 1)) em |= 1u << e;
+    return em;
+}
+
+// Lists every active block's Hermite samples in k_dc_solve's order (cells in order, edges in order)
+// with the representative of each (edge, direction): its first sample in that order. Each block
+// reserves a range of samples and representatives in the global lists; writes each sample's
+// representative index and each representative's edge point (w: the active block). A block whose range
+// does not fit keeps hbase.x = -1 and k_dc_solve evaluates its normals itself.
+struct HermSmem {
+    float field[FIELD_STRIDE];
+    unsigned key_tab[DC_EDGE_KEYS];  // first sample of each key, then its representative number
+    unsigned warp_sums[SOLVE_THREADS / 32];
+    int base_s, base_r, item;
+};
+
+__global__ void __launch_bounds__(SOLVE_THREADS) k_dc_hermite_reps(GridView g0, ActiveView av,
+                                                                  const float* __restrict__ fields, DcBuffers B,
+                                                                  DcSolveParams P, unsigned* __restrict__ counters,
+                                                                  unsigned* __restrict__ sample_rep, float4* __restrict__ reps,
+                                                                  unsigned sample_cap, unsigned rep_cap, unsigned* ticket) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    HermSmem& S = *reinterpret_cast<HermSmem*>(dyn_smem);
+    const int n = active_count(av);
+    for (;;) {
+        const int a = claim(ticket, n, &S.item);
+        if (a < 0) break;
+        GridView g = g0;
+        SceneView unused;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[a], g, unused, lin, bbase);
+        int bx, by, bz;
+        block_coord(g, lin, bx, by, bz);
+        const float4* src = reinterpret_cast<const float4*>(fields + (size_t)a * FIELD_STRIDE);
+        for (int i = threadIdx.x; i < FIELD_STRIDE / 4; i += blockDim.x) reinterpret_cast<float4*>(S.field)[i] = src[i];
+        for (int k = threadIdx.x; k < DC_EDGE_KEYS; k += blockDim.x) S.key_tab[k] = 0xFFFFFFFFu;
+        __syncthreads();
+        // this thread's two cells: their edge masks and sample counts
+        unsigned em[2];
+        CellInfo ci[2];
+        float cvs[2][8];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) em[h] = solved_cell_edges(g, B, P, S.field, a, bx, by, bz, 2 * threadIdx.x + h, ci[h], cvs[h]);
+        const unsigned mine = __popc(em[0]) + __popc(em[1]);
+        unsigned total = 0;
+        const unsigned k0 = block_exclusive<SOLVE_THREADS>(mine, S.warp_sums, &total);
+        // the first sample of every key
+        unsigned k = k0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+            for (int e = 0; e < 12; ++e)
+                if ((em[h] >> e) & 1u) atomicMin(&S.key_tab[hermite_key(2 * threadIdx.x + h, e)], k++);
+        __syncthreads();
+        unsigned nr = 0;
+        k = k0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+            for (int e = 0; e < 12; ++e)
+                if ((em[h] >> e) & 1u) nr += S.key_tab[hermite_key(2 * threadIdx.x + h, e)] == k++ ? 1u : 0u;
+        unsigned rtotal = 0;
+        const unsigned r0 = block_exclusive<SOLVE_THREADS>(nr, S.warp_sums, &rtotal);
+        if (threadIdx.x == 0) {
+            const unsigned bs = total ? atomicAdd(&counters[0], total) : 0u;
+            const unsigned br = rtotal ? atomicAdd(&counters[1], rtotal) : 0u;
+            const bool fits = (unsigned long long)bs + total <= sample_cap && (unsigned long long)br + rtotal <= rep_cap;
+            S.base_s = fits ? (int)bs : -1;
+            S.base_r = fits ? (int)br : -1;
+            B.hbase[a] = make_int4(S.base_s, S.base_r, (int)total, (int)rtotal);
+        }
+        __syncthreads();  // key_tab holds first samples until every thread has tested its own
+        const int bs = S.base_s, br = S.base_r;
+        if (bs >= 0) {
+            // representatives: their number replaces the key's first sample, and their edge point is listed
+            unsigned r = r0;
+            k = k0;
+            int rep_keys[24];
+            int nrk = 0;
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                for (int e = 0; e < 12; ++e)
+                    if ((em[h] >> e) & 1u) {
+                        const int key = hermite_key(2 * threadIdx.x + h, e);
+                        if (S.key_tab[key] == k) {
+                            const float3 pt = edge_point(g, ci[h].x, ci[h].y, ci[h].z, cvs[h], e);
+                            reps[(size_t)br + r] = make_float4(pt.x, pt.y, pt.z, __int_as_float(a));
+                            rep_keys[nrk++] = key;
+                            ++r;
+                        }
+                        ++k;
+                    }
+            __syncthreads();  // every first-sample test is done before the table is overwritten
+            r = r0;
+            for (int q = 0; q < nrk; ++q) S.key_tab[rep_keys[q]] = r++;
+            __syncthreads();
+            k = k0;
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                for (int e = 0; e < 12; ++e)
+                    if ((em[h] >> e) & 1u)
+                        sample_rep[(size_t)bs + k++] = (unsigned)br + S.key_tab[hermite_key(2 * threadIdx.x + h, e)];
+        }
+    }
+}
+
+// computeNormal (:814-844) at every listed representative's edge point, 32 per warp task with the four
+// stencil points of a lane walked together (map_multi), one scene's BVH at a time
+__global__ void __launch_bounds__(BLK_THREADS) k_dc_hermite_normals(GridView g0, SceneView sc0, float time,
+                                                                   ActiveView av, const float4* __restrict__ reps,
+                                                                   const unsigned* __restrict__ counters, unsigned rep_cap,
+                                                                   float4* __restrict__ normals, unsigned* ticket,
+                                                                   Diag* diag) {
+    const unsigned n = min(counters[1], rep_cap);
+    const int nact = active_count(av);
+    const int tasks = nact > 0 ? (int)((n + 31u) / 32u) : 0;
+    const int lane = threadIdx.x & 31;
+    const unsigned FULL = 0xffffffffu;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = (int)atomicAdd(ticket, 1u);
+        t = __shfl_sync(FULL, t, 0);
+        if (t >= tasks) break;
+        const unsigned r = (unsigned)t * 32u + (unsigned)lane;
+        const bool in = r < n;
+        const float4 rec = reps[in ? r : (unsigned)t * 32u];
+        const int ra = __float_as_int(rec.w);
+        const bool live = in && ra >= 0 && ra < nact;
+        GridView g = g0;
+        SceneView sc = sc0;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[live ? ra : 0], g, sc, lin, bbase);
+        const float3 c = f3(rec.x, rec.y, rec.z);
+        const float h = MUL(g.cell, 0.001f);
+        const float3 pts[4] = {c, f3(ADD(c.x, h), c.y, c.z), f3(c.x, ADD(c.y, h), c.z), f3(c.x, c.y, ADD(c.z, h))};
+        float d[4] = {0.f, 0.f, 0.f, 0.f};
+        unsigned pending = __ballot_sync(FULL, live);
+        while (pending) {
+            const unsigned lead = __shfl_sync(FULL, bbase, __ffs(pending) - 1);
+            const bool mine = live && bbase == lead && ((pending >> lane) & 1u);
+            SceneView scw = sc;
+            if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead)].sc;
+            float dm[4];
+            map_multi<4>(scw, pts, mine, time, dm, diag);
+            if (mine) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) d[q] = dm[q];
+            }
+            pending &= ~__ballot_sync(FULL, mine);
+        }
+        if (live) {
+            const float3 gr = f3(SUB(d[1], d[0]), SUB(d[2], d[0]), SUB(d[3], d[0]));
+            const float len = SQRT(dot3(gr, gr));
+            const float3 nn = len > 1e-6f ? f3(DIV(gr.x, len), DIV(gr.y, len), DIV(gr.z, len)) : f3(0.f, 1.f, 0.f);
+            normals[r] = make_float4(nn.x, nn.y, nn.z, 0.f);
+        }
+    }
+}
+
 // value and normalised gradient (computeNormal's differences) at the 32 points of a warp
 __device__ __forceinline__ float3 value_gradient_warp(const SceneView& sc, float3 p, bool valid, float time,
                                                       float cell, float& d, Diag* diag) {
@@ -384,6 +577,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
         __syncthreads();
         int bx, by, bz;
         block_coord(g, lin, bx, by, bz);
+        // the block's samples listed by k_dc_hermite_reps (their normals already evaluated), if any
+        const int4 hbase = B.hbase ? B.hbase[a] : make_int4(-1, -1, 0, 0);
+        const int hb = hbase.x;
+        unsigned hk0 = 0;  // samples of the earlier passes
         // The cells that get a vertex are processed in cell order, in passes bounded by the Hermite
         // staging capacity (a cell has at most 12 samples, so every pass makes progress).
         int cursor = 0;
@@ -442,7 +639,23 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
             const unsigned nh = ncells ? (unsigned)S.cell_h0[ncells - 1] + S.cell_m[ncells - 1] : 0u;
             // Hermite normals: computeNormal at each edge point (:1383-1411). The cells around an
             // edge that name it with the same direction compute the same float edge point from the
-            // same two samples, hence the same normal: it is evaluated once per (edge, direction).
+            // same two samples, hence the same normal: it is evaluated once per (edge, direction),
+            // by k_dc_hermite_normals for a listed block, here otherwise.
+            if (hb >= 0) {
+                // the listing enumerates the same samples; an index past its count is not followed
+                for (int i = threadIdx.x; i < (int)nh; i += blockDim.x) {
+                    float3 nn = f3(0.f, 1.f, 0.f);
+                    if (hk0 + (unsigned)i < (unsigned)hbase.z) {
+                        const float4 v = B.hnormals[B.hsample_rep[(size_t)hb + hk0 + i]];
+                        nn = f3(v.x, v.y, v.z);
+                    } else if (diag) {
+                        atomicExch(&diag->inconsistent, 1);
+                    }
+                    S.h_n[i] = nn;
+                }
+                hk0 += nh;
+                __syncthreads();
+            } else {
             for (int k = threadIdx.x; k < DC_EDGE_KEYS; k += blockDim.x) S.edge_rep[k] = 0xFFFF;
             if (threadIdx.x == 0) S.nrep = 0;
             __syncthreads();
@@ -485,6 +698,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
             for (int i = threadIdx.x; i < (int)nh; i += blockDim.x)
                 if (S.h_rep[i] != i) S.h_n[i] = S.h_n[S.h_rep[i]];
             __syncthreads();
+            }
             // per-cell solve
             for (int i = threadIdx.x; i < (int)ncells; i += blockDim.x) {
                 const CellInfo c = cell_info(g, bx, by, bz, S.cell_tid[i]);
@@ -912,6 +1126,123 @@ __device__ __forceinline__ bool quad_indices_ok(const DcBuffers& B, const int q[
            B.vert_offsets[q[3]] < maxV;
 }
 
+// Every counted quad of every active block, in emission order: quad q = (block offset + in-block count
+// prefix) / 6 gets (active block, cell << 2 | axis). The enumeration is k_dc_quads' own.
+__global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_list(GridView g0, ActiveView av, DcBuffers B,
+                                                             const unsigned* __restrict__ counts,
+                                                             const unsigned* __restrict__ block_offsets,
+                                                             uint2* __restrict__ recs, unsigned cap) {
+    __shared__ unsigned s_warp[BLK_THREADS / 32];
+    const int n = active_count(av);
+    for (int a = blockIdx.x; a < n; a += gridDim.x) {
+        GridView g = g0;
+        SceneView unused;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[a], g, unused, lin, bbase);
+        const int* b2a = B.block_to_active + bbase;
+        int bx, by, bz;
+        block_coord(g, lin, bx, by, bz);
+        unsigned cnt[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) cnt[h] = counts[(size_t)a * 512 + 2 * threadIdx.x + h];
+        unsigned tot;
+        const unsigned local = block_exclusive<BLK_THREADS>(cnt[0] + cnt[1], s_warp, &tot);
+        const unsigned q0 = block_offsets[a] / 6u;
+        unsigned q = q0 + local / 6u;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int tid = 2 * threadIdx.x + h;
+            if (cnt[h] == 0) continue;
+            const CellInfo c = cell_info(g, bx, by, bz, tid);
+            if (c.oob) continue;
+            const unsigned char m = B.masks[(size_t)a * 512 + tid];
+            const unsigned s0 = m & 1u;
+            for (int axis = 0; axis < 3; ++axis) {
+                if (((m >> edge_corner(axis)) & 1u) == s0) continue;
+                int qc[4];
+                if (!quad_cells(g, b2a, axis, c.x, c.y, c.z, qc)) continue;
+                if (!surface_mask(B.masks[qc[0]]) || !surface_mask(B.masks[qc[1]]) || !surface_mask(B.masks[qc[2]]) ||
+                    !surface_mask(B.masks[qc[3]]))
+                    continue;
+                if (q < cap) recs[q] = make_uint2((unsigned)a, (unsigned)((tid << 2) | axis));
+                ++q;
+            }
+        }
+        __syncthreads();  // s_warp is free for the next block
+    }
+}
+
+// computeNormal (:814-844) at the centre of every listed quad (its four decoded cell vertices), 32 quads
+// per warp task with the four stencil points of a lane walked together, one scene's BVH at a time
+__global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_normals(GridView g0, SceneView sc0, float time,
+                                                                ActiveView av, DcBuffers B,
+                                                                const uint2* __restrict__ recs,
+                                                                const unsigned* __restrict__ total_vertices,
+                                                                unsigned cap, unsigned maxV,
+                                                                float4* __restrict__ normals, unsigned* ticket,
+                                                                Diag* diag) {
+    const unsigned n = min(*total_vertices / 6u, cap);
+    const int nact = active_count(av);
+    const int tasks = nact > 0 ? (int)((n + 31u) / 32u) : 0;
+    const int lane = threadIdx.x & 31;
+    const unsigned FULL = 0xffffffffu;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = (int)atomicAdd(ticket, 1u);
+        t = __shfl_sync(FULL, t, 0);
+        if (t >= tasks) break;
+        const unsigned qi = (unsigned)t * 32u + (unsigned)lane;
+        const bool in = qi < n;
+        const uint2 rec = recs[in ? qi : (unsigned)t * 32u];
+        const int ra = (int)rec.x, tid = (int)(rec.y >> 2), axis = (int)(rec.y & 3u);
+        bool live = in && ra < nact && tid < 512 && axis < 3;
+        GridView g = g0;
+        SceneView sc = sc0;
+        int lin;
+        unsigned bbase;
+        resolve(av, av.list[live ? ra : 0], g, sc, lin, bbase);
+        const int* b2a = B.block_to_active + bbase;
+        int bx, by, bz;
+        block_coord(g, lin, bx, by, bz);
+        float3 qc = f3(0.f, 0.f, 0.f);
+        if (live) {
+            const CellInfo c = cell_info(g, bx, by, bz, tid);
+            int q[4];
+            if (quad_cells(g, b2a, axis, c.x, c.y, c.z, q)) {
+                QuadVerts Q;
+                Q.qc = f3(0.f, 0.f, 0.f);
+                quad_vertices(g, av.list, bbase, B, q, maxV, Q);  // a skipped quad's normal stays unused
+                qc = Q.qc;
+            }
+        }
+        const float h = MUL(g.cell, 0.001f);
+        const float3 pts[4] = {qc, f3(ADD(qc.x, h), qc.y, qc.z), f3(qc.x, ADD(qc.y, h), qc.z),
+                               f3(qc.x, qc.y, ADD(qc.z, h))};
+        float d[4] = {0.f, 0.f, 0.f, 0.f};
+        unsigned pending = __ballot_sync(FULL, live);
+        while (pending) {
+            const unsigned lead = __shfl_sync(FULL, bbase, __ffs(pending) - 1);
+            const bool mine = live && bbase == lead && ((pending >> lane) & 1u);
+            SceneView scw = sc;
+            if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead)].sc;
+            float dm[4];
+            map_multi<4>(scw, pts, mine, time, dm, diag);
+            if (mine) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) d[k] = dm[k];
+            }
+            pending &= ~__ballot_sync(FULL, mine);
+        }
+        if (live) {
+            const float3 gr = f3(SUB(d[1], d[0]), SUB(d[2], d[0]), SUB(d[3], d[0]));
+            const float len = SQRT(dot3(gr, gr));
+            const float3 nn = len > 1e-6f ? f3(DIV(gr.x, len), DIV(gr.y, len), DIV(gr.z, len)) : f3(0.f, 1.f, 0.f);
+            normals[qi] = make_float4(nn.x, nn.y, nn.z, 0.f);
+        }
+    }
+}
+
 // three CTAs per SM (80 registers): measured 4.2 ms for the 512^3 quads against 7.8 ms at 128 registers
 __global__ void __launch_bounds__(BLK_THREADS, 3) k_dc_quads(GridView g0, SceneView sc0, float time, ActiveView av,
                                                           DcBuffers B, const unsigned* __restrict__ offsets,
@@ -984,8 +1315,17 @@ __global__ void __launch_bounds__(BLK_THREADS, 3) k_dc_quads(GridView g0, SceneV
             }
             const unsigned nq = min(nslots_total - pass0, (unsigned)DC_QUAD_CAP);
             __syncthreads();
-            // the winding normal of every staged quad: computeNormal at the quad centre, the four points
-            // of each stencil spread over all warps
+            // the winding normal of every staged quad: computeNormal at the quad centre, listed by
+            // k_dc_quad_normals (quad = block offset / 6 + slot) or the four points of each stencil
+            // spread over all warps here
+            const unsigned qfirst = offsets ? 0u : block_offsets[a] / 6u + pass0;
+            if (B.qnormals && !offsets && qfirst + nq <= B.qcap) {
+                for (int i = threadIdx.x; i < (int)nq; i += blockDim.x) {
+                    const float4 v = B.qnormals[qfirst + i];
+                    S.q_fn[i][1] = f3(v.x, v.y, v.z);
+                }
+                __syncthreads();
+            } else
             stencil_all_warps(
                 sc, (int)nq, g.cell, time, S.st_d,
                 [&](int i) {

@@ -18,6 +18,7 @@ struct Ctrl {
     unsigned dc_vertices;
     unsigned halo_misses;  // listed halo samples of the block field (k_field_plan)
     unsigned welded_vertices;  // indexed marching-cubes output: vertices (one per owned crossed edge)
+    unsigned herm[2];          // dual contouring: Hermite samples and representatives listed (k_dc_hermite_reps)
     Diag diag;
 };
 
@@ -107,6 +108,19 @@ struct EngineImpl {
     float4* dc_proj_nsum = nullptr;        //   and the Hermite normal sums when cell normals are kept
     size_t dc_proj_cap = 0, dc_proj_nsum_cap = 0;
     unsigned last_dc_vertices = 0;         // DC vertices of the last collected extraction
+    // Hermite normals across blocks: per sample its representative, per representative the edge point
+    // and the normal, per active block the first sample and representative
+    unsigned* dc_hsamp = nullptr;
+    float4* dc_hreps = nullptr;
+    float4* dc_hnorm = nullptr;
+    int4* dc_hbase = nullptr;
+    size_t dc_hsamp_cap = 0, dc_hrep_cap = 0, dc_hbase_cap = 0;
+    unsigned last_herm[2] = {0u, 0u};
+    // quads' winding normals across blocks: per counted quad (active block, cell << 2 | axis) and normal
+    uint2* dc_qrec = nullptr;
+    float4* dc_qnorm = nullptr;
+    size_t dc_qcap = 0;
+    unsigned last_total_vertices = 0;
     unsigned char* ctrl_region = nullptr;  // Ctrl, then the three scan regions
     size_t ctrl_bytes = 0;
     size_t scanA_off = 0, scanB_off = 0, scanD_off = 0, scanC_off = 0;
@@ -166,7 +180,7 @@ struct EngineImpl {
         void* ptrs[] = {d_prims, d_nodes, flags, list, fields, block_totals, block_offsets, packet_counts,
                         packet_offsets, b2a, masks, dc_voff, dc_verts, dc_norms, ctrl_region, eval_diag, miss,
                         cell_words, bvh_work, weld_bits, weld_prefix, weld_totals, weld_base, dc_qef,
-                        dc_proj, dc_proj_nsum};
+                        dc_proj, dc_proj_nsum, dc_hsamp, dc_hreps, dc_hnorm, dc_hbase, dc_qrec, dc_qnorm};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         d_prims = nullptr; d_nodes = nullptr; flags = nullptr; list = nullptr; fields = nullptr;
@@ -183,6 +197,13 @@ struct EngineImpl {
         dc_qef_cap = 0;
         dc_proj = dc_proj_nsum = nullptr;
         dc_proj_cap = dc_proj_nsum_cap = 0;
+        dc_hsamp = nullptr;
+        dc_hreps = dc_hnorm = nullptr;
+        dc_hbase = nullptr;
+        dc_hsamp_cap = dc_hrep_cap = dc_hbase_cap = 0;
+        dc_qrec = nullptr;
+        dc_qnorm = nullptr;
+        dc_qcap = 0;
         prims_cap = nodes_cap = dc_cap = packet_cap = miss_cap = cell_words_cap = bvh_work_cap = 0;
         if (h_bvh_ctl) cudaFreeHost(h_bvh_ctl);
         h_bvh_ctl = nullptr;
@@ -674,6 +695,38 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
             if (dev_alloc(E.dc_qef, E.dc_cap) != SDF_OK) return SDF_ERR_NOMEM;
             E.dc_qef_cap = E.dc_cap;
         }
+        // the Hermite lists: sized by the last extraction's counts (a quarter and an eighth of the cells at
+        // first); blocks whose samples do not fit evaluate their normals inside k_dc_solve
+        {
+            const size_t ws = std::min<size_t>(E.dc_cap, std::max<size_t>(E.dc_cap / 4, (size_t)E.last_herm[0] +
+                                                                                        E.last_herm[0] / 4));
+            const size_t wr = std::min<size_t>(E.dc_cap, std::max<size_t>(E.dc_cap / 8, (size_t)E.last_herm[1] +
+                                                                                        E.last_herm[1] / 4));
+            auto grow = [](auto*& p, size_t& cap, size_t want) {
+                if (cap >= want) return;
+                if (p) cudaFree(p);
+                p = nullptr;
+                cap = 0;
+                if (dev_alloc(p, want) == SDF_OK) cap = want;
+                cudaGetLastError();
+            };
+            grow(E.dc_hsamp, E.dc_hsamp_cap, ws);
+            size_t rc = E.dc_hrep_cap, rc2 = E.dc_hrep_cap;
+            if (rc < wr) {
+                grow(E.dc_hreps, rc, wr);
+                grow(E.dc_hnorm, rc2, wr);
+                E.dc_hrep_cap = std::min(rc, rc2);
+            }
+            grow(E.dc_hbase, E.dc_hbase_cap, (size_t)cap);
+            const size_t wq = std::min<size_t>(E.dc_cap, std::max<size_t>(E.dc_cap / 16, (size_t)E.last_total_vertices / 6 +
+                                                                                         E.last_total_vertices / 24));
+            if (E.dc_qcap < wq) {
+                size_t c1 = E.dc_qcap, c2 = E.dc_qcap;
+                grow(E.dc_qrec, c1, wq);
+                grow(E.dc_qnorm, c2, wq);
+                E.dc_qcap = std::min(c1, c2);
+            }
+        }
         // projection records for k_dc_project: sized by the last extraction's vertices (an eighth of the
         // cells at first); vertices beyond them are projected inside k_dc_solve, so no size is wrong
         if (C.dc_solver == SDF_DC_SOLVER_MASSPOINT && C.projection_iters > 0) {
@@ -816,6 +869,14 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
         B.proj = project ? E.dc_proj : nullptr;
         B.proj_nsum = project && B.cell_normals ? E.dc_proj_nsum : nullptr;
         B.proj_cap = project ? (unsigned)std::min<size_t>(E.dc_proj_cap, 0xFFFFFFFFu) : 0u;
+        const bool herm = E.dc_hsamp && E.dc_hreps && E.dc_hnorm && E.dc_hbase && E.dc_hbase_cap >= (size_t)cap &&
+                          E.dc_hsamp_cap > 0 && E.dc_hrep_cap > 0;
+        B.hbase = herm ? E.dc_hbase : nullptr;
+        B.hsample_rep = herm ? E.dc_hsamp : nullptr;
+        B.hnormals = herm ? E.dc_hnorm : nullptr;
+        const bool qlist = E.dc_qrec && E.dc_qnorm && E.dc_qcap > 0;
+        B.qnormals = qlist ? E.dc_qnorm : nullptr;
+        B.qcap = qlist ? (unsigned)std::min<size_t>(E.dc_qcap, 0xFFFFFFFFu) : 0u;
         record(cudaMemsetAsync(E.b2a, 0xFF, (size_t)nb * sizeof(int), st));
         k_dc_block_map<<<(cap + 255) / 256, 256, 0, st>>>(E.list, &ctrl->active_count, cap, nb, E.b2a);
         check_launch();
@@ -837,6 +898,19 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
         sp.solver = C.dc_solver;
         sp.projection_iters = C.dc_solver == SDF_DC_SOLVER_MASSPOINT ? C.projection_iters : 0;
         sp.cond_threshold = C.cond_threshold > 0.f ? C.cond_threshold : 1e4f;
+        if (herm) {
+            const size_t hsmem = sizeof(HermSmem);
+            k_dc_hermite_reps<<<persistent_grid(k_dc_hermite_reps, SOLVE_THREADS, cap, hsmem), SOLVE_THREADS, hsmem, st>>>(
+                gv, av, E.fields, B, sp, ctrl->herm, E.dc_hsamp, E.dc_hreps,
+                (unsigned)std::min<size_t>(E.dc_hsamp_cap, 0xFFFFFFFFu),
+                (unsigned)std::min<size_t>(E.dc_hrep_cap, 0xFFFFFFFFu), &ctrl->tickets[7]);
+            k_dc_hermite_normals<<<persistent_grid(k_dc_hermite_normals, BLK_THREADS,
+                                                   std::max(1, (int)(E.dc_hrep_cap / 256))),
+                                   BLK_THREADS, 0, st>>>(gv, sv, time, av, E.dc_hreps, ctrl->herm,
+                                                         (unsigned)std::min<size_t>(E.dc_hrep_cap, 0xFFFFFFFFu),
+                                                         E.dc_hnorm, &ctrl->tickets[8], diag);
+            check_launch();
+        }
         const size_t solve_smem = sizeof(SolveSmem);
         k_dc_solve<<<persistent_grid(k_dc_solve, SOLVE_THREADS, cap, solve_smem), SOLVE_THREADS, solve_smem, st>>>(
             gv, sv, time, av, E.fields, B, sp, &ctrl->tickets[1], diag);
@@ -853,6 +927,14 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
             E.block_totals, E.block_offsets, (unsigned)cap, &ctrl->active_count, 1, scan_state(scanB),
             &ctrl->total_vertices, diag);
         check_launch();
+        if (qlist) {
+            k_dc_quad_list<<<std::min(cap, num_sms() * 8), BLK_THREADS, 0, st>>>(gv, av, B, E.packet_counts,
+                                                                                   E.block_offsets, E.dc_qrec, B.qcap);
+            k_dc_quad_normals<<<persistent_grid(k_dc_quad_normals, BLK_THREADS, std::max(1, (int)(B.qcap / 256))),
+                                BLK_THREADS, 0, st>>>(gv, sv, time, av, B, E.dc_qrec, &ctrl->total_vertices, B.qcap,
+                                                      mo.maxV, E.dc_qnorm, &ctrl->tickets[9], diag);
+            check_launch();
+        }
         DcQuadParams qp;
         qp.adaptive_diagonal = (C.dc_solver == SDF_DC_SOLVER_MASSPOINT) ? C.adaptive_diagonal : 0;
         const size_t quad_smem = sizeof(QuadSmem);
@@ -928,7 +1010,12 @@ static sdf_status engine_collect(EngineImpl& E, int slot, sdf_stats* stats, bool
         stats->total_vertices = h.total_vertices;
         stats->written_vertices = std::min<int64_t>(h.total_vertices, P.max_vertices);
         stats->dc_cell_vertices = h.dc_vertices;
-        if (P.dc) E.last_dc_vertices = h.dc_vertices;
+        if (P.dc) {
+            E.last_dc_vertices = h.dc_vertices;
+            E.last_herm[0] = h.herm[0];
+            E.last_herm[1] = h.herm[1];
+            E.last_total_vertices = h.total_vertices;
+        }
         stats->bvh_cap_hits = (int64_t)h.diag.cap_hits;
         stats->scouted_blocks = P.culled ? (int64_t)h.diag.scouted : (int64_t)P.nb;
         stats->dc_fp64_cells = (int64_t)h.diag.fp64_cells;
@@ -944,6 +1031,7 @@ static sdf_status engine_collect(EngineImpl& E, int slot, sdf_stats* stats, bool
     }
     if (h.diag.timeout) return SDF_ERR_TIMEOUT;
     if (h.diag.stack_overflow) return SDF_ERR_STACK;
+    if (h.diag.inconsistent) return SDF_ERR_CUDA;
     if (h.total_vertices > P.max_vertices || (P.dc && h.dc_vertices > P.dc_cap) ||
         (P.welded && (P.dc ? h.dc_vertices : h.welded_vertices) > P.max_vertices))
         return SDF_ERR_CAPACITY;

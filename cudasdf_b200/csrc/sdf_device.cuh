@@ -395,6 +395,7 @@ struct Diag {
     unsigned long long warp_leaves; //   and leaf steps (some lane evaluates the primitive)
     int stack_overflow;             // a search needed more than 64 stack entries
     int timeout;                    // a bounded wait gave up
+    int inconsistent;               // a kernel found another's list disagreeing with its own work (a bug)
 };
 
 // The stacks of map_multi (every point count shares them: a warp runs one walk at a time), 2 KB per

@@ -392,6 +392,11 @@ static DcBuffers dc_buffers_of(const sdf_grid& g) {
     b.proj = nullptr;
     b.proj_nsum = nullptr;
     b.proj_cap = 0;
+    b.hbase = nullptr;
+    b.hsample_rep = nullptr;
+    b.hnormals = nullptr;
+    b.qnormals = nullptr;
+    b.qcap = 0;
     return b;
 }
 
