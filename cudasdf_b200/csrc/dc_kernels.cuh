@@ -485,8 +485,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_dc_hermite_reps(GridView g0, 
     }
 }
 
-// computeNormal (:814-844) at every listed representative's edge point, 32 per warp task with the four
-// stencil points of a lane walked together (map_multi), one scene's BVH at a time
+// computeNormal (:814-844) at every listed representative's edge point, 8 per warp task with the four
+// stencil points on four lanes (one walk of 32 points; measured faster than 32 representatives with
+// their four points walked together per lane), one scene's BVH at a time
 __global__ void __launch_bounds__(BLK_THREADS) k_dc_hermite_normals(GridView g0, SceneView sc0, float time,
                                                                    ActiveView av, const float4* __restrict__ reps,
                                                                    const unsigned* __restrict__ counters, unsigned rep_cap,
@@ -494,7 +495,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_hermite_normals(GridView g0,
                                                                    Diag* diag) {
     const unsigned n = min(counters[1], rep_cap);
     const int nact = active_count(av);
-    const int tasks = nact > 0 ? (int)((n + 31u) / 32u) : 0;
+    const int tasks = nact > 0 ? (int)((n + 7u) / 8u) : 0;
     const int lane = threadIdx.x & 31;
     const unsigned FULL = 0xffffffffu;
     for (;;) {
@@ -502,9 +503,10 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_hermite_normals(GridView g0,
         if (lane == 0) t = (int)atomicAdd(ticket, 1u);
         t = __shfl_sync(FULL, t, 0);
         if (t >= tasks) break;
-        const unsigned r = (unsigned)t * 32u + (unsigned)lane;
+        const unsigned r = (unsigned)t * 8u + (unsigned)(lane >> 2);
+        const int kp = lane & 3;
         const bool in = r < n;
-        const float4 rec = reps[in ? r : (unsigned)t * 32u];
+        const float4 rec = reps[in ? r : (unsigned)t * 8u];
         const int ra = __float_as_int(rec.w);
         const bool live = in && ra >= 0 && ra < nact;
         GridView g = g0;
@@ -514,23 +516,25 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_hermite_normals(GridView g0,
         resolve(av, av.list[live ? ra : 0], g, sc, lin, bbase);
         const float3 c = f3(rec.x, rec.y, rec.z);
         const float h = MUL(g.cell, 0.001f);
-        const float3 pts[4] = {c, f3(ADD(c.x, h), c.y, c.z), f3(c.x, ADD(c.y, h), c.z), f3(c.x, c.y, ADD(c.z, h))};
-        float d[4] = {0.f, 0.f, 0.f, 0.f};
+        const float3 pt = kp == 0 ? c : (kp == 1 ? f3(ADD(c.x, h), c.y, c.z) : (kp == 2 ? f3(c.x, ADD(c.y, h), c.z)
+                                                                                     : f3(c.x, c.y, ADD(c.z, h))));
+        float dd = 0.f;
         unsigned pending = __ballot_sync(FULL, live);
         while (pending) {
             const unsigned lead = __shfl_sync(FULL, bbase, __ffs(pending) - 1);
             const bool mine = live && bbase == lead && ((pending >> lane) & 1u);
             SceneView scw = sc;
             if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead)].sc;
-            float dm[4];
-            map_multi<4>(scw, pts, mine, time, dm, diag);
-            if (mine) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) d[q] = dm[q];
-            }
+            MapState<false> st;
+            map_warp<false>(scw, pt, mine, time, st, diag);
+            if (mine) dd = st.d;
             pending &= ~__ballot_sync(FULL, mine);
         }
-        if (live) {
+        const int base = lane & ~3;
+        float d[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) d[q] = __shfl_sync(FULL, dd, base + q);
+        if (live && kp == 0) {
             const float3 gr = f3(SUB(d[1], d[0]), SUB(d[2], d[0]), SUB(d[3], d[0]));
             const float len = SQRT(dot3(gr, gr));
             const float3 nn = len > 1e-6f ? f3(DIV(gr.x, len), DIV(gr.y, len), DIV(gr.z, len)) : f3(0.f, 1.f, 0.f);
@@ -1173,8 +1177,8 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_list(GridView g0, Activ
     }
 }
 
-// computeNormal (:814-844) at the centre of every listed quad (its four decoded cell vertices), 32 quads
-// per warp task with the four stencil points of a lane walked together, one scene's BVH at a time
+// computeNormal (:814-844) at the centre of every listed quad (its four decoded cell vertices), 8 quads
+// per warp task with the four stencil points on four lanes, one scene's BVH at a time
 __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_normals(GridView g0, SceneView sc0, float time,
                                                                 ActiveView av, DcBuffers B,
                                                                 const uint2* __restrict__ recs,
@@ -1184,7 +1188,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_normals(GridView g0, Sc
                                                                 Diag* diag) {
     const unsigned n = min(*total_vertices / 6u, cap);
     const int nact = active_count(av);
-    const int tasks = nact > 0 ? (int)((n + 31u) / 32u) : 0;
+    const int tasks = nact > 0 ? (int)((n + 7u) / 8u) : 0;
     const int lane = threadIdx.x & 31;
     const unsigned FULL = 0xffffffffu;
     for (;;) {
@@ -1192,9 +1196,10 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_normals(GridView g0, Sc
         if (lane == 0) t = (int)atomicAdd(ticket, 1u);
         t = __shfl_sync(FULL, t, 0);
         if (t >= tasks) break;
-        const unsigned qi = (unsigned)t * 32u + (unsigned)lane;
+        const unsigned qi = (unsigned)t * 8u + (unsigned)(lane >> 2);
+        const int kp = lane & 3;
         const bool in = qi < n;
-        const uint2 rec = recs[in ? qi : (unsigned)t * 32u];
+        const uint2 rec = recs[in ? qi : (unsigned)t * 8u];
         const int ra = (int)rec.x, tid = (int)(rec.y >> 2), axis = (int)(rec.y & 3u);
         bool live = in && ra < nact && tid < 512 && axis < 3;
         GridView g = g0;
@@ -1217,24 +1222,24 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_normals(GridView g0, Sc
             }
         }
         const float h = MUL(g.cell, 0.001f);
-        const float3 pts[4] = {qc, f3(ADD(qc.x, h), qc.y, qc.z), f3(qc.x, ADD(qc.y, h), qc.z),
-                               f3(qc.x, qc.y, ADD(qc.z, h))};
-        float d[4] = {0.f, 0.f, 0.f, 0.f};
+        const float3 pt = kp == 0 ? qc : (kp == 1 ? f3(ADD(qc.x, h), qc.y, qc.z)
+                                                  : (kp == 2 ? f3(qc.x, ADD(qc.y, h), qc.z) : f3(qc.x, qc.y, ADD(qc.z, h))));
+        float dd = 0.f;
         unsigned pending = __ballot_sync(FULL, live);
         while (pending) {
             const unsigned lead = __shfl_sync(FULL, bbase, __ffs(pending) - 1);
             const bool mine = live && bbase == lead && ((pending >> lane) & 1u);
             SceneView scw = sc;
             if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead)].sc;
-            float dm[4];
-            map_multi<4>(scw, pts, mine, time, dm, diag);
-            if (mine) {
-#pragma unroll
-                for (int k = 0; k < 4; ++k) d[k] = dm[k];
-            }
+            MapState<false> st;
+            map_warp<false>(scw, pt, mine, time, st, diag);
+            if (mine) dd = st.d;
             pending &= ~__ballot_sync(FULL, mine);
         }
-        if (live) {
+        float d[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) d[k] = __shfl_sync(FULL, dd, (lane & ~3) + k);
+        if (live && kp == 0) {
             const float3 gr = f3(SUB(d[1], d[0]), SUB(d[2], d[0]), SUB(d[3], d[0]));
             const float len = SQRT(dot3(gr, gr));
             const float3 nn = len > 1e-6f ? f3(DIV(gr.x, len), DIV(gr.y, len), DIV(gr.z, len)) : f3(0.f, 1.f, 0.f);
