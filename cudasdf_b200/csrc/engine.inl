@@ -411,7 +411,8 @@ void sdf_engine_set_timing(sdf_engine* e, int enabled) {
 
 // debug bit 0: also write the per-cell counts/offsets of the drop-in layout (marching cubes);
 // debug bit 1: keep each mass-point QEF vertex before its projection steps (buffer 11, float4 per DC
-// vertex, w = 1 where the cell was solved in FP64)
+// vertex, w = 1 where the cell was solved in FP64); debug bit 2: dual contouring with cross-block lists
+// of a few hundred entries (tests of the in-block paths beside the listed ones)
 void sdf_engine_set_debug(sdf_engine* e, int flags) {
     if (e) e->impl.debug = flags;
 }
@@ -868,7 +869,13 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
                              (!B.cell_normals || E.dc_proj_nsum_cap >= E.dc_proj_cap);
         B.proj = project ? E.dc_proj : nullptr;
         B.proj_nsum = project && B.cell_normals ? E.dc_proj_nsum : nullptr;
-        B.proj_cap = project ? (unsigned)std::min<size_t>(E.dc_proj_cap, 0xFFFFFFFFu) : 0u;
+        // debug bit 2: lists of a few hundred entries, so most blocks, passes and vertices take the
+        // in-block paths next to listed ones (the results are the same either way)
+        const bool small_lists = (E.debug & 4) != 0;
+        auto list_cap = [&](size_t c, size_t small) {
+            return (unsigned)std::min<size_t>(small_lists ? std::min(c, small) : c, 0xFFFFFFFFu);
+        };
+        B.proj_cap = project ? list_cap(E.dc_proj_cap, 256) : 0u;
         const bool herm = E.dc_hsamp && E.dc_hreps && E.dc_hnorm && E.dc_hbase && E.dc_hbase_cap >= (size_t)cap &&
                           E.dc_hsamp_cap > 0 && E.dc_hrep_cap > 0;
         B.hbase = herm ? E.dc_hbase : nullptr;
@@ -876,7 +883,7 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
         B.hnormals = herm ? E.dc_hnorm : nullptr;
         const bool qlist = E.dc_qrec && E.dc_qnorm && E.dc_qcap > 0;
         B.qnormals = qlist ? E.dc_qnorm : nullptr;
-        B.qcap = qlist ? (unsigned)std::min<size_t>(E.dc_qcap, 0xFFFFFFFFu) : 0u;
+        B.qcap = qlist ? list_cap(E.dc_qcap, 512) : 0u;
         record(cudaMemsetAsync(E.b2a, 0xFF, (size_t)nb * sizeof(int), st));
         k_dc_block_map<<<(cap + 255) / 256, 256, 0, st>>>(E.list, &ctrl->active_count, cap, nb, E.b2a);
         check_launch();
@@ -901,14 +908,13 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
         if (herm) {
             const size_t hsmem = sizeof(HermSmem);
             k_dc_hermite_reps<<<persistent_grid(k_dc_hermite_reps, SOLVE_THREADS, cap, hsmem), SOLVE_THREADS, hsmem, st>>>(
-                gv, av, E.fields, B, sp, ctrl->herm, E.dc_hsamp, E.dc_hreps,
-                (unsigned)std::min<size_t>(E.dc_hsamp_cap, 0xFFFFFFFFu),
-                (unsigned)std::min<size_t>(E.dc_hrep_cap, 0xFFFFFFFFu), &ctrl->tickets[7]);
+                gv, av, E.fields, B, sp, ctrl->herm, E.dc_hsamp, E.dc_hreps, list_cap(E.dc_hsamp_cap, 512),
+                list_cap(E.dc_hrep_cap, 256), &ctrl->tickets[7]);
             k_dc_hermite_normals<<<persistent_grid(k_dc_hermite_normals, BLK_THREADS,
                                                    std::max(1, (int)(E.dc_hrep_cap / 256))),
                                    BLK_THREADS, 0, st>>>(gv, sv, time, av, E.dc_hreps, ctrl->herm,
-                                                         (unsigned)std::min<size_t>(E.dc_hrep_cap, 0xFFFFFFFFu),
-                                                         E.dc_hnorm, &ctrl->tickets[8], diag);
+                                                         list_cap(E.dc_hrep_cap, 256), E.dc_hnorm, &ctrl->tickets[8],
+                                                         diag);
             check_launch();
         }
         const size_t solve_smem = sizeof(SolveSmem);

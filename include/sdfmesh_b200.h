@@ -275,7 +275,9 @@ void sdf_engine_set_timing(sdf_engine* e, int enabled);
  * the per-cell vertex normals of the reference's dcSolveCellVertices (sdf_engine_buffer 6), which
  * no output of the engine needs; bit 1 keeps, with the mass-point solver, each cell's QEF vertex
  * before its projection steps (sdf_engine_buffer 11: float4 per DC vertex, w = 1 where FP64 solved
- * the cell). */
+ * the cell); bit 2 limits dual contouring's cross-block lists (Hermite normals, projection steps, quad
+ * winding normals) to a few hundred entries, so most of the work takes the in-block paths that handle
+ * what does not fit (the meshes are the same). */
 void sdf_engine_set_debug(sdf_engine* e, int flags);
 /* The scene as uploaded: sorted primitives (count = numPrimitives) and BVH nodes. */
 int sdf_engine_get_bvh(sdf_engine* e, sdf_bvh_node* nodes_out, int capacity, int* num_bvh_primitives);
