@@ -319,6 +319,113 @@ __device__ __forceinline__ void combine(MapState<ATTR>& st, int op, float k, con
     }
 }
 
+// ---------------------------------------------------------------- two points of one lane, one primitive
+// The two points of a map_warp2 lane, (x, y, z0) and (x, y, z1), folding the same primitive: the same
+// operations as two leaf_distance / combine<false> calls, with the type and operation dispatched once
+// and the parts of the transform that depend on x and y alone computed once.
+
+// the primitive-local points of to_local for both points (rotate's operations, shared terms once)
+__device__ __forceinline__ void to_local2(float3 pw, float z1, float4 rot, float4 pos, float4 scale, float3& q0,
+                                          float3& q1) {
+    const float ux = -rot.x, uy = -rot.y, uz = -rot.z, s = rot.w;
+    const float vx = SUB(pw.x, pos.x), vy = SUB(pw.y, pos.y);
+    const float vz0 = SUB(pw.z, pos.z), vz1 = SUB(z1, pos.z);
+    const float axy = FMA(uy, vy, MUL(ux, vx));                         // dot(u, v) without its z term
+    const float b = FMA(s, s, -FMA(uz, uz, FMA(ux, ux, MUL(uy, uy))));  // s*s - dot3(u, u)
+    const float c = MUL(2.0f, s);
+    const float crz = FMA(-uy, vx, MUL(ux, vy));
+    const float cyx = MUL(uz, vx);
+    const float a0 = MUL(2.0f, FMA(uz, vz0, axy)), a1 = MUL(2.0f, FMA(uz, vz1, axy));
+    const float crx0 = FMA(-uz, vy, MUL(uy, vz0)), crx1 = FMA(-uz, vy, MUL(uy, vz1));
+    const float cry0 = FMA(-ux, vz0, cyx), cry1 = FMA(-ux, vz1, cyx);
+    q0 = f3(DIV(FMA(c, crx0, FMA(b, vx, MUL(a0, ux))), scale.x), DIV(FMA(c, cry0, FMA(b, vy, MUL(a0, uy))), scale.y),
+            DIV(FMA(c, crz, FMA(b, vz0, MUL(a0, uz))), scale.z));
+    q1 = f3(DIV(FMA(c, crx1, FMA(b, vx, MUL(a1, ux))), scale.x), DIV(FMA(c, cry1, FMA(b, vy, MUL(a1, uy))), scale.y),
+            DIV(FMA(c, crz, FMA(b, vz1, MUL(a1, uz))), scale.z));
+}
+
+// the displacement of leaf_distance for one local point
+__device__ __forceinline__ float3 displace(const Leaf& L, float3 p, float time) {
+    if (L.disp == DSP_TWIST) {
+        const float c = cosf(MUL(L.dp0, p.y)), s = sinf(MUL(L.dp0, p.y));
+        p = f3(det2(c, p.x, s, p.z), p.y, FMA(c, p.z, MUL(s, p.x)));
+    } else if (L.disp == DSP_BEND) {
+        const float c = cosf(MUL(L.dp0, p.x)), s = sinf(MUL(L.dp0, p.x));
+        p = f3(det2(c, p.x, s, p.y), FMA(c, p.y, MUL(s, p.x)), p.z);
+    } else if (L.disp == DSP_SINE) {
+        p.y = FMA(sinf(FMA(p.x, L.dp0, time)), L.dp1, p.y);
+    }
+    return p;
+}
+
+// sd_eval for two points of the same primitive
+__device__ __forceinline__ void sd_eval2(int type, float3 p0, float3 p1, float4 pm, float& d0, float& d1) {
+    switch (type) {
+        case P_SPHERE: d0 = sd_sphere(p0, pm.x); d1 = sd_sphere(p1, pm.x); break;
+        case P_BOX: d0 = sd_box(p0, pm.x, pm.y, pm.z); d1 = sd_box(p1, pm.x, pm.y, pm.z); break;
+        case P_TORUS: d0 = sd_torus(p0, pm.x, pm.y); d1 = sd_torus(p1, pm.x, pm.y); break;
+        case P_CAPSULE: d0 = sd_capsule(p0, pm.x, pm.y); d1 = sd_capsule(p1, pm.x, pm.y); break;
+        default: d0 = sd_eval(type, p0, pm); d1 = sd_eval(type, p1, pm); break;
+    }
+}
+
+// leaf_distance at (pw.x, pw.y, pw.z) and (pw.x, pw.y, z1)
+__device__ __forceinline__ void leaf_distance2(const Leaf& L, float3 pw, float z1, float time, float& d0, float& d1) {
+    float3 q0, q1;
+    to_local2(pw, z1, L.rot, L.pos, L.scale, q0, q1);
+    if (L.disp != DSP_NONE) {
+        q0 = displace(L, q0, time);
+        q1 = displace(L, q1, time);
+    }
+    sd_eval2(L.type, q0, q1, L.prm, d0, d1);
+    const float ms = fminf(L.scale.x, fminf(L.scale.y, L.scale.z));
+    d0 = MUL(d0, ms);
+    d1 = MUL(d1, ms);
+    if (L.annular > 0.f) {
+        d0 = SUB(fabsf(d0), L.annular);
+        d1 = SUB(fabsf(d1), L.annular);
+    }
+    if (L.rounding > 0.f) {
+        d0 = SUB(d0, L.rounding);
+        d1 = SUB(d1, L.rounding);
+    }
+}
+
+// combine<false>'s new running distance for one point
+template <int OP>
+__device__ __forceinline__ float fold_d(float d, float dp, float k) {
+    if (d == 1e10f) return dp;
+    float h;
+    switch (OP) {
+        case OP_UNION: return dp < d ? dp : d;
+        case OP_SUB: return fmaxf(d, -dp);
+        case OP_INT: return dp > d ? dp : d;
+        case OP_UNION_BLEND:
+            h = CLAMP(ADD(0.5f, DIV(MUL(0.5f, SUB(d, dp)), k)), 0.f, 1.f);
+            return FMA(-MUL(k, h), SUB(1.f, h), mix_fy(d, dp, h));
+        case OP_SUB_BLEND:
+            h = CLAMP(SUB(0.5f, DIV(MUL(0.5f, ADD(d, dp)), k)), 0.f, 1.f);
+            return FMA(MUL(k, h), SUB(1.f, h), mix_fx(d, -dp, h));
+        case OP_INT_BLEND:
+            h = CLAMP(SUB(0.5f, DIV(MUL(0.5f, SUB(d, dp)), k)), 0.f, 1.f);
+            return FMA(MUL(k, h), SUB(1.f, h), mix_fy(d, dp, h));
+        default: return d;
+    }
+}
+
+// combine<false> for both points, the operation dispatched once
+__device__ __forceinline__ void combine_d2(int op, float k, float& d0, float& d1, float dp0, float dp1) {
+    switch (op) {
+        case OP_UNION: d0 = fold_d<OP_UNION>(d0, dp0, k); d1 = fold_d<OP_UNION>(d1, dp1, k); break;
+        case OP_SUB: d0 = fold_d<OP_SUB>(d0, dp0, k); d1 = fold_d<OP_SUB>(d1, dp1, k); break;
+        case OP_INT: d0 = fold_d<OP_INT>(d0, dp0, k); d1 = fold_d<OP_INT>(d1, dp1, k); break;
+        case OP_UNION_BLEND: d0 = fold_d<OP_UNION_BLEND>(d0, dp0, k); d1 = fold_d<OP_UNION_BLEND>(d1, dp1, k); break;
+        case OP_SUB_BLEND: d0 = fold_d<OP_SUB_BLEND>(d0, dp0, k); d1 = fold_d<OP_SUB_BLEND>(d1, dp1, k); break;
+        case OP_INT_BLEND: d0 = fold_d<OP_INT_BLEND>(d0, dp0, k); d1 = fold_d<OP_INT_BLEND>(d1, dp1, k); break;
+        default: d0 = fold_d<-1>(d0, dp0, k); d1 = fold_d<-1>(d1, dp1, k); break;
+    }
+}
+
 // intersectAABB (MarchingCubesKernels.cu:564-568): sqrt_rn(|p - box|^2) < running d.
 // The same decision without the square root in all but boundary cases: with D = dmin^2 rounded,
 // dd < D(1 - 2^-20) implies sqrt_rn(dd) < dmin, and dd > D(1 + 2^-20) implies sqrt_rn(dd) > dmin
@@ -572,8 +679,22 @@ __device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float 
                     cnt_leaves += __popc(hm0) + __popc(hm1);
                     cnt_wleaves += (__any_sync(FULL, h0 || h1) ? 1 : 0) + (__any_sync(FULL, h0 && h1) ? 1 : 0);
                 }
-                // first pass: each lane's first hit point; second pass: point 1 of lanes that hit both
-                if (h0 || h1) {
+                if (__any_sync(FULL, h0 && h1)) {
+                    // some lane folds the primitive into both its points: one pass evaluates both
+                    // points of every lane that hit with either, and each point keeps the fold only
+                    // where it hit (an unchanged distance leaves its prune bound unchanged)
+                    if (h0 || h1) {
+                        float dp0, dp1;
+                        leaf_distance2(L, p0, z1, time, dp0, dp1);
+                        float n0 = s0.d, n1 = s1.d;
+                        combine_d2(L.op, L.pos.w, n0, n1, dp0, dp1);
+                        s0.d = h0 ? n0 : s0.d;
+                        s1.d = h1 ? n1 : s1.d;
+                        b0.set(s0.d);
+                        b1.set(s1.d);
+                    }
+                } else if (h0 || h1) {
+                    // each lane folds the primitive into one point
                     const bool use0 = h0;
                     MapState<false> t;
                     t.d = use0 ? s0.d : s1.d;
@@ -587,12 +708,6 @@ __device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float 
                         s1.d = t.d;
                         b1.set(t.d);
                     }
-                }
-                if (h0 && h1) {
-                    float3 pre;
-                    const float dp = leaf_distance(L, p1, time, pre);
-                    combine<false>(s1, L.op, L.pos.w, pr, left, dp, pre);
-                    b1.set(s1.d);
                 }
             } else {
                 if (sp + 2 > MAP_STACK) { overflow = true; break; }  // the reference's stack holds both
