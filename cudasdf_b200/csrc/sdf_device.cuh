@@ -510,6 +510,36 @@ struct Diag {
 constexpr int MULTI_STACK_UINT4 = MAP_STACK * 2;  // uint4 per warp
 __shared__ uint4 s_multi_stack[MAP_WARPS * MULTI_STACK_UINT4];
 
+// The first pops of every walk. While no primitive has been folded, every running distance is 1e10,
+// and a box whose six coordinates are below 1e8 in magnitude passes the prune test for every point
+// below 1e8 (squared distance under 1.2e17, square root under 3.5e8 < 1e10). So every walk starts by
+// popping the root and descending along left children, each point hitting every node, each right
+// child pushed with the live masks, down to the first leaf. first_descent replays that without the
+// box tests: push(sp, right) stores one entry (lane 0), and the return value is the number of
+// internal nodes popped (each live point's pop count). It stops at a leaf, at a box outside the bound
+// and where the ordinary walk would overflow the stack; the ordinary walk then pops `node` next.
+constexpr float DESCENT_BOUND = 1e8f;
+__device__ __forceinline__ bool below_descent_bound(float x) { return fabsf(x) < DESCENT_BOUND; }  // NaN fails
+template <class Push>
+__device__ __forceinline__ int first_descent(const SceneView& sc, int& node, int& sp, Push push) {
+    int depth = 0;
+    for (;;) {
+        const float4 nb = __ldg(sc.nodes + 2 * node + 1);
+        const int right = __float_as_int(nb.w);
+        if (right == -1 || sp + 2 > MAP_STACK) break;
+        const float4 na = __ldg(sc.nodes + 2 * node);
+        if (!(below_descent_bound(na.x) && below_descent_bound(na.y) && below_descent_bound(na.z) &&
+              below_descent_bound(na.w) && below_descent_bound(nb.x) && below_descent_bound(nb.y)))
+            break;
+        push(sp, right);
+        ++sp;
+        node = __float_as_int(nb.z);
+        ++depth;
+    }
+    __syncwarp();  // the pushed entries are visible to the warp's pops
+    return depth;
+}
+
 // map() for the 32 points of a warp. Must be called by all 32 lanes together (warp-uniform control
 // flow); lanes with valid == false take part in the walk but own no point.
 template <bool ATTR, bool COUNT = false>
@@ -536,6 +566,14 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
         int node = 0;
         unsigned mask = live;
         bool have = true;
+        // counting runs walk every pop, so the work counters count the descent's tests too
+        if (!COUNT && __all_sync(FULL, !valid || (below_descent_bound(p.x) && below_descent_bound(p.y) &&
+                                                  below_descent_bound(p.z)))) {
+            const int depth = first_descent(sc, node, sp, [&](int s, int right) {
+                if (lane == 0) stk[s] = make_uint2((unsigned)right, live);
+            });
+            if (valid) iter = depth;
+        }
         for (;;) {
             if (!have) {
                 if (sp == 0) break;
@@ -643,6 +681,15 @@ __device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float 
         int node = 0;
         unsigned m0 = live0, m1 = live1;
         bool have = true;
+        const bool xy_ok = below_descent_bound(p0.x) && below_descent_bound(p0.y);
+        if (!COUNT && __all_sync(FULL, (!v0 || (xy_ok && below_descent_bound(p0.z))) &&
+                                           (!v1 || (xy_ok && below_descent_bound(z1))))) {
+            const int depth = first_descent(sc, node, sp, [&](int s, int right) {
+                if (lane == 0) stk[s] = make_uint4((unsigned)right, live0, live1, 0u);
+            });
+            if (v0) it0 = depth;
+            if (v1) it1 = depth;
+        }
         for (;;) {
             if (!have) {
                 if (sp == 0) break;
@@ -787,6 +834,29 @@ __device__ __forceinline__ void map_multi(const SceneView& sc, const float3 (&p)
 #pragma unroll
         for (int i = 0; i < NP; ++i) m[i] = live;
         bool have = true;
+        bool in_bound = true;
+#pragma unroll
+        for (int i = 0; i < NP; ++i)
+            in_bound = in_bound && below_descent_bound(p[i].x) && below_descent_bound(p[i].y) &&
+                       below_descent_bound(p[i].z);
+        if (__all_sync(FULL, !valid || in_bound)) {
+            const int depth = first_descent(sc, node, sp, [&](int s, int right) {
+                if (lane == 0) {
+                    unsigned w[4 * W4];
+                    w[0] = (unsigned)right;
+#pragma unroll
+                    for (int i = 0; i < NP; ++i) w[i + 1] = live;
+#pragma unroll
+                    for (int i = NP + 1; i < 4 * W4; ++i) w[i] = 0u;
+#pragma unroll
+                    for (int k = 0; k < W4; ++k) stk[s][k] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
+                }
+            });
+            if (valid) {
+#pragma unroll
+                for (int i = 0; i < NP; ++i) it[i] = depth;
+            }
+        }
         for (;;) {
             if (!have) {
                 if (sp == 0) break;
