@@ -485,9 +485,41 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_dc_hermite_reps(GridView g0, 
     }
 }
 
-// computeNormal (:814-844) at every listed representative's edge point, 8 per warp task with the four
-// stencil points on four lanes (one walk of 32 points; measured faster than 32 representatives with
-// their four points walked together per lane), one scene's BVH at a time
+// computeNormal (:814-844) at centre c, its four stencil points held by two neighbouring lanes (even lane:
+// c and c + h z; odd lane: c + h x and c + h y) and walked two per lane by map_pair, one scene's BVH at a
+// time (bbase: the lane's scene block base). The normal is returned on the even lane of each pair.
+__device__ __forceinline__ float3 stencil_normal_pairs(const ActiveView& av, const SceneView& sc, unsigned bbase,
+                                                       float3 c, float cell, bool live, float time, Diag* diag) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const bool odd = (lane & 1) != 0;
+    const float h = MUL(cell, 0.001f);
+    const float3 pa = odd ? f3(ADD(c.x, h), c.y, c.z) : c;
+    const float3 pb = odd ? f3(c.x, ADD(c.y, h), c.z) : f3(c.x, c.y, ADD(c.z, h));
+    float da = 0.f, db = 0.f;
+    unsigned pending = __ballot_sync(FULL, live);
+    while (pending) {
+        const unsigned lead = __shfl_sync(FULL, bbase, __ffs(pending) - 1);
+        const bool mine = live && bbase == lead && ((pending >> lane) & 1u);
+        SceneView scw = sc;
+        if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead)].sc;
+        float a, b;
+        map_pair<false, false>(scw, pa, pb, mine, mine, time, a, b, diag);
+        if (mine) {
+            da = a;
+            db = b;
+        }
+        pending &= ~__ballot_sync(FULL, mine);
+    }
+    const float d1 = __shfl_xor_sync(FULL, da, 1), d2 = __shfl_xor_sync(FULL, db, 1);  // the odd lane's points
+    const float3 gr = f3(SUB(d1, da), SUB(d2, da), SUB(db, da));
+    const float len = SQRT(dot3(gr, gr));
+    return len > 1e-6f ? f3(DIV(gr.x, len), DIV(gr.y, len), DIV(gr.z, len)) : f3(0.f, 1.f, 0.f);
+}
+
+// computeNormal at every listed representative's edge point, 16 per warp task with two stencil points
+// per lane on two lanes (measured faster than four lanes of one point, and than 32 representatives
+// with their four points walked together per lane)
 __global__ void __launch_bounds__(BLK_THREADS) k_dc_hermite_normals(GridView g0, SceneView sc0, float time,
                                                                    ActiveView av, const float4* __restrict__ reps,
                                                                    const unsigned* __restrict__ counters, unsigned rep_cap,
@@ -495,7 +527,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_hermite_normals(GridView g0,
                                                                    Diag* diag) {
     const unsigned n = min(counters[1], rep_cap);
     const int nact = active_count(av);
-    const int tasks = nact > 0 ? (int)((n + 7u) / 8u) : 0;
+    const int tasks = nact > 0 ? (int)((n + 15u) / 16u) : 0;
     const int lane = threadIdx.x & 31;
     const unsigned FULL = 0xffffffffu;
     for (;;) {
@@ -503,10 +535,9 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_hermite_normals(GridView g0,
         if (lane == 0) t = (int)atomicAdd(ticket, 1u);
         t = __shfl_sync(FULL, t, 0);
         if (t >= tasks) break;
-        const unsigned r = (unsigned)t * 8u + (unsigned)(lane >> 2);
-        const int kp = lane & 3;
+        const unsigned r = (unsigned)t * 16u + (unsigned)(lane >> 1);
         const bool in = r < n;
-        const float4 rec = reps[in ? r : (unsigned)t * 8u];
+        const float4 rec = reps[in ? r : (unsigned)t * 16u];
         const int ra = __float_as_int(rec.w);
         const bool live = in && ra >= 0 && ra < nact;
         GridView g = g0;
@@ -514,32 +545,8 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_hermite_normals(GridView g0,
         int lin;
         unsigned bbase;
         resolve(av, av.list[live ? ra : 0], g, sc, lin, bbase);
-        const float3 c = f3(rec.x, rec.y, rec.z);
-        const float h = MUL(g.cell, 0.001f);
-        const float3 pt = kp == 0 ? c : (kp == 1 ? f3(ADD(c.x, h), c.y, c.z) : (kp == 2 ? f3(c.x, ADD(c.y, h), c.z)
-                                                                                     : f3(c.x, c.y, ADD(c.z, h))));
-        float dd = 0.f;
-        unsigned pending = __ballot_sync(FULL, live);
-        while (pending) {
-            const unsigned lead = __shfl_sync(FULL, bbase, __ffs(pending) - 1);
-            const bool mine = live && bbase == lead && ((pending >> lane) & 1u);
-            SceneView scw = sc;
-            if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead)].sc;
-            MapState<false> st;
-            map_warp<false>(scw, pt, mine, time, st, diag);
-            if (mine) dd = st.d;
-            pending &= ~__ballot_sync(FULL, mine);
-        }
-        const int base = lane & ~3;
-        float d[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) d[q] = __shfl_sync(FULL, dd, base + q);
-        if (live && kp == 0) {
-            const float3 gr = f3(SUB(d[1], d[0]), SUB(d[2], d[0]), SUB(d[3], d[0]));
-            const float len = SQRT(dot3(gr, gr));
-            const float3 nn = len > 1e-6f ? f3(DIV(gr.x, len), DIV(gr.y, len), DIV(gr.z, len)) : f3(0.f, 1.f, 0.f);
-            normals[r] = make_float4(nn.x, nn.y, nn.z, 0.f);
-        }
+        const float3 nn = stencil_normal_pairs(av, sc, bbase, f3(rec.x, rec.y, rec.z), g.cell, live, time, diag);
+        if (live && (lane & 1) == 0) normals[r] = make_float4(nn.x, nn.y, nn.z, 0.f);
     }
 }
 
@@ -729,7 +736,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
             // independent of finite differences of the field at the vertex, and every operation is
             // rounded on its own, so a float32 restatement on the host reproduces the steps.
             // The steps of a block's few cells leave most warps of the CTA idle at the next barrier, so
-            // every cell whose vertex slot has a projection record is handed to k_dc_project (32 cells
+            // every cell whose vertex slot has a projection record is handed to k_dc_project (64 cells
             // per warp over all blocks) with its start point and direction; the others finish here.
             const bool handoff = P.solver == SDF_DC_SOLVER_MASSPOINT && P.projection_iters > 0 && B.proj;
             if (P.solver == SDF_DC_SOLVER_MASSPOINT && P.projection_iters > 0) {
@@ -833,18 +840,101 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 3) k_dc_solve(GridView g0, Scen
     }
 }
 
-// The mass-point projection steps and the finishing of the DC vertices handed off by k_dc_solve: 32
-// vertices per warp task in vertex order (so a warp's cells are neighbours from one or two blocks),
-// each lane taking x <- x - f(x) n along its cell's mean Hermite normal, in cell-local coordinates kept
-// in the cell widened by 0.1 cell, then the clamps, the blend and the encoding of k_dc_solve. The same
-// operations as there, so the vertices are the same; a warp walks one scene's BVH at a time.
+// one vertex of k_dc_project: its record's cell corner, mean Hermite normal and cell-local point
+struct ProjVertex {
+    unsigned v;
+    bool live, has_dir;
+    unsigned bbase;
+    float cell;
+    float3 cm, nbar, y;
+};
+
+__device__ __forceinline__ ProjVertex proj_vertex(const GridView& g0, const ActiveView& av, const DcBuffers& B,
+                                                  unsigned v, unsigned n, unsigned first, int nact) {
+    ProjVertex V;
+    V.v = v;
+    const unsigned vv = v < n ? v : first;  // vertices past the end read the task's first record
+    const float4 r0 = B.proj[2 * (size_t)vv], r1 = B.proj[2 * (size_t)vv + 1];
+    const int ra = __float_as_int(r0.w);
+    const unsigned cw = __float_as_uint(r1.w);
+    // every vertex below n has a record from k_dc_solve; a record that names no active block or cell
+    // is skipped rather than followed
+    const bool ok = ra >= 0 && ra < nact && (cw & 0xFFFFu) < 512u;
+    V.live = v < n && ok;
+    V.has_dir = V.live && ((cw >> 16) & 1u);
+    GridView g = g0;
+    SceneView unused;
+    int lin;
+    resolve(av, av.list[ok ? ra : 0], g, unused, lin, V.bbase);
+    int bx, by, bz;
+    block_coord(g, lin, bx, by, bz);
+    const CellInfo c = cell_info(g, bx, by, bz, ok ? (int)(cw & 0xFFFFu) : 0);
+    V.cm = grid_loc(g, c.x, c.y, c.z);
+    V.cell = g.cell;
+    V.nbar = f3(r1.x, r1.y, r1.z);
+    V.y = f3(r0.x, r0.y, r0.z);
+    return V;
+}
+
+// one projection step: y <- y - f n, kept in the cell widened by 0.1 cell
+__device__ __forceinline__ void proj_step(ProjVertex& V, bool mine, float d) {
+    if (mine && V.has_dir && isfinite(d)) {
+        const float margin = MUL(0.10f, V.cell), hi = ADD(V.cell, margin);
+        const float3 yn = sub3(V.y, scl3(V.nbar, d));
+        V.y = f3(CLAMP(yn.x, -margin, hi), CLAMP(yn.y, -margin, hi), CLAMP(yn.z, -margin, hi));
+    }
+}
+
+// soft clamp, hard clamp to the cell, blend towards the cell centre (:1556-1577)
+__device__ __forceinline__ float3 proj_finish(const ProjVertex& V, float qef_blend) {
+    const float3 cm = V.cm;
+    const float margin = MUL(0.10f, V.cell);
+    float3 x = add3(cm, V.y);
+    const float3 cmax = f3(ADD(cm.x, V.cell), ADD(cm.y, V.cell), ADD(cm.z, V.cell));
+    x = f3(CLAMP(x.x, SUB(cm.x, margin), ADD(cmax.x, margin)), CLAMP(x.y, SUB(cm.y, margin), ADD(cmax.y, margin)),
+           CLAMP(x.z, SUB(cm.z, margin), ADD(cmax.z, margin)));
+    x = f3(CLAMP(x.x, cm.x, cmax.x), CLAMP(x.y, cm.y, cmax.y), CLAMP(x.z, cm.z, cmax.z));
+    const float3 ctr = f3(FMA(0.5f, V.cell, cm.x), FMA(0.5f, V.cell, cm.y), FMA(0.5f, V.cell, cm.z));
+    return lerp3(ctr, x, qef_blend);
+}
+
+// vertex normal: averaged Hermite normals, oriented by the SDF gradient at the vertex
+__device__ __forceinline__ void proj_normal(const ActiveView& av, const SceneView& sc0, const DcBuffers& B,
+                                            const ProjVertex& V, float3 x, float time, Diag* diag) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    unsigned pending = __ballot_sync(FULL, V.live);
+    while (pending) {
+        const unsigned lead = __shfl_sync(FULL, V.bbase, __ffs(pending) - 1);
+        const bool mine = V.live && V.bbase == lead && ((pending >> lane) & 1u);
+        SceneView scw = sc0;
+        if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead)].sc;
+        const float3 nref = normal_warp(scw, x, mine, time, V.cell, diag);
+        if (mine) {
+            const float4 r = B.proj_nsum[V.v];
+            const float3 nsum = f3(r.x, r.y, r.z);
+            const float len = SQRT(dot3(nsum, nsum));
+            float3 nout = (len > 1e-6f) ? f3(DIV(nsum.x, len), DIV(nsum.y, len), DIV(nsum.z, len)) : nref;
+            if (dot3(nout, nref) < 0.f) nout = f3(-nout.x, -nout.y, -nout.z);
+            B.cell_normals[V.v] = encode_normal(nout);
+        }
+        pending &= ~__ballot_sync(FULL, mine);
+    }
+}
+
+// The mass-point projection steps and the finishing of the DC vertices handed off by k_dc_solve: 64
+// vertices per warp task in vertex order (so a warp's cells are neighbours from one or two blocks), two
+// consecutive vertices per lane walked together by map_pair (each point its own walk), each taking
+// x <- x - f(x) n along its cell's mean Hermite normal, in cell-local coordinates kept in the cell
+// widened by 0.1 cell, then the clamps, the blend and the encoding of k_dc_solve. The same operations
+// as there, so the vertices are the same; a warp walks one scene's BVH at a time.
 __global__ void __launch_bounds__(BLK_THREADS) k_dc_project(GridView g0, SceneView sc0, float time, ActiveView av,
                                                            DcBuffers B, DcSolveParams P,
                                                            const unsigned* __restrict__ nverts, unsigned* ticket,
                                                            Diag* diag) {
     const unsigned n = min(min(*nverts, B.proj_cap), P.max_cell_vertices);
     const int nact = active_count(av);
-    const int tasks = nact > 0 ? (int)((n + 31u) / 32u) : 0;
+    const int tasks = nact > 0 ? (int)((n + 63u) / 64u) : 0;
     const int lane = threadIdx.x & 31;
     const unsigned FULL = 0xffffffffu;
     for (;;) {
@@ -852,73 +942,34 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_project(GridView g0, SceneVi
         if (lane == 0) t = (int)atomicAdd(ticket, 1u);
         t = __shfl_sync(FULL, t, 0);
         if (t >= tasks) break;
-        const unsigned v = (unsigned)t * 32u + (unsigned)lane;
-        const unsigned vv = v < n ? v : (unsigned)t * 32u;  // lanes past the end read the task's first record
-        const float4 r0 = B.proj[2 * (size_t)vv], r1 = B.proj[2 * (size_t)vv + 1];
-        const int ra = __float_as_int(r0.w);
-        const unsigned cw = __float_as_uint(r1.w);
-        // every vertex below n has a record from k_dc_solve; a record that names no active block or cell
-        // is skipped rather than followed
-        const bool ok = ra >= 0 && ra < nact && (cw & 0xFFFFu) < 512u;
-        const bool live = v < n && ok;
-        const int a = ok ? ra : 0;
-        const bool has_dir = live && ((cw >> 16) & 1u);
-        GridView g = g0;
-        SceneView sc = sc0;
-        int lin;
-        unsigned bbase;
-        resolve(av, av.list[a], g, sc, lin, bbase);
-        int bx, by, bz;
-        block_coord(g, lin, bx, by, bz);
-        const CellInfo c = cell_info(g, bx, by, bz, ok ? (int)(cw & 0xFFFFu) : 0);
-        const float3 cm = grid_loc(g, c.x, c.y, c.z);
-        const float3 nbar = f3(r1.x, r1.y, r1.z);
-        float3 y = f3(r0.x, r0.y, r0.z);
-        const float margin = MUL(0.10f, g.cell), hi = ADD(g.cell, margin);
+        const unsigned first = (unsigned)t * 64u, v0 = first + 2u * (unsigned)lane;
+        ProjVertex V0 = proj_vertex(g0, av, B, v0, n, first, nact);
+        ProjVertex V1 = proj_vertex(g0, av, B, v0 + 1u, n, first, nact);
         for (int it = 0; it < P.projection_iters; ++it) {
-            unsigned pending = __ballot_sync(FULL, live);
-            while (pending) {
-                const unsigned lead = __shfl_sync(FULL, bbase, __ffs(pending) - 1);
-                const bool mine = live && bbase == lead && ((pending >> lane) & 1u);
-                SceneView scw = sc;
+            unsigned pend0 = __ballot_sync(FULL, V0.live), pend1 = __ballot_sync(FULL, V1.live);
+            while (pend0 | pend1) {
+                // the scene of the first pending point (every point of a lane in it walks now)
+                const unsigned lead = pend0 ? __shfl_sync(FULL, V0.bbase, __ffs(pend0) - 1)
+                                            : __shfl_sync(FULL, V1.bbase, __ffs(pend1) - 1);
+                const bool mine0 = V0.live && V0.bbase == lead && ((pend0 >> lane) & 1u);
+                const bool mine1 = V1.live && V1.bbase == lead && ((pend1 >> lane) & 1u);
+                SceneView scw = sc0;
                 if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead)].sc;
-                MapState<false> st;
-                map_warp<false>(scw, add3(cm, y), mine && has_dir, time, st, diag);
-                if (mine && has_dir && isfinite(st.d)) {
-                    const float3 yn = sub3(y, scl3(nbar, st.d));
-                    y = f3(CLAMP(yn.x, -margin, hi), CLAMP(yn.y, -margin, hi), CLAMP(yn.z, -margin, hi));
-                }
-                pending &= ~__ballot_sync(FULL, mine);
+                float d0, d1;
+                map_pair<false, false>(scw, add3(V0.cm, V0.y), add3(V1.cm, V1.y), mine0 && V0.has_dir,
+                                       mine1 && V1.has_dir, time, d0, d1, diag);
+                proj_step(V0, mine0, d0);
+                proj_step(V1, mine1, d1);
+                pend0 &= ~__ballot_sync(FULL, mine0);
+                pend1 &= ~__ballot_sync(FULL, mine1);
             }
         }
-        // soft clamp, hard clamp to the cell, blend towards the cell centre (:1556-1577)
-        float3 x = add3(cm, y);
-        const float3 cmax = f3(ADD(cm.x, g.cell), ADD(cm.y, g.cell), ADD(cm.z, g.cell));
-        x = f3(CLAMP(x.x, SUB(cm.x, margin), ADD(cmax.x, margin)), CLAMP(x.y, SUB(cm.y, margin), ADD(cmax.y, margin)),
-               CLAMP(x.z, SUB(cm.z, margin), ADD(cmax.z, margin)));
-        x = f3(CLAMP(x.x, cm.x, cmax.x), CLAMP(x.y, cm.y, cmax.y), CLAMP(x.z, cm.z, cmax.z));
-        const float3 ctr = f3(FMA(0.5f, g.cell, cm.x), FMA(0.5f, g.cell, cm.y), FMA(0.5f, g.cell, cm.z));
-        x = lerp3(ctr, x, P.qef_blend);
-        if (live) B.cell_verts[v] = encode_vertex(x, cm, g.cell);
-        // vertex normal: averaged Hermite normals, oriented by the SDF gradient at the vertex
+        const float3 x0 = proj_finish(V0, P.qef_blend), x1 = proj_finish(V1, P.qef_blend);
+        if (V0.live) B.cell_verts[V0.v] = encode_vertex(x0, V0.cm, V0.cell);
+        if (V1.live) B.cell_verts[V1.v] = encode_vertex(x1, V1.cm, V1.cell);
         if (B.cell_normals && B.proj_nsum) {
-            unsigned pending = __ballot_sync(FULL, live);
-            while (pending) {
-                const unsigned lead = __shfl_sync(FULL, bbase, __ffs(pending) - 1);
-                const bool mine = live && bbase == lead && ((pending >> lane) & 1u);
-                SceneView scw = sc;
-                if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead)].sc;
-                const float3 nref = normal_warp(scw, x, mine, time, g.cell, diag);
-                if (mine) {
-                    const float4 r = B.proj_nsum[v];
-                    const float3 nsum = f3(r.x, r.y, r.z);
-                    const float len = SQRT(dot3(nsum, nsum));
-                    float3 nout = (len > 1e-6f) ? f3(DIV(nsum.x, len), DIV(nsum.y, len), DIV(nsum.z, len)) : nref;
-                    if (dot3(nout, nref) < 0.f) nout = f3(-nout.x, -nout.y, -nout.z);
-                    B.cell_normals[v] = encode_normal(nout);
-                }
-                pending &= ~__ballot_sync(FULL, mine);
-            }
+            proj_normal(av, sc0, B, V0, x0, time, diag);
+            proj_normal(av, sc0, B, V1, x1, time, diag);
         }
     }
 }
@@ -1177,8 +1228,8 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_list(GridView g0, Activ
     }
 }
 
-// computeNormal (:814-844) at the centre of every listed quad (its four decoded cell vertices), 8 quads
-// per warp task with the four stencil points on four lanes, one scene's BVH at a time
+// computeNormal (:814-844) at the centre of every listed quad (its four decoded cell vertices), 16 quads
+// per warp task with two stencil points per lane on two lanes, one scene's BVH at a time
 __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_normals(GridView g0, SceneView sc0, float time,
                                                                 ActiveView av, DcBuffers B,
                                                                 const uint2* __restrict__ recs,
@@ -1188,7 +1239,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_normals(GridView g0, Sc
                                                                 Diag* diag) {
     const unsigned n = min(*total_vertices / 6u, cap);
     const int nact = active_count(av);
-    const int tasks = nact > 0 ? (int)((n + 7u) / 8u) : 0;
+    const int tasks = nact > 0 ? (int)((n + 15u) / 16u) : 0;
     const int lane = threadIdx.x & 31;
     const unsigned FULL = 0xffffffffu;
     for (;;) {
@@ -1196,10 +1247,9 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_normals(GridView g0, Sc
         if (lane == 0) t = (int)atomicAdd(ticket, 1u);
         t = __shfl_sync(FULL, t, 0);
         if (t >= tasks) break;
-        const unsigned qi = (unsigned)t * 8u + (unsigned)(lane >> 2);
-        const int kp = lane & 3;
+        const unsigned qi = (unsigned)t * 16u + (unsigned)(lane >> 1);
         const bool in = qi < n;
-        const uint2 rec = recs[in ? qi : (unsigned)t * 8u];
+        const uint2 rec = recs[in ? qi : (unsigned)t * 16u];
         const int ra = (int)rec.x, tid = (int)(rec.y >> 2), axis = (int)(rec.y & 3u);
         bool live = in && ra < nact && tid < 512 && axis < 3;
         GridView g = g0;
@@ -1221,30 +1271,8 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_normals(GridView g0, Sc
                 qc = Q.qc;
             }
         }
-        const float h = MUL(g.cell, 0.001f);
-        const float3 pt = kp == 0 ? qc : (kp == 1 ? f3(ADD(qc.x, h), qc.y, qc.z)
-                                                  : (kp == 2 ? f3(qc.x, ADD(qc.y, h), qc.z) : f3(qc.x, qc.y, ADD(qc.z, h))));
-        float dd = 0.f;
-        unsigned pending = __ballot_sync(FULL, live);
-        while (pending) {
-            const unsigned lead = __shfl_sync(FULL, bbase, __ffs(pending) - 1);
-            const bool mine = live && bbase == lead && ((pending >> lane) & 1u);
-            SceneView scw = sc;
-            if (av.scenes) scw = av.scenes[scene_of_block(av.scenes, av.nscenes, lead)].sc;
-            MapState<false> st;
-            map_warp<false>(scw, pt, mine, time, st, diag);
-            if (mine) dd = st.d;
-            pending &= ~__ballot_sync(FULL, mine);
-        }
-        float d[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) d[k] = __shfl_sync(FULL, dd, (lane & ~3) + k);
-        if (live && kp == 0) {
-            const float3 gr = f3(SUB(d[1], d[0]), SUB(d[2], d[0]), SUB(d[3], d[0]));
-            const float len = SQRT(dot3(gr, gr));
-            const float3 nn = len > 1e-6f ? f3(DIV(gr.x, len), DIV(gr.y, len), DIV(gr.z, len)) : f3(0.f, 1.f, 0.f);
-            normals[qi] = make_float4(nn.x, nn.y, nn.z, 0.f);
-        }
+        const float3 nn = stencil_normal_pairs(av, sc, bbase, qc, g.cell, live, time, diag);
+        if (live && (lane & 1) == 0) normals[qi] = make_float4(nn.x, nn.y, nn.z, 0.f);
     }
 }
 

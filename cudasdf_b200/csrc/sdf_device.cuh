@@ -320,9 +320,9 @@ __device__ __forceinline__ void combine(MapState<ATTR>& st, int op, float k, con
 }
 
 // ---------------------------------------------------------------- two points of one lane, one primitive
-// The two points of a map_warp2 lane, (x, y, z0) and (x, y, z1), folding the same primitive: the same
-// operations as two leaf_distance / combine<false> calls, with the type and operation dispatched once
-// and the parts of the transform that depend on x and y alone computed once.
+// The two points of a map_pair lane folding the same primitive: the same operations as two
+// leaf_distance / combine<false> calls, with the type and operation dispatched once and, for points
+// (x, y, z0) and (x, y, z1), the parts of the transform that depend on x and y alone computed once.
 
 // the primitive-local points of to_local for both points (rotate's operations, shared terms once)
 __device__ __forceinline__ void to_local2(float3 pw, float z1, float4 rot, float4 pos, float4 scale, float3& q0,
@@ -369,10 +369,16 @@ __device__ __forceinline__ void sd_eval2(int type, float3 p0, float3 p1, float4 
     }
 }
 
-// leaf_distance at (pw.x, pw.y, pw.z) and (pw.x, pw.y, z1)
-__device__ __forceinline__ void leaf_distance2(const Leaf& L, float3 pw, float z1, float time, float& d0, float& d1) {
+// leaf_distance at p0 and p1 (SAME_XY: p1 differs from p0 only in z, and the transform shares terms)
+template <bool SAME_XY>
+__device__ __forceinline__ void leaf_distance2(const Leaf& L, float3 p0, float3 p1, float time, float& d0, float& d1) {
     float3 q0, q1;
-    to_local2(pw, z1, L.rot, L.pos, L.scale, q0, q1);
+    if (SAME_XY) {
+        to_local2(p0, p1.z, L.rot, L.pos, L.scale, q0, q1);
+    } else {
+        q0 = to_local(p0, L.rot, L.pos, L.scale);
+        q1 = to_local(p1, L.rot, L.pos, L.scale);
+    }
     if (L.disp != DSP_NONE) {
         q0 = displace(L, q0, time);
         q1 = displace(L, q1, time);
@@ -656,12 +662,12 @@ __device__ __forceinline__ void map_warp(const SceneView& sc, float3 p, bool val
 // the ballots and the push are shared by the two walks while every point still makes its own prune
 // decision at every node it pops: each point's sequence of pops is its own depth-first walk with the
 // 64-entry stack and the 256-pop cap, exactly as in map_warp. Must be called by all 32 lanes.
-// The two points of a lane differ only in z (p1 = (p0.x, p0.y, z1)), so the x and y part of each box
-// distance is computed once for both.
-template <bool COUNT = false>
-__device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float z1, bool v0, bool v1, float time,
-                                          float& d0, float& d1, Diag* diag) {
-    const float3 p1 = f3(p0.x, p0.y, z1);
+// SAME_XY: the two points of every lane differ only in z (p1.x == p0.x, p1.y == p0.y), so the x and y
+// part of each box distance and of each primitive transform is computed once for both.
+template <bool COUNT, bool SAME_XY>
+__device__ __forceinline__ void map_pair(const SceneView& sc, float3 p0, float3 p1, bool v0, bool v1, float time,
+                                         float& d0, float& d1, Diag* diag) {
+    const float z1 = p1.z;
     unsigned long long cnt_pops = 0, cnt_leaves = 0, cnt_wpops = 0, cnt_wtests = 0, cnt_wleaves = 0;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -681,9 +687,9 @@ __device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float 
         int node = 0;
         unsigned m0 = live0, m1 = live1;
         bool have = true;
-        const bool xy_ok = below_descent_bound(p0.x) && below_descent_bound(p0.y);
-        if (!COUNT && __all_sync(FULL, (!v0 || (xy_ok && below_descent_bound(p0.z))) &&
-                                           (!v1 || (xy_ok && below_descent_bound(z1))))) {
+        const bool ok0 = below_descent_bound(p0.x) && below_descent_bound(p0.y) && below_descent_bound(p0.z);
+        const bool ok1 = below_descent_bound(p1.x) && below_descent_bound(p1.y) && below_descent_bound(p1.z);
+        if (!COUNT && __all_sync(FULL, (!v0 || ok0) && (!v1 || ok1))) {
             const int depth = first_descent(sc, node, sp, [&](int s, int right) {
                 if (lane == 0) stk[s] = make_uint4((unsigned)right, live0, live1, 0u);
             });
@@ -714,8 +720,9 @@ __device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float 
             const float4 na = __ldg(sc.nodes + 2 * node);
             const float4 nb = __ldg(sc.nodes + 2 * node + 1);
             const float xy = PruneBound::box_dd_xy(p0, na, nb);
+            const float xy1 = SAME_XY ? xy : PruneBound::box_dd_xy(p1, na, nb);
             const bool h0 = a0 && b0.closer_dd(PruneBound::box_dd_z(p0.z, na, nb, xy));
-            const bool h1 = a1 && b1.closer_dd(PruneBound::box_dd_z(z1, na, nb, xy));
+            const bool h1 = a1 && b1.closer_dd(PruneBound::box_dd_z(z1, na, nb, xy1));
             const unsigned hm0 = __ballot_sync(FULL, h0), hm1 = __ballot_sync(FULL, h1);
             if ((hm0 | hm1) == 0) continue;
             const int left = __float_as_int(nb.z), right = __float_as_int(nb.w);
@@ -732,7 +739,7 @@ __device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float 
                     // where it hit (an unchanged distance leaves its prune bound unchanged)
                     if (h0 || h1) {
                         float dp0, dp1;
-                        leaf_distance2(L, p0, z1, time, dp0, dp1);
+                        leaf_distance2<SAME_XY>(L, p0, p1, time, dp0, dp1);
                         float n0 = s0.d, n1 = s1.d;
                         combine_d2(L.op, L.pos.w, n0, n1, dp0, dp1);
                         s0.d = h0 ? n0 : s0.d;
@@ -800,6 +807,13 @@ __device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float 
     }
     d0 = s0.d;
     d1 = s1.d;
+}
+
+// map_pair for two points per lane that differ only in z: (p0.x, p0.y, p0.z) and (p0.x, p0.y, z1)
+template <bool COUNT = false>
+__device__ __forceinline__ void map_warp2(const SceneView& sc, float3 p0, float z1, bool v0, bool v1, float time,
+                                          float& d0, float& d1, Diag* diag) {
+    map_pair<COUNT, true>(sc, p0, f3(p0.x, p0.y, z1), v0, v1, time, d0, d1, diag);
 }
 
 // map() distance for NP points per lane (32 x NP per warp) that are close together, such as the four
