@@ -235,28 +235,41 @@ __device__ __forceinline__ int scout_bricks(const GridView& g) {
 
 // CULL: the brick lies in coarse block (wx, wy, wz / 2) of 4 x 4 x 4 blocks (32^3 cells); when the
 // surrogate's value at that coarse block's centre exceeds `margin` in magnitude, the brick's blocks
-// are marked inactive without evaluating the scene.
+// are marked inactive without evaluating the scene. The culled scout is a persistent grid whose warps
+// claim one brick at a time (ticket): a culled brick only writes its zero flags, so the resident warps
+// keep walking kept bricks instead of idling in CTAs whose other warps were culled. The plain scout is
+// one warp per brick.
 template <bool CULL>
 __global__ void __launch_bounds__(BLK_THREADS) k_scout_t(GridView g, SceneView sc, float time, unsigned* flags,
                                                          Diag* diag, const float* __restrict__ coarse_f,
-                                                         float margin) {
+                                                         float margin, unsigned* ticket) {
     const int lane = threadIdx.x & 31;
-    const int warp_global = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int nbx = (g.bx + 3) >> 2, nby = (g.by + 3) >> 2, nbz = (g.bz + 1) >> 1;
-    if (warp_global >= nbx * nby * nbz) return;
-    const int wx = warp_global % nbx, t = warp_global / nbx, wy = t % nby, wz = t / nby;
-    if (CULL) {
+    const int nbricks = nbx * nby * nbz;
+    if (!CULL) {
+        const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        if (w >= nbricks) return;
+        const int wx = w % nbx, t = w / nbx, wy = t % nby, wz = t / nby;
+        scout_brick(g, sc, time, wx, wy, wz, flags, diag);
+        return;
+    }
+    for (;;) {
+        int w = 0;
+        if (lane == 0) w = (int)atomicAdd(ticket, 1u);
+        w = __shfl_sync(0xffffffffu, w, 0);
+        if (w >= nbricks) break;
+        const int wx = w % nbx, t = w / nbx, wy = t % nby, wz = t / nby;
         const int bx = wx * 4 + (lane & 3), by = wy * 4 + ((lane >> 2) & 3), bz = wz * 2 + (lane >> 4);
         const bool valid = bx < g.bx && by < g.by && bz < g.bz;
         const float fc = coarse_f[wx + nbx * (wy + nby * (wz >> 1))];
         if (fabsf(fc) > margin) {
             if (valid) flags[bx + g.bx * (by + g.by * bz)] = 0u;
-            return;
+            continue;
         }
         const unsigned v = __ballot_sync(0xffffffffu, valid);
         if (lane == 0) atomicAdd(&diag->scouted, (unsigned long long)__popc(v));
+        scout_brick(g, sc, time, wx, wy, wz, flags, diag);
     }
-    scout_brick(g, sc, time, wx, wy, wz, flags, diag);
 }
 
 // the scout of every scene of a batch in one launch: global brick -> scene -> brick of that scene;

@@ -270,7 +270,7 @@ static cudaError_t run_scout_compact(const GridView& gv, const SceneView& sv, fl
     const int nbricks = ((gv.bx + 3) / 4) * ((gv.by + 3) / 4) * ((gv.bz + 1) / 2);
     const int warps_per_cta = BLK_THREADS / 32;
     k_scout_t<false><<<(nbricks + warps_per_cta - 1) / warps_per_cta, BLK_THREADS, 0, stream>>>(gv, sv, time, flags, diag,
-                                                                                          nullptr, 0.f);
+                                                                                          nullptr, 0.f, nullptr);
     cudaError_t err = check_launch();
     const unsigned tiles = scan_tiles((unsigned)nblocks);
     const cudaError_t em = cudaMemsetAsync(status, 0, (tiles + 1) * sizeof(unsigned long long), stream);

@@ -440,7 +440,7 @@ sdf_status sdf_surrogate_audit(sdf_engine* e, float time, int64_t* violations, i
     const GridView& gv = E.gv;
     const int nbricks = ((gv.bx + 3) / 4) * ((gv.by + 3) / 4) * ((gv.bz + 1) / 2);
     k_scout_t<false><<<(nbricks + BLK_THREADS / 32 - 1) / (BLK_THREADS / 32), BLK_THREADS>>>(gv, sv, time, E.flags,
-                                                                                            &ctrl->diag, nullptr, 0.f);
+                                                                                            &ctrl->diag, nullptr, 0.f, nullptr);
     sdf_status s = surrogate_coarse_eval(E, 0, time);
     if (s != SDF_OK) return s;
     int cx, cy, cz;
