@@ -323,7 +323,7 @@ static sdf_status build_group(BatchGroup& B, const sdf_batch_scene* scenes, unsi
         d.block_base = (unsigned)blocks;
         d.brick_base = (unsigned)bricks;
         blocks += (long long)gv.bx * gv.by * gv.bz;
-        bricks += (long long)((gv.bx + 3) / 4) * ((gv.by + 3) / 4) * ((gv.bz + 1) / 2);
+        bricks += (long long)sdfb::scout_pair_bricks(gv);
         prim_off.push_back(prims.size());
         node_off.push_back(nodes.size());
         prims.insert(prims.end(), sorted.begin(), sorted.end());

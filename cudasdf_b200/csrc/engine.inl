@@ -369,7 +369,7 @@ static void run_culled_scout_compact(EngineImpl& E, const sdfb::SceneView& sv, f
     using namespace sdfb;
     const GridView& gv = E.gv;
     surrogate_coarse_eval(E, st, time);
-    const int nbricks = ((gv.bx + 3) / 4) * ((gv.by + 3) / 4) * ((gv.bz + 1) / 2);
+    const int nbricks = scout_single_bricks(gv);
     const int warps_per_cta = BLK_THREADS / 32;
     k_scout_t<true><<<persistent_grid(k_scout_t<true>, BLK_THREADS, (nbricks + warps_per_cta - 1) / warps_per_cta),
                       BLK_THREADS, 0, st>>>(gv, sv, time, E.flags, &ctrl->diag, E.sur->coarse_f, surrogate_margin(E),

@@ -36,7 +36,7 @@ struct SceneDesc {
     GridView g;
     SceneView sc;
     unsigned block_base;
-    unsigned brick_base;   // first global scout brick (4 x 4 x 2 blocks) of the scene
+    unsigned brick_base;   // first global scout brick (4 x 4 x 4 blocks) of the scene
 };
 
 struct ActiveView {
@@ -210,9 +210,9 @@ __device__ __forceinline__ CellInfo cell_info(const GridView& g, int bx, int by,
 }
 
 // ------------------------------------------------------------------------------------------------
-// scout (MarchingCubesKernels.cu:850-889). Warps take 4x4x2 bricks of blocks so the 32 block
-// centres of a warp are spatially close and their BVH walks coincide; the result is a 0/1 flag per
-// linear block index, compacted in index order afterwards.
+// scout (MarchingCubesKernels.cu:850-889). Warps take bricks of blocks (4x4x4 with two centres per
+// lane, or 4x4x2 with one) so the block centres of a warp are spatially close and their BVH walks
+// coincide; the result is a 0/1 flag per linear block index, compacted in index order afterwards.
 // ------------------------------------------------------------------------------------------------
 // scoutActiveBlocks (MarchingCubesKernels.cu:850-889) for one brick of 4 x 4 x 2 blocks: one warp,
 // one lane per block centre
@@ -229,7 +229,29 @@ __device__ __forceinline__ void scout_brick(const GridView& g, const SceneView& 
     if (valid) flags[bx + g.bx * (by + g.by * bz)] = fabsf(st.d) <= r ? 1u : 0u;
 }
 
-__device__ __forceinline__ int scout_bricks(const GridView& g) {
+// scoutActiveBlocks for one brick of 4 x 4 x 4 blocks: one warp, two z-neighbouring block centres per
+// lane walked together (map_warp2)
+__device__ __forceinline__ void scout_brick_pairs(const GridView& g, const SceneView& sc, float time, int wx, int wy,
+                                                  int wz, unsigned* flags, Diag* diag) {
+    const int lane = threadIdx.x & 31;
+    const int bx = wx * 4 + (lane & 3), by = wy * 4 + ((lane >> 2) & 3), bz0 = wz * 4 + 2 * (lane >> 4), bz1 = bz0 + 1;
+    const bool v0 = bx < g.bx && by < g.by && bz0 < g.bz, v1 = bx < g.bx && by < g.by && bz1 < g.bz;
+    const float3 c0 = f3(FMA(ADD((float)(bx * 8), 4.f), g.cell, g.ox), FMA(ADD((float)(by * 8), 4.f), g.cell, g.oy),
+                         FMA(ADD((float)(bz0 * 8), 4.f), g.cell, g.oz));
+    const float z1 = FMA(ADD((float)(bz1 * 8), 4.f), g.cell, g.oz);
+    float d0, d1;
+    map_warp2<false>(sc, c0, z1, v0, v1, time, d0, d1, diag);
+    const float r = MUL(8 * 0.5f * 1.73205f + 2.0f, g.cell);
+    if (v0) flags[bx + g.bx * (by + g.by * bz0)] = fabsf(d0) <= r ? 1u : 0u;
+    if (v1) flags[bx + g.bx * (by + g.by * bz1)] = fabsf(d1) <= r ? 1u : 0u;
+}
+
+// scout bricks of a grid: 4 x 4 x 4 blocks each for the plain scout (two centres per lane), 4 x 4 x 2
+// for the culled one (one centre per lane)
+__host__ __device__ __forceinline__ int scout_pair_bricks(const GridView& g) {
+    return ((g.bx + 3) >> 2) * ((g.by + 3) >> 2) * ((g.bz + 3) >> 2);
+}
+__host__ __device__ __forceinline__ int scout_single_bricks(const GridView& g) {
     return ((g.bx + 3) >> 2) * ((g.by + 3) >> 2) * ((g.bz + 1) >> 1);
 }
 
@@ -237,22 +259,23 @@ __device__ __forceinline__ int scout_bricks(const GridView& g) {
 // surrogate's value at that coarse block's centre exceeds `margin` in magnitude, the brick's blocks
 // are marked inactive without evaluating the scene. The culled scout is a persistent grid whose warps
 // claim one brick at a time (ticket): a culled brick only writes its zero flags, so the resident warps
-// keep walking kept bricks instead of idling in CTAs whose other warps were culled. The plain scout is
-// one warp per brick.
+// keep walking kept bricks instead of idling in CTAs whose other warps were culled; it keeps one centre
+// per lane, since its few kept bricks are about one wave of warps, which pairs would halve while
+// lengthening each. The plain scout is one warp per 4 x 4 x 4 brick, two centres per lane.
 template <bool CULL>
 __global__ void __launch_bounds__(BLK_THREADS) k_scout_t(GridView g, SceneView sc, float time, unsigned* flags,
                                                          Diag* diag, const float* __restrict__ coarse_f,
                                                          float margin, unsigned* ticket) {
     const int lane = threadIdx.x & 31;
-    const int nbx = (g.bx + 3) >> 2, nby = (g.by + 3) >> 2, nbz = (g.bz + 1) >> 1;
-    const int nbricks = nbx * nby * nbz;
+    const int nbx = (g.bx + 3) >> 2, nby = (g.by + 3) >> 2;
     if (!CULL) {
         const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-        if (w >= nbricks) return;
+        if (w >= scout_pair_bricks(g)) return;
         const int wx = w % nbx, t = w / nbx, wy = t % nby, wz = t / nby;
-        scout_brick(g, sc, time, wx, wy, wz, flags, diag);
+        scout_brick_pairs(g, sc, time, wx, wy, wz, flags, diag);
         return;
     }
+    const int nbricks = scout_single_bricks(g);
     for (;;) {
         int w = 0;
         if (lane == 0) w = (int)atomicAdd(ticket, 1u);
@@ -289,7 +312,7 @@ __global__ void __launch_bounds__(BLK_THREADS) k_scout_batch(const SceneDesc* __
     const int local = (int)(w - d.brick_base);
     const int nbx = (g.bx + 3) >> 2, nby = (g.by + 3) >> 2;
     const int wx = local % nbx, t = local / nbx, wy = t % nby, wz = t / nby;
-    scout_brick(g, d.sc, time, wx, wy, wz, flags + d.block_base, diag);
+    scout_brick_pairs(g, d.sc, time, wx, wy, wz, flags + d.block_base, diag);
 }
 
 // first output vertex of every scene of a batch: the offset of its first active block (the active

@@ -267,7 +267,7 @@ static cudaError_t run_scout_compact(const GridView& gv, const SceneView& sv, fl
                                      unsigned long long* status, int* list, int* count, Diag* diag,
                                      cudaStream_t stream) {
     const int nblocks = gv.bx * gv.by * gv.bz;
-    const int nbricks = ((gv.bx + 3) / 4) * ((gv.by + 3) / 4) * ((gv.bz + 1) / 2);
+    const int nbricks = scout_pair_bricks(gv);
     const int warps_per_cta = BLK_THREADS / 32;
     k_scout_t<false><<<(nbricks + warps_per_cta - 1) / warps_per_cta, BLK_THREADS, 0, stream>>>(gv, sv, time, flags, diag,
                                                                                           nullptr, 0.f, nullptr);

@@ -438,7 +438,7 @@ sdf_status sdf_surrogate_audit(sdf_engine* e, float time, int64_t* violations, i
     record(cudaMemsetAsync(&ctrl->diag, 0, sizeof(Diag), 0));
     const SceneView sv = engine_scene_view(E);
     const GridView& gv = E.gv;
-    const int nbricks = ((gv.bx + 3) / 4) * ((gv.by + 3) / 4) * ((gv.bz + 1) / 2);
+    const int nbricks = scout_pair_bricks(gv);
     k_scout_t<false><<<(nbricks + BLK_THREADS / 32 - 1) / (BLK_THREADS / 32), BLK_THREADS>>>(gv, sv, time, E.flags,
                                                                                             &ctrl->diag, nullptr, 0.f, nullptr);
     sdf_status s = surrogate_coarse_eval(E, 0, time);
