@@ -220,11 +220,12 @@ static void enqueue_group(BatchGroup& B, const BatchGrids& G, float time, const 
             k_dc_quad_list<<<G.count_quads, BLK_THREADS, 0, st>>>(g0, av, D, B.packet_counts, B.block_offsets, B.qrec,
                                                                  D.qcap);
             k_dc_quad_normals<<<G.flat, BLK_THREADS, 0, st>>>(g0, sc0, time, av, D, B.qrec, &ctrl->total_vertices,
-                                                              D.qcap, mo.maxV, B.qnorm, &ctrl->tickets[9], diag);
+                                                              D.qcap, mo.maxV, B.qnorm, &ctrl->tickets[9], diag,
+                                                              &ctrl->dc_vertices, mo, m, B.qp);
         }
         k_dc_quads<<<G.quads, BLK_THREADS, sizeof(QuadSmem), st>>>(g0, sc0, time, av, D, nullptr, B.packet_counts,
                                                                    B.block_offsets, mo, m, B.qp, &ctrl->tickets[2],
-                                                                   diag);
+                                                                   diag, &ctrl->total_vertices, &ctrl->dc_vertices);
     }
     k_batch_scene_first<<<(B.n + 1 + 127) / 128, 128, 0, st>>>(B.desc, B.n, av, B.block_offsets,
                                                                 &ctrl->total_vertices, B.first);

@@ -1181,6 +1181,49 @@ __device__ __forceinline__ bool quad_indices_ok(const DcBuffers& B, const int q[
            B.vert_offsets[q[3]] < maxV;
 }
 
+// The quads can be emitted from the quad list (by k_dc_quad_normals, which holds each quad's corners and
+// winding normal) instead of per block (k_dc_quads) when nothing overflows: every counted quad listed,
+// every cell vertex index and every output vertex within the output's capacity, so every counted quad
+// is emitted, at six times its list index; and no output needs map() at the quad or per-face normals.
+// Both kernels take the decision from the same counts, so exactly one of them emits.
+__device__ __forceinline__ bool quads_from_list(const DcBuffers& B, const unsigned* offsets,
+                                                const unsigned* total_vertices, const unsigned* dc_vertices,
+                                                unsigned maxV, unsigned mask) {
+    if (!B.qnormals || offsets || !total_vertices || !dc_vertices || B.qcap == 0) return false;
+    if (mask & (OUT_COLORS | OUT_PRIMIDS | OUT_UVS | OUT_NORMALS)) return false;
+    const unsigned total = *total_vertices;
+    return total / 6u <= B.qcap && total <= maxV && *dc_vertices <= maxV;
+}
+
+// one emitted quad without per-quad attributes, as k_dc_quads writes it: winding against the normal at
+// the centre, the split diagonal, then the six vertices with identity indices at w, or (indexed output)
+// the corners' cell vertex indices
+__device__ __forceinline__ void emit_quad_plain(QuadVerts& Q, float3 nref, unsigned w, unsigned mask,
+                                                const DcQuadParams& QP, const MeshOut& out) {
+    const int order_a[6] = {0, 1, 2, 0, 2, 3}, order_b[6] = {1, 2, 3, 1, 3, 0};
+    const float3 nt = cross_ff(sub3(Q.v[1], Q.v[0]), sub3(Q.v[2], Q.v[0]));
+    if (dot3(nt, nref) < 0.f) {
+        const float3 t = Q.v[1]; Q.v[1] = Q.v[3]; Q.v[3] = t;
+        const unsigned u = Q.vi[1]; Q.vi[1] = Q.vi[3]; Q.vi[3] = u;
+    }
+    bool alt = false;
+    if (QP.adaptive_diagonal) {
+        const float3 e02 = sub3(Q.v[2], Q.v[0]), e13 = sub3(Q.v[3], Q.v[1]);
+        alt = dot3_rn(e13, e13) < dot3_rn(e02, e02);
+    }
+    if (mask & OUT_WELDED) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) out.indices[w + j] = Q.vi[alt ? order_b[j] : order_a[j]];
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        const int vj = alt ? order_b[j] : order_a[j];
+        out.verts[w + j] = make_float4(Q.v[vj].x, Q.v[vj].y, Q.v[vj].z, 1.f);
+        if ((mask & OUT_INDICES) && out.indices) out.indices[w + j] = w + j;
+    }
+}
+
 // Every counted quad of every active block, in emission order: quad q = (block offset + in-block count
 // prefix) / 6 gets (active block, cell << 2 | axis). The enumeration is k_dc_quads' own.
 __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_list(GridView g0, ActiveView av, DcBuffers B,
@@ -1236,8 +1279,10 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_normals(GridView g0, Sc
                                                                 const unsigned* __restrict__ total_vertices,
                                                                 unsigned cap, unsigned maxV,
                                                                 float4* __restrict__ normals, unsigned* ticket,
-                                                                Diag* diag) {
+                                                                Diag* diag, const unsigned* __restrict__ dc_vertices,
+                                                                MeshOut out, unsigned mask, DcQuadParams QP) {
     const unsigned n = min(*total_vertices / 6u, cap);
+    const bool emit = quads_from_list(B, nullptr, total_vertices, dc_vertices, out.maxV, mask);
     const int nact = active_count(av);
     const int tasks = nact > 0 ? (int)((n + 15u) / 16u) : 0;
     const int lane = threadIdx.x & 31;
@@ -1261,18 +1306,22 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_normals(GridView g0, Sc
         int bx, by, bz;
         block_coord(g, lin, bx, by, bz);
         float3 qc = f3(0.f, 0.f, 0.f);
+        QuadVerts Q;
+        bool ok = false;
         if (live) {
             const CellInfo c = cell_info(g, bx, by, bz, tid);
             int q[4];
             if (quad_cells(g, b2a, axis, c.x, c.y, c.z, q)) {
-                QuadVerts Q;
                 Q.qc = f3(0.f, 0.f, 0.f);
-                quad_vertices(g, av.list, bbase, B, q, maxV, Q);  // a skipped quad's normal stays unused
+                ok = quad_vertices(g, av.list, bbase, B, q, maxV, Q);  // a skipped quad's normal stays unused
                 qc = Q.qc;
             }
         }
         const float3 nn = stencil_normal_pairs(av, sc, bbase, qc, g.cell, live, time, diag);
-        if (live && (lane & 1) == 0) normals[qi] = make_float4(nn.x, nn.y, nn.z, 0.f);
+        if (live && (lane & 1) == 0) {
+            normals[qi] = make_float4(nn.x, nn.y, nn.z, 0.f);
+            if (emit && ok) emit_quad_plain(Q, nn, 6u * qi, mask, QP, out);  // k_dc_quads stands aside
+        }
     }
 }
 
@@ -1282,9 +1331,12 @@ __global__ void __launch_bounds__(BLK_THREADS, 3) k_dc_quads(GridView g0, SceneV
                                                           const unsigned* __restrict__ counts,
                                                           const unsigned* __restrict__ block_offsets, MeshOut out,
                                                           unsigned mask, DcQuadParams QP, unsigned* ticket,
-                                                          Diag* diag) {
+                                                          Diag* diag, const unsigned* __restrict__ total_vertices,
+                                                          const unsigned* __restrict__ dc_vertices) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     QuadSmem& S = *reinterpret_cast<QuadSmem*>(dyn_smem);
+    // k_dc_quad_normals emitted every quad from the quad list
+    if (quads_from_list(B, offsets, total_vertices, dc_vertices, out.maxV, mask)) return;
     const int n = active_count(av);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     const int order_a[6] = {0, 1, 2, 0, 2, 3}, order_b[6] = {1, 2, 3, 1, 3, 0};

@@ -934,19 +934,21 @@ static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* o
             E.block_totals, E.block_offsets, (unsigned)cap, &ctrl->active_count, 1, scan_state(scanB),
             &ctrl->total_vertices, diag);
         check_launch();
+        DcQuadParams qp;
+        qp.adaptive_diagonal = (C.dc_solver == SDF_DC_SOLVER_MASSPOINT) ? C.adaptive_diagonal : 0;
         if (qlist) {
             k_dc_quad_list<<<std::min(cap, num_sms() * 8), BLK_THREADS, 0, st>>>(gv, av, B, E.packet_counts,
                                                                                    E.block_offsets, E.dc_qrec, B.qcap);
             k_dc_quad_normals<<<persistent_grid(k_dc_quad_normals, BLK_THREADS, std::max(1, (int)(B.qcap / 256))),
                                 BLK_THREADS, 0, st>>>(gv, sv, time, av, B, E.dc_qrec, &ctrl->total_vertices, B.qcap,
-                                                      mo.maxV, E.dc_qnorm, &ctrl->tickets[9], diag);
+                                                      mo.maxV, E.dc_qnorm, &ctrl->tickets[9], diag, &ctrl->dc_vertices,
+                                                      mo, mask, qp);
             check_launch();
         }
-        DcQuadParams qp;
-        qp.adaptive_diagonal = (C.dc_solver == SDF_DC_SOLVER_MASSPOINT) ? C.adaptive_diagonal : 0;
         const size_t quad_smem = sizeof(QuadSmem);
         k_dc_quads<<<persistent_grid(k_dc_quads, BLK_THREADS, cap, quad_smem), BLK_THREADS, quad_smem, st>>>(
-            gv, sv, time, av, B, nullptr, E.packet_counts, E.block_offsets, mo, mask, qp, &ctrl->tickets[2], diag);
+            gv, sv, time, av, B, nullptr, E.packet_counts, E.block_offsets, mo, mask, qp, &ctrl->tickets[2], diag,
+            &ctrl->total_vertices, &ctrl->dc_vertices);
         check_launch();
         if (welded) {  // indexed output: the cell vertices themselves
             k_dc_weld_vertices<<<persistent_grid(k_dc_weld_vertices, 256, cap * 2), 256, 0, st>>>(

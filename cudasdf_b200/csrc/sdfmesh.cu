@@ -482,7 +482,8 @@ void launchDCGenerateQuads(sdf_grid* grid, int numActiveBlocks, float time) {
     const size_t smem = sizeof(QuadSmem);
     k_dc_quads<<<persistent_grid(k_dc_quads, BLK_THREADS, numActiveBlocks, smem), BLK_THREADS, smem>>>(
         grid_view(*grid), scene_view(*grid), time, av, dc_buffers_of(*grid), grid->d_packetVertexOffsets,
-        grid->d_packetVertexCounts, nullptr, mesh_out_of(*grid), out_mask_of(*grid), qp, s.tickets, s.diag);
+        grid->d_packetVertexCounts, nullptr, mesh_out_of(*grid), out_mask_of(*grid), qp, s.tickets, s.diag, nullptr,
+        nullptr);
     check_launch();
 }
 
