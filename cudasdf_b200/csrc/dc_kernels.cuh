@@ -1321,6 +1321,9 @@ __global__ void __launch_bounds__(BLK_THREADS) k_dc_quad_normals(GridView g0, Sc
         if (live && (lane & 1) == 0) {
             normals[qi] = make_float4(nn.x, nn.y, nn.z, 0.f);
             if (emit && ok) emit_quad_plain(Q, nn, 6u * qi, mask, QP, out);  // k_dc_quads stands aside
+            // a listed quad always has its cells and corners when nothing overflows; one without them
+            // would be written by neither kernel
+            if (emit && !ok && diag) atomicExch(&diag->inconsistent, 1);
         }
     }
 }
