@@ -381,8 +381,8 @@ sdf_status sdf_surrogate_enable(sdf_engine* e, int enabled);
  * network: the exact map() at each coarse centre, one evaluation per 32^3 cells, culled when
  * |f| > K + extra_margin (extra_margin >= 0 is ignored by the other modes). The capped, pruned field
  * of smooth-blended primitives is not 1-Lipschitz (a coarse centre whose search hits the 256-step cap
- * can read far too large a distance), so extra_margin = 0 is not safe in general; the audit below is
- * the judge. The exact mode needs no training and stays on across scene changes. */
+ * can read far too large a distance), so extra_margin = 0 is not safe in general; the audit below
+ * decides whether a margin is. The exact mode needs no training and stays on across scene changes. */
 #define SDF_CULL_NONE 0
 #define SDF_CULL_SURROGATE 1
 #define SDF_CULL_EXACT 2
