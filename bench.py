@@ -3,8 +3,8 @@
 Workload (default, c4): marching cubes over a 1024^3 grid on [-1, 1]^3 of a seeded composite scene of
 16384 smooth-blended primitives (sphere/box/capsule/torus, sizes log-uniform in [0.02, 0.2]); VBO
 (float4 positions) + EBO (uint32 indices). A step is one full extraction with the scene already on
-the device: (surrogate coarse-block inference ->) scout -> compaction -> block field (own samples,
-then halos) -> block scan -> emission.
+the device: (surrogate coarse-block inference, once per scene ->) scout -> compaction -> block field
+(own samples, then halos, then the gather's classification and counts) -> block scan -> emission.
 
   value  = grid samples (1024^3) per second of device time of the surrogate-culled extraction, summed
            over ranks; the network is trained, certified and audited once before the timed region
@@ -235,7 +235,12 @@ def run_ours(args, rank, world):
     times, st, out["plain_stages"] = timed_extractions(eng, buf, args.steps, flush, world)
     plain_ms = max_over_ranks(sum(times) / len(times), world)
     out["plain"] = {"ms": plain_ms, "value": job_throughput(world, voxels, plain_ms), "stats": st}
-    launches_per_step = 6  # scout, compaction, own field, halo field, block scan, emission
+    # marching cubes: scout, compaction, halo plan, own samples, halo misses, gather (classification and
+    # counts), block scan, emission; dual contouring (mass-point, projection steps): scout, compaction,
+    # block map, halo plan, own samples, halo misses, gather, mark, cell scan, Hermite representatives,
+    # Hermite normals, solve, projection, quad counts, block scan, quad list, quad normals (and their
+    # emission), quads
+    launches_per_step = 8 if tech == 0 else 18
     if surrogate:
         plain_verts = buf.vertices[:V].clone()
         t0 = time.perf_counter()
@@ -245,8 +250,7 @@ def run_ours(args, rank, world):
         audit = eng.surrogate_audit(0.0)
         out["surrogate"] = {"train": sst, "train_wall_ms": train_wall, "audit": audit}
         if audit["violations"] == 0:
-            eng.surrogate_enable(True)
-            launches_per_step = 7  # + the surrogate's coarse-block inference
+            eng.surrogate_enable(True)  # the coarse values are kept while the scene is unchanged
         else:  # the exact audit decides: a violated certificate falls back to the plain path
             out["surrogate"]["fallback"] = "audit found active blocks in culled coarse blocks"
         for _ in range(args.warmup):
@@ -991,10 +995,14 @@ def roofline(r):
     ms_field = r["stages"]["ms_field"]
     if not c or not peak or not ms_field:
         return None
+    # the walks' time: the block-field stage without its gather (timed by its own events), which
+    # classifies and counts
+    ms_walks = ms_field - (r["stages"].get("ms_classify") or 0.0)
     flops = c["field_node_visits"] * FLOP_PER_NODE + c["field_leaf_evals"] * FLOP_PER_LEAF
-    achieved = flops / (ms_field * 1e-3) / 1e12
+    achieved = flops / (ms_walks * 1e-3) / 1e12
     active = r["stats"]["active_blocks"]
-    return {"kernel": "block field stage (k_field_own + k_field_miss: warp-coherent BVH map())", "bound": "fp32",
+    return {"kernel": "block field stage (k_field_plan + k_field_own + k_field_miss: warp-coherent BVH map())",
+            "bound": "fp32", "ms": ms_walks,
             "achieved": achieved,
             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": "measured by the library's FMA loop on this GPU (no FP32 figure in MEASURED_PEAKS.json)",
