@@ -66,3 +66,21 @@ def test_stage_roofline_arithmetic():
     assert abs(out["emission"]["frac"] - out["emission"]["achieved"] / peak) < 1e-12
     untimed = bench.stage_roofline({"stats": r["stats"], "stages": {}})  # timing off: no stage entries
     assert "scan" not in untimed and "emission" not in untimed and untimed["peak"] == peak
+
+
+def test_field_roofline_arithmetic():
+    """The dominant kernel's FP32 fraction: counted FLOPs over the field stage's time without its gather."""
+    import bench
+    c = {"field_node_visits": 1_000_000, "field_leaf_evals": 100_000}
+    r = {"counters": c, "fp32_peak": 70.0, "stats": {"active_blocks": 1000},
+         "stages": {"ms_field": 1.2, "ms_classify": 0.2}}
+    out = bench.roofline(r)
+    flops = 1_000_000 * bench.FLOP_PER_NODE + 100_000 * bench.FLOP_PER_LEAF
+    assert abs(out["ms"] - 1.0) < 1e-12
+    assert abs(out["achieved"] - flops / 1e-3 / 1e12) < 1e-9
+    assert abs(out["frac"] - out["achieved"] / 70.0) < 1e-12
+    assert abs(out["traffic"] - bench.TRAFFIC_PER_ACTIVE_BLOCK * 1000) < 1e-6
+    # without the gather's own timing the whole stage counts
+    r["stages"] = {"ms_field": 1.2}
+    assert abs(bench.roofline(r)["ms"] - 1.2) < 1e-12
+    assert bench.roofline({"counters": None, "fp32_peak": 70.0, "stats": {}, "stages": {"ms_field": 1.0}}) is None
