@@ -165,6 +165,10 @@ struct EngineImpl {
     // per-cell DC arrays, weld bitmaps); grown after an extraction that found more (engine_grow_rows)
     int rows_cap = 0;
     cudaEvent_t ev[8] = {};
+    // the halo misses run on a second stream beside the own samples (they write other row entries and
+    // both need only the plan): the miss kernel's CTAs take the SMs the own-sample kernel's last wave frees
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     size_t packet_cap = 0;
     unsigned* miss = nullptr;          // listed halo samples, capacity nblocks * HALO_N
     size_t miss_cap = 0;
@@ -219,6 +223,9 @@ struct EngineImpl {
         scene_ev_pending = false;
         for (auto& e : ev)
             if (e) { cudaEventDestroy(e); e = nullptr; }
+        if (fork_ev) { cudaEventDestroy(fork_ev); fork_ev = nullptr; }
+        if (join_ev) { cudaEventDestroy(join_ev); join_ev = nullptr; }
+        if (side) { cudaStreamDestroy(side); side = nullptr; }
         delete sur;
         sur = nullptr;
     }
@@ -285,12 +292,23 @@ static sdf_status run_block_field(EngineImpl& E, const sdfb::SceneView& sv, floa
     }
     k_field_plan<<<num_sms() * 8, 256, 0, st>>>(E.gv, av, E.flags, E.fields, E.b2a, E.miss, &ctrl->halo_misses);
     check_launch();
+    // own samples on the extraction's stream, then the halo misses beside them on the second stream
+    const bool fork = E.side && E.fork_ev && E.join_ev;
+    if (fork) {
+        record(cudaEventRecord(E.fork_ev, st));
+        record(cudaStreamWaitEvent(E.side, E.fork_ev, 0));
+    }
     k_field_own<COUNT><<<persistent_grid(k_field_own<COUNT>, BLK_THREADS, E.rows_cap), BLK_THREADS, 0, st>>>(
         E.gv, sv, time, av, E.fields, &ctrl->tickets[0], &ctrl->diag);
     check_launch();
-    k_field_miss<COUNT><<<persistent_grid(k_field_miss<COUNT>, BLK_THREADS, 1 << 30), BLK_THREADS, 0, st>>>(
-        E.gv, sv, time, av, E.fields, E.miss, &ctrl->halo_misses, &ctrl->tickets[4], &ctrl->diag);
+    k_field_miss<COUNT><<<persistent_grid(k_field_miss<COUNT>, BLK_THREADS, 1 << 30), BLK_THREADS, 0,
+                          fork ? E.side : st>>>(E.gv, sv, time, av, E.fields, E.miss, &ctrl->halo_misses,
+                                                &ctrl->tickets[4], &ctrl->diag);
     check_launch();
+    if (fork) {
+        record(cudaEventRecord(E.join_ev, E.side));
+        record(cudaStreamWaitEvent(st, E.join_ev, 0));
+    }
     if (E.timing) cudaEventRecord(E.ev[5], st);  // the gather: halos, case codes, counts
     k_field_gather<<<persistent_grid(k_field_gather, BLK_THREADS, (E.rows_cap + GATHER_WARPS - 1) / GATHER_WARPS),
                      BLK_THREADS, 0, st>>>(E.gv, av, E.fields, E.b2a, E.flags,
@@ -396,6 +414,14 @@ sdf_status sdf_engine_create(sdf_engine** out, int device) {
     for (auto& ev : e->impl.ev) cudaEventCreate(&ev);
     for (auto& pd : e->impl.pend) cudaEventCreateWithFlags(&pd.done, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&e->impl.scene_ev, cudaEventDisableTiming);
+    // without the second stream or its events the halo misses run after the own samples on one stream
+    if (cudaStreamCreateWithFlags(&e->impl.side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->impl.fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->impl.join_ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (e->impl.side) cudaStreamDestroy(e->impl.side);
+        e->impl.side = nullptr;
+    }
     *out = e;
     return SDF_OK;
 }
