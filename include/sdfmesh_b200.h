@@ -254,8 +254,7 @@ sdf_status sdf_engine_set_scene_device(sdf_engine* e, const sdf_primitive* prims
 /* One extraction on `stream` (a cudaStream_t, NULL = legacy default stream). The only host
  * synchronisation is the final count read-back into *stats. One stage (the halo samples of the block
  * field) runs on a second, non-blocking stream the engine owns, forked from and joined back into
- * `stream` by events, so the extraction stays ordered on `stream` as a whole (and can be captured from
- * it into a CUDA graph). */
+ * `stream` by events, so the extraction stays ordered on `stream` as a whole. */
 sdf_status sdf_engine_extract(sdf_engine* e, float time, const sdf_outputs* out, void* stream, sdf_stats* stats);
 /* The extraction of sdf_engine_extract split in two, so that a caller can keep the GPU busy while it
  * reads back earlier results: _async enqueues the whole extraction on `stream` and returns without
