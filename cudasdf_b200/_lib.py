@@ -170,6 +170,7 @@ ENGINE_SYMBOLS = ["sdf_engine_create", "sdf_engine_destroy", "sdf_engine_configu
                   "sdf_engine_set_scene_device",
                   "sdf_engine_set_scene_async", "sdf_engine_extract_async", "sdf_engine_extract_wait",
                   "sdf_engine_extract", "sdf_engine_set_timing", "sdf_engine_set_debug", "sdf_engine_get_bvh",
+                  "sdf_build_bvh_host",
                   "sdf_engine_buffer", "sdf_engine_read_buffer", "sdf_engine_eval", "sdf_engine_eval_distance", "sdf_engine_eval_normals", "sdf_engine_count_work", "sdf_measure_fp32_peak", "sdf_extract", "sdf_last_error", "sdf_version"]
 
 _lib = None

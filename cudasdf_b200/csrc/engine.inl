@@ -700,6 +700,24 @@ int sdf_engine_get_bvh(sdf_engine* e, sdf_bvh_node* nodes_out, int capacity, int
     return E.nnodes;
 }
 
+int sdf_build_bvh_host(const sdf_primitive* prims, int count, sdf_primitive* sorted_out, sdf_bvh_node* nodes_out,
+                       int capacity, int* num_bvh_primitives) {
+    if (count < 0 || (count > 0 && (!prims || !sorted_out))) return -1;
+    std::vector<sdf_primitive> sorted;
+    std::vector<sdf_bvh_node> nodes;
+    int nbvh = 0;
+    try {
+        nbvh = sdfb::prepare_scene(prims, count, sorted, nodes);
+    } catch (...) {
+        return -1;  // out of host memory
+    }
+    if (!nodes.empty() && (!nodes_out || capacity < (int)nodes.size())) return -1;
+    for (int i = 0; i < count; ++i) sorted_out[i] = sorted[i];
+    for (size_t i = 0; i < nodes.size(); ++i) nodes_out[i] = nodes[i];
+    if (num_bvh_primitives) *num_bvh_primitives = nbvh;
+    return (int)nodes.size();
+}
+
 // Enqueues one extraction on `st` (no host synchronisation): the final counts are copied into the
 // slot's pinned Ctrl and the slot's event is recorded after them.
 static sdf_status engine_enqueue(EngineImpl& E, float time, const sdf_outputs* out, cudaStream_t st,

@@ -283,6 +283,14 @@ void sdf_engine_set_timing(sdf_engine* e, int enabled);
 void sdf_engine_set_debug(sdf_engine* e, int flags);
 /* The scene as uploaded: sorted primitives (count = numPrimitives) and BVH nodes. */
 int sdf_engine_get_bvh(sdf_engine* e, sdf_bvh_node* nodes_out, int capacity, int* num_bvh_primitives);
+/* The host scene build of sdf_engine_set_scene on its own, no GPU involved: CudaSDFMesh::UpdateBVH
+ * (CudaSDFMesh.cpp:216-249) with getPrimitiveAABB and buildBVHRecursive (CudaSDFUtil.h:507-603).
+ * `sorted_out` (count records) receives the primitives, unions first in their order and then the rest
+ * in theirs; `nodes_out` (capacity >= 2 * unions - 1) the BVH over the unions in the reference's node
+ * order. Returns the number of nodes (0 without unions), or -1 for a null pointer, a negative count or
+ * too small a capacity; *num_bvh_primitives (if set) receives the number of unions. */
+int sdf_build_bvh_host(const sdf_primitive* prims, int count, sdf_primitive* sorted_out, sdf_bvh_node* nodes_out,
+                       int capacity, int* num_bvh_primitives);
 /* Device pointer to the last extraction's internal arrays, for inspection: 0 active block list,
  * 1 per-cell vertex counts (compat layout), 2 per-cell offsets, 3 DC corner masks, 4 DC cell vertex
  * offsets, 5 DC cell vertices, 6 DC cell normals, 7 per-block vertex totals, 8 block field rows; and
